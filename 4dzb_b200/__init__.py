@@ -1,0 +1,382 @@
+"""fdzb-b200: B200-native FDZB soft shadows (4DZB's FDZB_Soft_Shadow path).
+
+The compute path is ``libfdzb.so`` (hand-written sm_100a CUDA behind the C ABI
+declared in ``include/fdzb.h``).  This module is a thin ctypes binding:
+
+* :class:`Context` wraps the re-entrant ``fdzb_ctx_*`` API;
+* the ``FD*`` functions mirror the reference's ``namespace FD`` entry points
+  (4DZB/FDZB_Soft_Shadow/api.h:10-56) on a process-wide context, with device
+  tensors (or raw device pointers) in place of GL object names.
+
+There is no CPU fallback: importing works anywhere, but every call that needs
+the library raises :class:`FdzbError` if ``libfdzb.so`` is missing or no CUDA
+device is present.  Build with ``python 4dzb_b200/build.py``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfdzb.so")
+
+FDZB_OK = 0
+ERRORS = {
+    -1: "FDZB_ERR_INVALID_ARG", -2: "FDZB_ERR_CUDA", -3: "FDZB_ERR_NOT_INITIALIZED",
+    -4: "FDZB_ERR_NO_MEMORY", -5: "FDZB_ERR_CAPACITY", -6: "FDZB_ERR_DEVICE_TIMEOUT",
+    -7: "FDZB_ERR_UNSUPPORTED", -8: "FDZB_ERR_NOT_READY",
+}
+
+ARRAYS = {
+    "sample_keys": (0, np.int32), "sorted_sample_keys": (1, np.int32), "sorted_sample_ids": (2, np.int32),
+    "bin_sample_start": (3, np.int32), "bin_sample_end": (4, np.int32), "bin_maxz": (5, np.float32),
+    "bin_range": (6, np.float32), "tri_count": (7, np.int32), "pair_bin": (8, np.int32),
+    "pair_tri": (9, np.int32), "sorted_pair_bin": (10, np.int32), "sorted_pair_tri": (11, np.int32),
+    "bin_tri_start": (12, np.int32), "bin_tri_end": (13, np.int32), "tri_aabb": (14, np.float32),
+}
+
+# Every symbol declared in include/fdzb.h.
+EXPORTED = [
+    "fdzb_init", "fdzb_set_backface_cull", "fdzb_add_model", "fdzb_set_sample_buffers",
+    "fdzb_set_output_buffer", "fdzb_register_resources", "fdzb_unregister_resources",
+    "fdzb_set_bin_num", "fdzb_set_view", "fdzb_set_scenes_esp", "fdzb_set_scene_params",
+    "fdzb_set_area_light", "fdzb_launch", "fdzb_move_model", "fdzb_last_error",
+    "fdzb_ctx_create", "fdzb_ctx_destroy", "fdzb_ctx_set_stream", "fdzb_ctx_set_backface_cull",
+    "fdzb_ctx_add_model", "fdzb_ctx_set_sample_buffers", "fdzb_ctx_set_output_buffer",
+    "fdzb_ctx_set_bin_num", "fdzb_ctx_set_view", "fdzb_ctx_set_scenes_esp",
+    "fdzb_ctx_set_scene_params", "fdzb_ctx_set_area_light", "fdzb_ctx_move_model",
+    "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
+    "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_light_setup", "fdzb_version",
+]
+
+
+class FdzbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class AreaLightDesc(ctypes.Structure):
+    """Same 52-byte layout as AreaLightDes (4DZB/FDZB_Soft_Shadow/AreaLightDesc.h:3-14)."""
+    _fields_ = [("rightRadius", ctypes.c_float), ("topRadius", ctypes.c_float),
+                ("position", ctypes.c_float * 3), ("viewDir", ctypes.c_float * 3),
+                ("upDir", ctypes.c_float * 3), ("lightResWidth", ctypes.c_int32),
+                ("lightResHeight", ctypes.c_int32)]
+
+    @classmethod
+    def from_light(cls, light) -> "AreaLightDesc":
+        d = cls()
+        d.rightRadius = light.right_radius
+        d.topRadius = light.top_radius
+        d.position[:] = list(light.position)
+        d.viewDir[:] = list(light.view_dir)
+        d.upDir[:] = list(light.up_dir)
+        d.lightResWidth = light.n
+        d.lightResHeight = light.n
+        return d
+
+
+class FrameStats(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("valid_samples", ctypes.c_int32),
+                ("valid_triangles", ctypes.c_int32), ("num_pairs", ctypes.c_int32),
+                ("num_bins", ctypes.c_int32), ("pair_capacity", ctypes.c_int32),
+                ("pair_tests", ctypes.c_int64), ("f", ctypes.c_float), ("sub", ctypes.c_float * 2),
+                ("lp_begin", ctypes.c_float * 3), ("lp_end", ctypes.c_float * 3),
+                ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 6),
+                ("model_aabb", ctypes.c_float * 6), ("replans", ctypes.c_int32),
+                ("quirk_key_range", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def lib_available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def load() -> ctypes.CDLL:
+    """Load libfdzb.so (raises FdzbError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FdzbError(-3, f"{LIB_PATH} not built (python 4dzb_b200/build.py)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, sz, f32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_float
+    P = ctypes.POINTER
+    sig = {
+        "fdzb_init": ([], i32), "fdzb_set_backface_cull": ([i32], i32),
+        "fdzb_add_model": ([vp, sz, sz, vp, sz, ctypes.c_char_p], i32),
+        "fdzb_set_sample_buffers": ([vp, vp], i32), "fdzb_set_output_buffer": ([vp, vp], i32),
+        "fdzb_register_resources": ([], i32), "fdzb_unregister_resources": ([], i32),
+        "fdzb_set_bin_num": ([sz], i32), "fdzb_set_view": ([i32, i32], i32),
+        "fdzb_set_scenes_esp": ([f32], i32), "fdzb_set_scene_params": ([sz, sz], i32),
+        "fdzb_set_area_light": ([P(AreaLightDesc)], i32), "fdzb_launch": ([], f32),
+        "fdzb_move_model": ([P(ctypes.c_float)], i32), "fdzb_last_error": ([], ctypes.c_char_p),
+        "fdzb_ctx_create": ([P(vp), i32], i32), "fdzb_ctx_destroy": ([vp], i32),
+        "fdzb_ctx_set_stream": ([vp, vp], i32), "fdzb_ctx_set_backface_cull": ([vp, i32], i32),
+        "fdzb_ctx_add_model": ([vp, vp, sz, sz, vp, sz, ctypes.c_char_p], i32),
+        "fdzb_ctx_set_sample_buffers": ([vp, vp, vp], i32),
+        "fdzb_ctx_set_output_buffer": ([vp, vp, vp], i32), "fdzb_ctx_set_bin_num": ([vp, sz], i32),
+        "fdzb_ctx_set_view": ([vp, i32, i32], i32), "fdzb_ctx_set_scenes_esp": ([vp, f32], i32),
+        "fdzb_ctx_set_scene_params": ([vp, sz, sz], i32),
+        "fdzb_ctx_set_area_light": ([vp, P(AreaLightDesc)], i32),
+        "fdzb_ctx_move_model": ([vp, P(ctypes.c_float)], i32),
+        "fdzb_ctx_launch": ([vp, P(ctypes.c_float)], i32), "fdzb_ctx_launch_async": ([vp], i32),
+        "fdzb_ctx_sync": ([vp], i32), "fdzb_ctx_get_stats": ([vp, P(FrameStats)], i32),
+        "fdzb_ctx_export": ([vp, i32, vp, sz], i32), "fdzb_ctx_set_debug": ([vp, i32], i32),
+        "fdzb_light_setup": ([P(AreaLightDesc), P(ctypes.c_float), P(ctypes.c_float),
+                              P(ctypes.c_float), P(ctypes.c_float)], i32),
+        "fdzb_version": ([], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> int:
+    if rc != FDZB_OK:
+        msg = load().fdzb_last_error().decode()
+        raise FdzbError(rc, msg)
+    return rc
+
+
+def _ptr(x) -> Optional[int]:
+    """Device pointer of a torch tensor, or an int pointer, or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return int(x.data_ptr())
+
+
+def light_setup(light) -> dict:
+    """Host light setup (FS/api.cpp:303-400) as computed by the library."""
+    lib = load()
+    d = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+    mat = (ctypes.c_float * 16)()
+    rf = (ctypes.c_float * 2)()
+    corners = (ctypes.c_float * 12)()
+    deltas = (ctypes.c_float * 6)()
+    _check(lib.fdzb_light_setup(ctypes.byref(d), mat, rf, corners, deltas))
+    return dict(mat=np.array(mat, dtype=np.float32), RF=np.array(rf, dtype=np.float32),
+                corners=np.array(corners, dtype=np.float32).reshape(4, 3),
+                deltas=np.array(deltas, dtype=np.float32).reshape(2, 3))
+
+
+def mask_words(n: int) -> int:
+    return (n * n + 31) // 32
+
+
+class Context:
+    """One scene / view / light on one device (the fdzb_ctx_* API)."""
+
+    def __init__(self, device: int = -1):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        _check(self._lib.fdzb_ctx_create(ctypes.byref(h), device))
+        self._h = h
+        self._keep = []  # tensors whose memory the context references
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fdzb_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream) -> None:
+        _check(self._lib.fdzb_ctx_set_stream(self._h, ctypes.c_void_p(stream)))
+
+    def set_backface_cull(self, enable: bool) -> None:
+        _check(self._lib.fdzb_ctx_set_backface_cull(self._h, int(bool(enable))))
+
+    def set_debug(self, flags: int) -> None:
+        """flags bit 0: keep pre-sort copies of the key arrays for export()."""
+        _check(self._lib.fdzb_ctx_set_debug(self._h, int(flags)))
+
+    def add_model(self, vtx, n_vtx: int, stride_bytes: int, idx, n_tri: int, name: str = "") -> None:
+        self._keep += [vtx, idx]
+        _check(self._lib.fdzb_ctx_add_model(self._h, _ptr(vtx), n_vtx, stride_bytes, _ptr(idx), n_tri,
+                                             name.encode()))
+
+    def set_sample_buffers(self, pos, nrm) -> None:
+        self._keep += [pos, nrm]
+        _check(self._lib.fdzb_ctx_set_sample_buffers(self._h, _ptr(pos), _ptr(nrm)))
+
+    def set_output_buffer(self, shadow, masks=None) -> None:
+        self._keep += [shadow, masks]
+        _check(self._lib.fdzb_ctx_set_output_buffer(self._h, _ptr(shadow), _ptr(masks)))
+
+    def set_bin_num(self, n: int) -> None:
+        _check(self._lib.fdzb_ctx_set_bin_num(self._h, n))
+
+    def set_view(self, w: int, h: int) -> None:
+        _check(self._lib.fdzb_ctx_set_view(self._h, w, h))
+
+    def set_scenes_esp(self, esp: float) -> None:
+        _check(self._lib.fdzb_ctx_set_scenes_esp(self._h, esp))
+
+    def set_scene_params(self, max_tri: int, max_vert: int) -> None:
+        _check(self._lib.fdzb_ctx_set_scene_params(self._h, max_tri, max_vert))
+
+    def set_area_light(self, light) -> None:
+        d = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+        _check(self._lib.fdzb_ctx_set_area_light(self._h, ctypes.byref(d)))
+
+    def move_model(self, m) -> None:
+        arr = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
+        _check(self._lib.fdzb_ctx_move_model(self._h, arr))
+
+    def launch(self) -> float:
+        ms = ctypes.c_float()
+        _check(self._lib.fdzb_ctx_launch(self._h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def launch_async(self) -> None:
+        _check(self._lib.fdzb_ctx_launch_async(self._h))
+
+    def sync(self) -> None:
+        _check(self._lib.fdzb_ctx_sync(self._h))
+
+    def stats(self) -> dict:
+        st = FrameStats()
+        _check(self._lib.fdzb_ctx_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def export(self, name: str, count: int) -> np.ndarray:
+        what, dt = ARRAYS[name]
+        out = np.empty(count, dtype=dt)
+        if count:
+            _check(self._lib.fdzb_ctx_export(self._h, what, out.ctypes.data, out.nbytes))
+        return out
+
+
+# ---- FD:: namespace mirror (process-wide context) --------------------------
+
+_fd_keep: list = []
+
+
+def FDinit() -> None:
+    """FD::FDinit (FS/api.h:15)."""
+    _fd_keep.clear()
+    _check(load().fdzb_init())
+
+
+def FDsetBackfaceCull(enable: bool) -> None:
+    _check(load().fdzb_set_backface_cull(int(bool(enable))))
+
+
+def FDaddModel(vtx, idx, vertex_size_bytes: int, model_name: str = "", n_vtx: Optional[int] = None,
+               n_tri: Optional[int] = None) -> None:
+    """FD::FDaddModel (FS/api.h:21): vtx/idx are device tensors (VBO/IBO)."""
+    _fd_keep.extend([vtx, idx])
+    if n_vtx is None:
+        n_vtx = vtx.numel() * vtx.element_size() // vertex_size_bytes
+    if n_tri is None:
+        n_tri = idx.numel() // 3
+    _check(load().fdzb_add_model(_ptr(vtx), n_vtx, vertex_size_bytes, _ptr(idx), n_tri, model_name.encode()))
+
+
+def FDsetSampleGLTex(pos, nrm) -> None:
+    """FD::FDsetSampleGLTex (FS/api.h:24): device float4 position / normal images."""
+    _fd_keep.extend([pos, nrm])
+    _check(load().fdzb_set_sample_buffers(_ptr(pos), _ptr(nrm)))
+
+
+def FDsetOutputGLBuffer(shadow, masks=None) -> None:
+    """FD::FDsetOutputGLBuffer (FS/api.h:27)."""
+    _fd_keep.extend([shadow, masks])
+    _check(load().fdzb_set_output_buffer(_ptr(shadow), _ptr(masks)))
+
+
+def FDregisterGLres() -> None:
+    _check(load().fdzb_register_resources())
+
+
+def FDunregisterGLres() -> None:
+    _check(load().fdzb_unregister_resources())
+
+
+def FDsetBinNum(bin_num: int) -> int:
+    """FD::FDsetBinNum (FS/api.h:36): 0 on success, -1 if rejected."""
+    rc = load().fdzb_set_bin_num(bin_num)
+    return 0 if rc == FDZB_OK else -1
+
+
+def FDsetView(w: int, h: int) -> None:
+    _check(load().fdzb_set_view(w, h))
+
+
+def FDsetScenesEsp(esp: float) -> None:
+    _check(load().fdzb_set_scenes_esp(esp))
+
+
+def FDsetSceneParams(max_tri: int, max_vert: int) -> None:
+    _check(load().fdzb_set_scene_params(max_tri, max_vert))
+
+
+def FDsetAreaLight(light) -> None:
+    d = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+    _check(load().fdzb_set_area_light(ctypes.byref(d)))
+
+
+def FDLaunch() -> float:
+    """FD::FDLaunch (FS/api.h:52): frame GPU time in ms."""
+    ms = float(load().fdzb_launch())
+    if ms < 0:
+        _check(int(ms))
+    return ms
+
+
+def moveModel(m) -> None:
+    arr = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
+    _check(load().fdzb_move_model(arr))
+
+
+def upload_scene(scene, device: str = "cuda"):
+    """Device tensors of a scenes.Scene: (pos, nrm, vtx, idx)."""
+    import torch
+    pos = torch.from_numpy(scene.pos).to(device)
+    nrm = torch.from_numpy(scene.nrm).to(device)
+    vtx = torch.from_numpy(scene.vtx).to(device)
+    idx = torch.from_numpy(scene.idx).to(device)
+    return pos, nrm, vtx, idx
+
+
+def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bool = False):
+    """A Context with the scene's buffers uploaded and outputs allocated.
+    Returns (ctx, tensors dict)."""
+    import torch
+    pos, nrm, vtx, idx = upload_scene(scene, device)
+    shadow = torch.empty(scene.S, dtype=torch.float32, device=device)
+    mk = torch.empty(scene.S * mask_words(scene.light.n), dtype=torch.int32, device=device) if masks else None
+    ctx = Context()
+    if debug:
+        ctx.set_debug(1)
+    ctx.set_view(scene.W, scene.H)
+    ctx.set_bin_num(scene.bins)
+    ctx.set_scenes_esp(scene.esp)
+    ctx.set_backface_cull(scene.cull)
+    ctx.add_model(vtx, scene.V, 16, idx, scene.T, scene.name)
+    ctx.set_sample_buffers(pos, nrm)
+    ctx.set_output_buffer(shadow, mk)
+    ctx.set_area_light(scene.light)
+    return ctx, dict(pos=pos, nrm=nrm, vtx=vtx, idx=idx, shadow=shadow, masks=mk)

@@ -1,0 +1,132 @@
+// fdzb_internal.h -- shared host/device definitions of the B200 FDZB pipeline.
+//
+// One launch processes a batch of frames (a single FD-style frame is a batch of
+// one).  Samples, triangles and light-plane bins of all frames are laid out back
+// to back in HBM, so the binning, sorting and occlusion stages run over one
+// global index space: global bin = frame.binBase + local bin, and the unbinned
+// key is the total bin count.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fdzb {
+
+constexpr float kF32Max = 3.402823466e+38f;   // FD_F32_MAX, FS/util/Util.h:59
+constexpr int kMaxLightN = 32;                 // U32 mask rows (K/Step5_2_shadowCalPerSample.inl:251)
+constexpr int kMaxBins = 512;                  // bins per side
+
+// Light block derived on the host (FS/api.cpp:303-400), device copy per frame.
+struct LightParams {
+    float mat[16];          // column-major upRight-corner projection
+    float RF[2];            // RectangleFactor
+    float ur[3], ul[3], dl[3], dr[3];  // light corners
+    float xd[3], yd[3];     // x_delt, y_delt
+    int N;                  // light grid side (lightResWidth == lightResHeight)
+    uint32_t full;          // N low bits set
+};
+
+// Per-frame inputs, outputs and batch offsets (host-filled).
+struct FrameDesc {
+    const float4 *pos;
+    const float4 *nrm;
+    const float *vtx;
+    const int32_t *idx;
+    float *shadow;
+    uint32_t *masks;        // nullable
+    int W, H, log2up;       // view; log2up = ceil(log2 W) (FS/api.cpp:209)
+    int V, vstride, T;      // vertices, floats per vertex, triangles
+    int Wb, log2Wb, numBins;
+    int cull;
+    float esp;
+    int maskWords;
+    int sampleBase, triBase, binBase;
+    int pad;
+    LightParams light;
+};
+
+// Slots of FrameState::acc (order-preserving uint32 encodings of floats).
+enum AccSlot {
+    ACC_SMAXW = 0,   // max light depth over non-background samples (k1)
+    ACC_TMAXW,       // max light depth over all vertices (k2)
+    ACC_S_MINU, ACC_S_MINV, ACC_S_MINW, ACC_S_MAXA, ACC_S_MAXB, ACC_S_MAXW,  // front samples (k3)
+    ACC_M_MINU, ACC_M_MINV, ACC_M_MINW, ACC_M_MAXA, ACC_M_MAXB, ACC_M_MAXW,  // vertices (k4)
+    ACC_COUNT
+};
+
+// Per-frame values computed on the device.
+struct FrameState {
+    uint32_t acc[ACC_COUNT];
+    int nFront;             // non-background front-facing samples
+    int state;              // 0 / 1 / 2 (see fdzb_frame_stats)
+    int nValidTris;
+    int nValidSamples;
+    float f, subx, suby;
+    float Bx, By, Bz, Ex, Ey, Ez;
+    float fx, fy;
+    float sampleAabb[6], modelAabb[6];
+    int quirkKeyRange;
+    int pad[3];
+};
+
+// Launch-wide counters and error word (zeroed every launch).
+struct Counters {
+    int pairCount;          // triangle/bin pairs produced
+    int pairOverflow;       // 1 if pairCount > capacity
+    int itemCount;          // occlusion work items
+    int itemCursor;         // occlusion work queue head
+    int triTileCounter;     // look-back scan tile ticket
+    int errorFlags;         // bit 0: look-back wait gave up, bit 1: mbarrier wait gave up
+    unsigned long long pairTests;
+    int sortTileCounter[8]; // one ticket per radix pass (4 sample + 4 pair)
+};
+
+enum ErrorBits { ERR_LOOKBACK_TIMEOUT = 1, ERR_MBAR_TIMEOUT = 2, ERR_BAD_INPUT = 4, ERR_INTERNAL = 8 };
+
+// Device buffers of one launch (carved from one arena).
+struct DeviceBuffers {
+    FrameDesc *frames;        // [nframes]
+    FrameState *states;       // [nframes]
+    Counters *counters;
+    int nframes;
+    int totalSamples, totalTris, totalBins;
+    int pairCapacity;
+    // samples
+    uint32_t *keysA, *valsA, *keysB, *valsB;   // [totalSamples]
+    int32_t *binSampleStart, *binSampleEnd;    // [totalBins + 1]
+    uint32_t *binStat;                          // [8 * totalBins] ordered encodings: maxz, Rx, Ry, Rz, Rw, 3 pad
+    // triangles
+    float4 *triRec;                             // [4 * totalTris]
+    int32_t *triCount;                          // [totalTris]
+    unsigned long long *triScanStatus;          // [triTiles] epoch-tagged look-back words
+    // pairs
+    uint32_t *pkeysA, *pvalsA, *pkeysB, *pvalsB;  // [pairCapacity]
+    int32_t *binTriStart, *binTriEnd;          // [totalBins]
+    // sort scratch
+    uint32_t *sortHist;                         // [8 * 256]: 4 sample passes, 4 pair passes
+    unsigned long long *sortStatus;             // [sortStatusTiles * 256] epoch-tagged
+    size_t sortStatusTiles;
+    int *sampleBases, *triBases, *binBases;     // [nframes] ascending global bases
+    // occlusion work list
+    int4 *items;                                // [itemCapacity]
+    int itemCapacity;
+    // sorted data lands in the A buffers after an even number of passes, B after odd
+    int samplePasses, pairPasses;
+    uint32_t epoch;                             // launch sequence number (look-back tags)
+    // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays
+    uint32_t *dbgKeys, *dbgVals, *dbgPKeys, *dbgPVals;
+};
+
+// Host side.
+void light_setup(const float rightRadius, const float topRadius, const float position[3],
+                 const float viewDir[3], const float upDir[3], int resW, int resH,
+                 LightParams *out);
+
+// Kernel drivers (fdzb_pipeline.cu).  All enqueue on `stream`, no host syncs.
+// maxS / maxT / maxV: largest per-frame sample / triangle / vertex counts.
+cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t stream);
+int sort_passes_for(long long keyRangeExclusive);
+cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t stream);
+constexpr int kSortTileHost = 4096;   // keys per radix-sort tile (fdzb_sort.cuh)
+constexpr int kTriTileHost = 256;     // triangles per pair-scan tile
+
+}  // namespace fdzb

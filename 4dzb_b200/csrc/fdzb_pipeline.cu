@@ -1,0 +1,954 @@
+// fdzb_pipeline.cu -- the B200 FDZB soft-shadow pipeline.
+//
+// Stage map (reference kernels in 4DZB/FDZB_Soft_Shadow/cuda/, "K/"):
+//   k_init        clears per-launch bin state
+//   k_reduce      k1+k2+k3+k4 fused: one pass over samples (pos+normal, 128-bit
+//                 loads) and vertices computes the far-plane depth maxima and the
+//                 sample / vertex rectangle bounds (K/Step2_1_*, K/Step2_2_*)
+//   k_plan        light plane, far plane f, sub-constant, bin factor
+//                 (K/Step2_3_defineFDbuffer.inl:5-111)
+//   k_tri_setup   per-triangle cull + footprint AABB + 64-byte record
+//                 (K/Step0_triangleSetup.inl:37-191)
+//   k_sample_keys bin key per sample, back-facing/unbinned outputs, per-bin
+//                 sample stats by warp-aggregated atomics (k6 + k9,
+//                 K/Step3_bindSampleToBin.inl:5-104)
+//   radix sort    sample pairs (k7) and triangle/bin pairs (k12), fdzb_sort.cuh
+//   k_tri_pairs   count + decoupled look-back scan + pair write in one pass
+//                 (k10 + exclusive_scan + k11, K/Step4_RasterizeTriangleToBin.inl)
+//   k_items       per-bin work items for the occlusion kernel
+//   k_occlusion   per-bin occlusion + popcount shading (k13,
+//                 K/Step5_2_shadowCalPerSample.inl:37-231): a warp owns 32 samples
+//                 of one bin; the bin's triangle records are staged into shared
+//                 memory 32 at a time and every lane walks them against its own
+//                 sample, OR-accumulating N-bit row masks.
+#include "fdzb_device.cuh"
+#include "fdzb_sort.cuh"
+
+namespace fdzb {
+
+// ---------------------------------------------------------------------------
+// k_init: empty bin statistics (K/Step3_bindSampleToBin.inl:83-84) and cleared
+// segment tables (K/binRaster.inl:39-40, 52-53).
+// ---------------------------------------------------------------------------
+__global__ void k_init(FrameState *states, int nframes, uint32_t *binStat, int32_t *bss,
+                       int32_t *bse, int32_t *bts, int32_t *bte, int totalBins)
+{
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    const uint32_t neg = f2o(-kF32Max), pos = f2o(kF32Max);
+    for (int b = gid; b < totalBins; b += stride) {
+        uint4 s0 = make_uint4(neg, neg, neg, pos);
+        uint4 s1 = make_uint4(pos, 0u, 0u, 0u);
+        reinterpret_cast<uint4 *>(binStat)[2 * b] = s0;
+        reinterpret_cast<uint4 *>(binStat)[2 * b + 1] = s1;
+        bts[b] = 0;
+        bte[b] = 0;
+    }
+    for (int b = gid; b <= totalBins; b += stride) {
+        bss[b] = 0;
+        bse[b] = 0;
+    }
+    for (int f = gid; f < nframes; f += stride) {
+        FrameState &s = states[f];
+        s.acc[ACC_SMAXW] = f2o(-1.0f);  // thrust::reduce init value (K/Step2_1_*.inl:43)
+        s.acc[ACC_TMAXW] = f2o(-1.0f);  // (K/Step2_2_*.inl:40)
+        s.acc[ACC_S_MINU] = pos; s.acc[ACC_S_MINV] = pos; s.acc[ACC_S_MINW] = pos;
+        s.acc[ACC_S_MAXA] = neg; s.acc[ACC_S_MAXB] = neg; s.acc[ACC_S_MAXW] = neg;
+        s.acc[ACC_M_MINU] = pos; s.acc[ACC_M_MINV] = pos; s.acc[ACC_M_MINW] = pos;
+        s.acc[ACC_M_MAXA] = neg; s.acc[ACC_M_MAXB] = neg; s.acc[ACC_M_MAXW] = neg;
+        s.nFront = 0;
+        s.state = 0;
+        s.nValidTris = 0;
+        s.nValidSamples = 0;
+        s.quirkKeyRange = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_reduce: grid (x, frame, 2): z = 0 samples, z = 1 vertices.
+// Sample part: k1 (max depth over non-background samples) and k3's bounds over
+// front-facing samples.  The bound on rect.x + RF.x/w - sub is reduced before
+// the subtraction (sub = RF/f needs f first): fl(x - sub) is monotone in x, so
+// max_i fl(a_i - sub) == fl(max_i a_i - sub) exactly.
+// Vertex part: k2 (max depth) and k4 (vertex rectangle bounds).
+// ---------------------------------------------------------------------------
+constexpr int kReduceThreads = 256;
+
+__device__ __forceinline__ void acc_max(uint32_t &a, float v)
+{
+    if (!isnan(v)) a = max(a, f2o(v));
+}
+__device__ __forceinline__ void acc_min(uint32_t &a, float v)
+{
+    if (!isnan(v)) a = min(a, f2o(v));
+}
+
+__global__ void __launch_bounds__(kReduceThreads)
+    k_reduce(const FrameDesc *__restrict__ frames, FrameState *states)
+{
+    const FrameDesc &fr = frames[blockIdx.y];
+    FrameState &st = states[blockIdx.y];
+    const float *M = fr.light.mat;
+    const float RFx = fr.light.RF[0], RFy = fr.light.RF[1];
+    __shared__ uint32_t s_acc[kReduceThreads / 32][8];
+    __shared__ int s_cnt[kReduceThreads / 32];
+
+    // slot layout in a[]: 0 max depth, 1 min u, 2 min v, 3 min w, 4 max a, 5 max b, 6 max w
+    uint32_t a[7] = {0u, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    int cnt = 0;
+    const int stride = gridDim.x * blockDim.x;
+    if (blockIdx.z == 0) {
+        const int S = fr.W * fr.H;
+        const f3 ur = ld3(fr.light.ur), ul = ld3(fr.light.ul), dl = ld3(fr.light.dl),
+                 dr = ld3(fr.light.dr);
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S; p += stride) {
+            const float4 P = __ldg(fr.pos + p);
+            if (isnan(P.x)) continue;
+            const f3 q = mk3(P.x, P.y, P.z);
+            acc_max(a[0], light_depth(M, q));
+            const float4 Nv = __ldg(fr.nrm + p);
+            const f3 n = mk3(Nv.x, Nv.y, Nv.z);
+            const bool back = dot3(sub3(ur, q), n) <= 0.0f && dot3(sub3(ul, q), n) <= 0.0f &&
+                              dot3(sub3(dl, q), n) <= 0.0f && dot3(sub3(dr, q), n) <= 0.0f;
+            if (back) continue;
+            ++cnt;
+            const f3 r = light_project(M, q);
+            acc_min(a[1], r.x);
+            acc_min(a[2], r.y);
+            acc_min(a[3], r.z);
+            acc_max(a[4], __fadd_rn(r.x, __fdiv_rn(RFx, r.z)));
+            acc_max(a[5], __fadd_rn(r.y, __fdiv_rn(RFy, r.z)));
+            acc_max(a[6], r.z);
+        }
+    } else {
+        for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < fr.V; v += stride) {
+            const f3 q = ld3(fr.vtx + (size_t)v * fr.vstride);
+            acc_max(a[0], light_depth(M, q));
+            const f3 r = light_project(M, q);
+            acc_min(a[1], r.x);
+            acc_min(a[2], r.y);
+            acc_min(a[3], r.z);
+            acc_max(a[4], __fadd_rn(r.x, __fdiv_rn(RFx, r.z)));
+            acc_max(a[5], __fadd_rn(r.y, __fdiv_rn(RFy, r.z)));
+            acc_max(a[6], r.z);
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t w[7];
+    w[0] = __reduce_max_sync(kFullWarp, a[0]);
+    w[1] = __reduce_min_sync(kFullWarp, a[1]);
+    w[2] = __reduce_min_sync(kFullWarp, a[2]);
+    w[3] = __reduce_min_sync(kFullWarp, a[3]);
+    w[4] = __reduce_max_sync(kFullWarp, a[4]);
+    w[5] = __reduce_max_sync(kFullWarp, a[5]);
+    w[6] = __reduce_max_sync(kFullWarp, a[6]);
+    const int c = __reduce_add_sync(kFullWarp, cnt);
+    if (lane == 0) {
+        for (int i = 0; i < 7; ++i) s_acc[warp][i] = w[i];
+        s_cnt[warp] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        const int i = threadIdx.x;
+        if (i < 7) {
+            uint32_t r = s_acc[0][i];
+            const bool isMin = (i >= 1 && i <= 3);
+            for (int k = 1; k < kReduceThreads / 32; ++k)
+                r = isMin ? min(r, s_acc[k][i]) : max(r, s_acc[k][i]);
+            const bool vert = blockIdx.z == 1;
+            int slot;
+            if (i == 0) slot = vert ? ACC_TMAXW : ACC_SMAXW;
+            else slot = (vert ? ACC_M_MINU : ACC_S_MINU) + (i - 1);
+            if (isMin) {
+                if (r != 0xffffffffu) atomicMin(&st.acc[slot], r);
+            } else {
+                if (r != 0u) atomicMax(&st.acc[slot], r);
+            }
+        } else if (blockIdx.z == 0) {
+            int t = 0;
+            for (int k = 0; k < kReduceThreads / 32; ++k) t += s_cnt[k];
+            if (t) atomicAdd(&st.nFront, t);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_plan: one thread per frame; host logic of lightPlaneParamCal
+// (K/Step2_3_defineFDbuffer.inl:14-104) with the early exits as frame states.
+// ---------------------------------------------------------------------------
+__global__ void k_plan(const FrameDesc *__restrict__ frames, FrameState *states, int nframes)
+{
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= nframes) return;
+    const FrameDesc &fr = frames[fi];
+    FrameState &st = states[fi];
+    const float smax = o2f(st.acc[ACC_SMAXW]);
+    const float tmax = o2f(st.acc[ACC_TMAXW]);
+    st.state = 0;
+    if (smax < 0.0f || tmax < 0.0f) return;
+    const float f = __fadd_rn(fmaxf(smax, tmax), 0.1f);
+    const float subx = __fdiv_rn(fr.light.RF[0], f), suby = __fdiv_rn(fr.light.RF[1], f);
+    st.f = f;
+    st.subx = subx;
+    st.suby = suby;
+    st.state = 1;
+    float s[6], m[6];
+    s[0] = o2f(st.acc[ACC_S_MINU]);
+    s[1] = o2f(st.acc[ACC_S_MINV]);
+    s[2] = o2f(st.acc[ACC_S_MINW]);
+    s[3] = st.nFront ? __fsub_rn(o2f(st.acc[ACC_S_MAXA]), subx) : -kF32Max;
+    s[4] = st.nFront ? __fsub_rn(o2f(st.acc[ACC_S_MAXB]), suby) : -kF32Max;
+    s[5] = o2f(st.acc[ACC_S_MAXW]);
+    m[0] = o2f(st.acc[ACC_M_MINU]);
+    m[1] = o2f(st.acc[ACC_M_MINV]);
+    m[2] = o2f(st.acc[ACC_M_MINW]);
+    m[3] = fr.V ? __fsub_rn(o2f(st.acc[ACC_M_MAXA]), subx) : -kF32Max;
+    m[4] = fr.V ? __fsub_rn(o2f(st.acc[ACC_M_MAXB]), suby) : -kF32Max;
+    m[5] = o2f(st.acc[ACC_M_MAXW]);
+    for (int i = 0; i < 6; ++i) {
+        st.sampleAabb[i] = s[i];
+        st.modelAabb[i] = m[i];
+    }
+    if (st.nFront == 0) return;  // K/Step2_1_samplerRectangleAABB.inl:178-181
+    if (m[0] > m[3] || m[1] > m[4] || s[0] > s[3] || s[1] > s[4]) return;
+    st.Bx = fmaxf(s[0], m[0]);
+    st.By = fmaxf(s[1], m[1]);
+    st.Ex = fminf(s[3], m[3]);
+    st.Ey = fminf(s[4], m[4]);
+    st.Bz = m[2];
+    st.Ez = s[5];
+    if (st.Bx >= st.Ex || st.By >= st.Ey) return;
+    st.fx = __fdiv_rn((float)fr.Wb, __fsub_rn(st.Ex, st.Bx));
+    st.fy = __fdiv_rn((float)fr.Wb, __fsub_rn(st.Ey, st.By));
+    st.state = 2;
+}
+
+// ---------------------------------------------------------------------------
+// k_tri_setup: grid (x, frame).  Record layout (4 x float4 = 64 B):
+//   q0 = (v0, minz) q1 = (v1, maxz) q2 = (v2, 0) q3 = (aabb min x,y, aabb max x,y)
+// Culled triangles keep the inverted AABB of the reference's triAABB buffer, so
+// the pair counter's skip test rejects them exactly as K/Step4_*.inl:41 does.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_tri_setup(const FrameDesc *__restrict__ frames, FrameState *states, float4 *__restrict__ rec,
+                int *err)
+{
+    const FrameDesc &fr = frames[blockIdx.y];
+    FrameState &st = states[blockIdx.y];
+    if (st.state < 2) return;
+    const float *M = fr.light.mat;
+    const float RFx = fr.light.RF[0], RFy = fr.light.RF[1];
+    const float subx = st.subx, suby = st.suby;
+    const float Bx = st.Bx, By = st.By, Ex = st.Ex, Ey = st.Ey;
+    const f3 ur = ld3(fr.light.ur), ul = ld3(fr.light.ul), dl = ld3(fr.light.dl),
+             dr = ld3(fr.light.dr);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < fr.T; base += stride) {
+        const int t = base + lane;
+        bool inLP = false;
+        if (t < fr.T) {
+            const int i0 = fr.idx[3 * (size_t)t], i1 = fr.idx[3 * (size_t)t + 1],
+                      i2 = fr.idx[3 * (size_t)t + 2];
+            float mnx = kF32Max, mny = kF32Max, mnz = kF32Max;
+            float mxx = -kF32Max, mxy = -kF32Max, mxz = -kF32Max;
+            f3 v0 = mk3(0.f, 0.f, 0.f), v1 = v0, v2 = v0;
+            const bool okIdx = i0 >= 0 && i0 < fr.V && i1 >= 0 && i1 < fr.V && i2 >= 0 && i2 < fr.V;
+            if (!okIdx) {
+                atomicOr(err, (int)ERR_BAD_INPUT);
+            } else {
+                v0 = ld3(fr.vtx + (size_t)i0 * fr.vstride);
+                v1 = ld3(fr.vtx + (size_t)i1 * fr.vstride);
+                v2 = ld3(fr.vtx + (size_t)i2 * fr.vstride);
+                const f3 n = cross3(sub3(v0, v2), sub3(v1, v0));
+                const bool culled =
+                    fr.cull && dot3(n, sub3(ur, v0)) <= 0.0f && dot3(n, sub3(ur, v1)) <= 0.0f &&
+                    dot3(n, sub3(ur, v2)) <= 0.0f && dot3(n, sub3(ul, v0)) <= 0.0f &&
+                    dot3(n, sub3(ul, v1)) <= 0.0f && dot3(n, sub3(ul, v2)) <= 0.0f &&
+                    dot3(n, sub3(dr, v0)) <= 0.0f && dot3(n, sub3(dr, v1)) <= 0.0f &&
+                    dot3(n, sub3(dr, v2)) <= 0.0f && dot3(n, sub3(dl, v0)) <= 0.0f &&
+                    dot3(n, sub3(dl, v1)) <= 0.0f && dot3(n, sub3(dl, v2)) <= 0.0f;
+                if (!culled) {
+                    const f3 vv[3] = {v0, v1, v2};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const f3 r = light_project(M, vv[k]);
+                        mnx = fminf(mnx, r.x);
+                        mny = fminf(mny, r.y);
+                        mnz = fminf(mnz, r.z);
+                        mxz = fmaxf(mxz, r.z);
+                        mxx = fmaxf(mxx, __fsub_rn(__fadd_rn(r.x, __fdiv_rn(RFx, r.z)), subx));
+                        mxy = fmaxf(mxy, __fsub_rn(__fadd_rn(r.y, __fdiv_rn(RFy, r.z)), suby));
+                    }
+                    inLP = !(mnx > Ex || mny > Ey || mxx < Bx || mxy < By);
+                }
+            }
+            float4 *o = rec + 4 * (size_t)(fr.triBase + t);
+            o[0] = make_float4(v0.x, v0.y, v0.z, mnz);
+            o[1] = make_float4(v1.x, v1.y, v1.z, mxz);
+            o[2] = make_float4(v2.x, v2.y, v2.z, 0.0f);
+            o[3] = make_float4(mnx, mny, mxx, mxy);
+        }
+        const unsigned b = __ballot_sync(kFullWarp, inLP);
+        if (lane == 0 && b) atomicAdd(&st.nValidTris, __popc(b));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_sample_keys: grid (x, frame).  k3's back-face/validity decision and
+// rectangle, k6's key (K/Step3_bindSampleToBin.inl:29-57) and k9's per-bin
+// statistics (max w, max rect.min x/y, min rect.max x/y; :61-104) by
+// warp-aggregated atomics on order-preserving encodings.  Samples that get no
+// bin receive their final output here: 1 (full mask) if back-facing, else 0.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_sample_keys(const FrameDesc *__restrict__ frames, FrameState *states, uint32_t *__restrict__ keys,
+                  uint32_t *__restrict__ vals, uint32_t *binStat, int invalidKey)
+{
+    const FrameDesc &fr = frames[blockIdx.y];
+    FrameState &st = states[blockIdx.y];
+    const int state = st.state;
+    const bool binning = state == 2 && st.nValidTris > 0;
+    const float *M = fr.light.mat;
+    const float RFx = fr.light.RF[0], RFy = fr.light.RF[1];
+    const float subx = st.subx, suby = st.suby;
+    const float Bx = st.Bx, By = st.By, Ex = st.Ex, Ey = st.Ey, fx = st.fx, fy = st.fy;
+    const f3 ur = ld3(fr.light.ur), ul = ld3(fr.light.ul), dl = ld3(fr.light.dl),
+             dr = ld3(fr.light.dr);
+    const int S = fr.W * fr.H;
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    const int words = fr.maskWords;
+    const int NN = fr.light.N * fr.light.N;
+    int nvalid = 0, nquirk = 0;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < S; base += stride) {
+        const int p = base + lane;
+        const bool in = p < S;
+        bool valid = false, back = false;
+        uint32_t key = (uint32_t)invalidKey;
+        float w = 0.f, bx0 = 0.f, by0 = 0.f, ex0 = 0.f, ey0 = 0.f;
+        if (in && state >= 1) {
+            const float4 P = __ldg(fr.pos + p);
+            if (!isnan(P.x)) {
+                const float4 Nv = __ldg(fr.nrm + p);
+                const f3 q = mk3(P.x, P.y, P.z), n = mk3(Nv.x, Nv.y, Nv.z);
+                back = dot3(sub3(ur, q), n) <= 0.0f && dot3(sub3(ul, q), n) <= 0.0f &&
+                       dot3(sub3(dl, q), n) <= 0.0f && dot3(sub3(dr, q), n) <= 0.0f;
+                if (!back && binning) {
+                    const f3 r = light_project(M, q);
+                    bx0 = r.x;
+                    by0 = r.y;
+                    ex0 = __fsub_rn(__fadd_rn(r.x, __fdiv_rn(RFx, r.z)), subx);
+                    ey0 = __fsub_rn(__fadd_rn(r.y, __fdiv_rn(RFy, r.z)), suby);
+                    w = r.z;
+                    if (!((bx0 > ex0 || by0 > ey0) || (bx0 < Bx || by0 < By || ex0 > Ex || ey0 > Ey))) {
+                        const float cx = __fdiv_rn(__fadd_rn(ex0, bx0), 2.0f);
+                        const float cy = __fdiv_rn(__fadd_rn(ey0, by0), 2.0f);
+                        const int bxi = __float2int_rz(floorf(__fmul_rn(__fsub_rn(cx, Bx), fx)));
+                        const int byi = __float2int_rz(floorf(__fmul_rn(__fsub_rn(cy, By), fy)));
+                        if (bxi >= 0 && bxi < fr.Wb && byi >= 0 && byi < fr.Wb) {
+                            key = (uint32_t)(fr.binBase + ((byi << fr.log2Wb) | bxi));
+                            valid = true;
+                        } else {
+                            ++nquirk;
+                        }
+                    }
+                }
+            }
+        }
+        if (in) {
+            keys[fr.sampleBase + p] = key;
+            vals[fr.sampleBase + p] = (uint32_t)(fr.sampleBase + p);
+            if (!valid) {
+                fr.shadow[p] = back ? 1.0f : 0.0f;
+                if (fr.masks) {
+                    uint32_t *mo = fr.masks + (size_t)p * words;
+                    for (int wi = 0; wi < words; ++wi) {
+                        uint32_t v = 0u;
+                        if (back) {
+                            const int rem = NN - 32 * wi;
+                            v = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+                        }
+                        mo[wi] = v;
+                    }
+                }
+            }
+        }
+        // per-bin statistics, one atomic per distinct key per warp
+        unsigned todo = __ballot_sync(kFullWarp, valid);
+        nvalid += valid ? 1 : 0;
+        while (todo) {
+            const int leader = __ffs(todo) - 1;
+            const uint32_t lk = __shfl_sync(kFullWarp, key, leader);
+            const bool mine = valid && key == lk;
+            const unsigned grp = __ballot_sync(kFullWarp, mine);
+            const uint32_t mz = __reduce_max_sync(kFullWarp, mine ? f2o(w) : 0u);
+            const uint32_t rx = __reduce_max_sync(kFullWarp, mine ? f2o(bx0) : 0u);
+            const uint32_t ry = __reduce_max_sync(kFullWarp, mine ? f2o(by0) : 0u);
+            const uint32_t rz = __reduce_min_sync(kFullWarp, mine ? f2o(ex0) : 0xffffffffu);
+            const uint32_t rw = __reduce_min_sync(kFullWarp, mine ? f2o(ey0) : 0xffffffffu);
+            if (lane == leader) {
+                uint32_t *s = binStat + 8 * (size_t)lk;
+                atomicMax(s + 0, mz);
+                atomicMax(s + 1, rx);
+                atomicMax(s + 2, ry);
+                atomicMin(s + 3, rz);
+                atomicMin(s + 4, rw);
+            }
+            todo &= ~grp;
+        }
+    }
+    nvalid = __reduce_add_sync(kFullWarp, nvalid);
+    nquirk = __reduce_add_sync(kFullWarp, nquirk);
+    if (lane == 0) {
+        if (nvalid) atomicAdd(&st.nValidSamples, nvalid);
+        if (nquirk) atomicAdd(&st.quirkKeyRange, nquirk);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_tri_pairs: persistent tiles of 256 triangles.  For each triangle, the
+// candidate bins of its light-plane-clamped AABB are tested against the bin
+// statistics (strict comparisons, K/Step4_RasterizeTriangleToBin.inl:74-103);
+// the tile's pair count is scanned, the tile's global offset found by a
+// decoupled look-back over previous tiles, and the (bin, triangle) pairs are
+// written in triangle order, bins row-major -- the reference's layout
+// (:184-202) with the counting predicate used for both passes.
+// ---------------------------------------------------------------------------
+constexpr int kTriThreads = 256;
+// Look-back status word of a triangle tile: [63:32] launch epoch, [31:30] flag,
+// [29:0] pair count (the pair capacity stays below 2^30).
+constexpr unsigned long long kScanAgg = 1ull << 30;
+constexpr unsigned long long kScanPrefix = 2ull << 30;
+constexpr unsigned long long kScanMask = (1ull << 30) - 1ull;
+
+struct TriBins {
+    int cbx, cby, cex, cey;
+    float bx, by, bz, ex, ey;
+    bool any;
+};
+
+__device__ __forceinline__ TriBins tri_candidates(const float4 q0, const float4 q1, const float4 q3,
+                                                  const FrameState &st, int Wb)
+{
+    TriBins r;
+    r.any = false;
+    float bx = q3.x, by = q3.y, bz = q0.w, ex = q3.z, ey = q3.w, ez = q1.w;
+    if (bx > ex || by > ey || bz > ez || bx > st.Ex || by > st.Ey || ex < st.Bx || ey < st.By)
+        return r;
+    bx = fmaxf(bx, st.Bx);
+    by = fmaxf(by, st.By);
+    ex = fminf(ex, st.Ex);
+    ey = fminf(ey, st.Ey);
+    // float -> ushort conversions of the reference saturate to [0, 65535]
+    const float fbx = fmaxf(floorf(__fmul_rn(__fsub_rn(bx, st.Bx), st.fx)), 0.0f);
+    const float fby = fmaxf(floorf(__fmul_rn(__fsub_rn(by, st.By), st.fy)), 0.0f);
+    const float fex = fminf(ceilf(__fmul_rn(__fsub_rn(ex, st.Bx), st.fx)), (float)Wb);
+    const float fey = fminf(ceilf(__fmul_rn(__fsub_rn(ey, st.By), st.fy)), (float)Wb);
+    r.cbx = (int)__float2uint_rz(fminf(fbx, 65535.0f));
+    r.cby = (int)__float2uint_rz(fminf(fby, 65535.0f));
+    r.cex = (int)__float2uint_rz(fmaxf(fex, 0.0f));
+    r.cey = (int)__float2uint_rz(fmaxf(fey, 0.0f));
+    r.bx = bx; r.by = by; r.bz = bz; r.ex = ex; r.ey = ey;
+    r.any = true;
+    return r;
+}
+
+__device__ __forceinline__ bool bin_accepts(const uint32_t *binStat, int gbin, const TriBins &c)
+{
+    const uint4 s = __ldg(reinterpret_cast<const uint4 *>(binStat) + 2 * (size_t)gbin);
+    const uint32_t s4 = __ldg(binStat + 8 * (size_t)gbin + 4);
+    const float maxz = o2f(s.x), Rx = o2f(s.y), Ry = o2f(s.z), Rz = o2f(s.w), Rw = o2f(s4);
+    return maxz >= c.bz && c.bx < Rx && c.by < Ry && Rz < c.ex && Rw < c.ey;
+}
+
+__global__ void __launch_bounds__(kTriThreads)
+    k_tri_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
+                const int *__restrict__ triBases, int nframes, int totalTris,
+                const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
+                int32_t *__restrict__ triCount, unsigned long long *scanStatus, uint32_t epoch,
+                uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
+                Counters *ctr)
+{
+    constexpr int WARPS = kTriThreads / 32;
+    __shared__ int s_tile;
+    __shared__ unsigned long long s_wsum[WARPS];
+    __shared__ unsigned long long s_excl;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ntiles = (totalTris + kTriThreads - 1) / kTriThreads;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_tile = atomicAdd(&ctr->triTileCounter, 1);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        const int g = tile * kTriThreads + tid;
+        TriBins c;
+        c.any = false;
+        int fi = 0, cnt = 0;
+        if (g < totalTris) {
+            fi = frame_of(triBases, nframes, g);
+            const FrameState &st = states[fi];
+            if (st.state == 2 && st.nValidTris > 0) {
+                const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
+                             q3 = __ldg(rec + 4 * (size_t)g + 3);
+                c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
+                if (c.any) {
+                    const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
+                    for (int j = c.cby; j < c.cey; ++j)
+                        for (int i = c.cbx; i < c.cex; ++i)
+                            cnt += bin_accepts(binStat, bb + ((j << l2) | i), c) ? 1 : 0;
+                }
+            }
+            triCount[g] = cnt;
+        }
+        // block inclusive scan of cnt
+        unsigned long long x = (unsigned long long)cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long y = __shfl_up_sync(kFullWarp, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();
+        unsigned long long wbase = 0, total = 0;
+        for (int w = 0; w < WARPS; ++w) {
+            if (w < warp) wbase += s_wsum[w];
+            total += s_wsum[w];
+        }
+        const unsigned long long mine_excl = wbase + x - (unsigned long long)cnt;
+        if (tid == 0) {
+            unsigned long long excl = 0;
+            unsigned long long *my = scanStatus + tile;
+            const unsigned long long ep = (unsigned long long)epoch << 32;
+            const unsigned long long tot = total > kScanMask ? kScanMask : total;
+            if (tile == 0) {
+                st_volatile_u64(my, ep | kScanPrefix | tot);
+            } else {
+                st_volatile_u64(my, ep | kScanAgg | tot);
+                int t = tile - 1;
+                unsigned spins = 0;
+                while (t >= 0) {
+                    const unsigned long long s = ld_volatile_u64(scanStatus + t);
+                    const unsigned long long flag = ((s >> 32) == epoch) ? (s & 0xC0000000ull) : 0ull;
+                    if (flag == 0) {
+                        if (++spins > kSpinLimit) {
+                            atomicOr(&ctr->errorFlags, (int)ERR_LOOKBACK_TIMEOUT);
+                            break;
+                        }
+                        continue;
+                    }
+                    excl += s & kScanMask;
+                    if (flag == kScanPrefix) break;
+                    --t;
+                }
+                const unsigned long long inc = excl + total > kScanMask ? kScanMask : excl + total;
+                st_volatile_u64(my, ep | kScanPrefix | inc);
+            }
+            s_excl = excl;
+            if (tile == ntiles - 1) {
+                const unsigned long long all = excl + total;
+                ctr->pairCount = (int)(all > 0x7fffffffull ? 0x7fffffffull : all);
+                if (all > (unsigned long long)capacity) ctr->pairOverflow = 1;
+            }
+        }
+        __syncthreads();
+        if (cnt > 0) {
+            unsigned long long pos = s_excl + mine_excl;
+            const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
+            for (int j = c.cby; j < c.cey; ++j)
+                for (int i = c.cbx; i < c.cex; ++i) {
+                    const int gb = bb + ((j << l2) | i);
+                    if (bin_accepts(binStat, gb, c)) {
+                        if (pos < (unsigned long long)capacity) {
+                            pkeys[pos] = (uint32_t)gb;
+                            pvals[pos] = (uint32_t)g;
+                        }
+                        ++pos;
+                    }
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_items: one thread per bin; a bin with n samples yields ceil(n/32) warp items.
+// ---------------------------------------------------------------------------
+__global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
+                        const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
+                        const int *__restrict__ binBases, int nframes, int totalBins,
+                        int4 *__restrict__ items, int capacity, Counters *ctr)
+{
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < totalBins;
+         base += gridDim.x * blockDim.x) {
+        const int b = base + lane;
+        int n = 0;
+        if (b < totalBins) n = (bse[b] - bss[b] + 31) >> 5;
+        int x = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFullWarp, x, o);
+            if (lane >= o) x += y;
+        }
+        const int tot = __shfl_sync(kFullWarp, x, 31);
+        int wbase = 0;
+        if (lane == 0 && tot) wbase = atomicAdd(&ctr->itemCount, tot);
+        wbase = __shfl_sync(kFullWarp, wbase, 0);
+        if (n) {
+            const int f = frame_of(binBases, nframes, b);
+            const int hasTris = bte[b] > bts[b] ? 1 : 0;
+            for (int k = 0; k < n; ++k) {
+                const int slot = wbase + x - n + k;
+                if (slot < capacity) items[slot] = make_int4(b, 32 * k, f, hasTris);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Occlusion.  Per sample/triangle pair, exactly the reference arithmetic of
+// K/Step5_2_shadowCalPerSample.inl:120-222.  A, B, C are formed with the
+// unflipped light vectors and negated when dir < 0: with round-to-nearest,
+// dot(n, -t) == -dot(n, t) except for the sign of an exact zero, which no later
+// comparison, product or sum can observe.
+// ---------------------------------------------------------------------------
+
+// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(N-1) precomputed (same
+// product) and the result limited to the N-bit light grid.
+__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full)
+{
+    const bool f1 = D >= 0.0f;
+    const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
+    if (f1 && f2) return full;
+    if (!f1 && !f2) return 0u;
+    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
+    const int k = __float2int_rz(ceilf(q));
+    uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
+    m -= 1u;
+    if (!f1) m = ~m;
+    return m & full;
+}
+
+// K/Step5_2_shadowCal.inl:213-222
+__device__ __forceinline__ bool point_in_tri(f3 A, f3 B, f3 C, f3 P)
+{
+    const f3 N1 = cross3(sub3(B, A), sub3(P, B));
+    const f3 N2 = cross3(sub3(C, B), sub3(P, C));
+    if (dot3(N1, N2) < 0.0f) return false;
+    const f3 N3 = cross3(sub3(A, C), sub3(P, A));
+    if (dot3(N2, N3) < 0.0f) return false;
+    return true;
+}
+
+constexpr int kOccWarps = 4;
+constexpr int kOccThreads = kOccWarps * 32;
+
+__global__ void __launch_bounds__(kOccThreads)
+    k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
+                const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
+                const uint32_t *__restrict__ sortedVals,
+                const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
+                const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
+                const uint32_t *__restrict__ pairTri, const float4 *__restrict__ rec, int totalTris,
+                int totalBins, int nframes)
+{
+    __shared__ float4 s_tri[kOccWarps][32][4];
+    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t(*rows)[32] = s_rows[warp];
+    unsigned long long tested = 0;
+    int nitems = *(volatile const int *)&ctr->itemCount;
+    if (nitems > itemCapacity) nitems = itemCapacity;
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(&ctr->itemCursor, 1);
+        it = __shfl_sync(kFullWarp, it, 0);
+        if (it >= nitems) break;
+        const int4 item = items[it];
+        const int bin = item.x, fi = item.z;
+        if ((unsigned)bin >= (unsigned)totalBins || (unsigned)fi >= (unsigned)nframes) {
+            if (lane == 0) atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+            continue;
+        }
+        const FrameDesc &fr = frames[fi];
+        const FrameState &st = states[fi];
+        const int N = fr.light.N;
+        const uint32_t FULL = fr.light.full;
+        const float nm1 = (float)(N - 1);
+        const int sLo = bss[bin] + item.y;
+        const int sHi = min(sLo + 32, bse[bin]);
+        const int k = sLo + lane;
+        const bool active = k < sHi;
+
+        f3 Q = mk3(0.f, 0.f, 0.f);
+        float spx = 0.f, spy = 0.f, spz = 0.f, spw = 0.f, spZ = 0.f;
+        int local = 0;
+        if (active) {
+            local = (int)sortedVals[k] - fr.sampleBase;
+            if ((unsigned)local >= (unsigned)(fr.W * fr.H)) {
+                atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                local = 0;
+            }
+            const float4 P = __ldg(fr.pos + local);
+            Q = mk3(P.x, P.y, P.z);
+            const f3 r = light_project(fr.light.mat, Q);
+            spx = r.x;
+            spy = r.y;
+            spz = __fsub_rn(__fadd_rn(r.x, __fdiv_rn(fr.light.RF[0], r.z)), st.subx);
+            spw = __fsub_rn(__fadd_rn(r.y, __fdiv_rn(fr.light.RF[1], r.z)), st.suby);
+            spZ = r.z;
+        }
+        for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+        uint32_t fullRows = 0u;
+        bool done = !active;
+
+        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd);
+        const f3 L0Q = sub3(ld3(fr.light.ur), Q);
+        const float esp = fr.esp;
+        const int tS = bts[bin], tE = bte[bin];
+        for (int c = tS; c < tE; c += 32) {
+            if (__all_sync(kFullWarp, done)) break;
+            const int m = min(32, tE - c);
+            __syncwarp();
+            if (lane < m) {
+                int tri = (int)pairTri[c + lane];
+                if ((unsigned)tri >= (unsigned)totalTris) {
+                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                    tri = 0;
+                }
+                const float4 *rp = rec + 4 * (size_t)tri;
+                s_tri[warp][lane][0] = __ldg(rp);
+                s_tri[warp][lane][1] = __ldg(rp + 1);
+                s_tri[warp][lane][2] = __ldg(rp + 2);
+                s_tri[warp][lane][3] = __ldg(rp + 3);
+            }
+            __syncwarp();
+            for (int t = 0; t < m; ++t) {
+                if (done) continue;
+                const float4 q3 = s_tri[warp][t][3];
+                const float4 q0 = s_tri[warp][t][0];
+                if (!(q3.x <= spx && q3.y <= spy && spz <= q3.z && spw <= q3.w && q0.w <= spZ))
+                    continue;
+                ++tested;
+                const float4 q1 = s_tri[warp][t][1];
+                const float4 q2 = s_tri[warp][t][2];
+                const f3 v0 = mk3(q0.x, q0.y, q0.z), v1 = mk3(q1.x, q1.y, q1.z),
+                         v2 = mk3(q2.x, q2.y, q2.z);
+                const f3 n = cross3(sub3(v1, v0), sub3(v2, v1));
+                const float dir = dot3(sub3(Q, v0), n);
+                if (fabsf(dir) < esp && point_in_tri(v0, v1, v2, Q)) continue;
+                const f3 n0 = cross3(sub3(v1, Q), sub3(v0, v1));
+                const f3 n1 = cross3(sub3(v2, Q), sub3(v1, v2));
+                const f3 n2 = cross3(sub3(v0, Q), sub3(v2, v0));
+                float A0 = dot3(n0, xd), B0 = dot3(n0, yd), C0 = dot3(n0, L0Q);
+                float A1 = dot3(n1, xd), B1 = dot3(n1, yd), C1 = dot3(n1, L0Q);
+                float A2 = dot3(n2, xd), B2 = dot3(n2, yd), C2 = dot3(n2, L0Q);
+                if (dir < 0.0f) {
+                    A0 = -A0; B0 = -B0; C0 = -C0;
+                    A1 = -A1; B1 = -B1; C1 = -C1;
+                    A2 = -A2; B2 = -B2; C2 = -C2;
+                }
+                const float An0 = __fmul_rn(A0, nm1), An1 = __fmul_rn(A1, nm1), An2 = __fmul_rn(A2, nm1);
+                const float Bn0 = __fmul_rn(B0, nm1), Bn1 = __fmul_rn(B1, nm1), Bn2 = __fmul_rn(B2, nm1);
+                const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL);
+                const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL);
+                const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL);
+                uint32_t vr = N0 & N1 & N2 & ~fullRows;
+                while (vr) {
+                    const int r = __ffs(vr) - 1;
+                    vr &= vr - 1u;
+                    const float fr_ = (float)r;
+                    const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr_), C0), Bn0, B0, FULL);
+                    const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr_), C1), Bn1, B1, FULL);
+                    const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr_), C2), Bn2, B2, FULL);
+                    const uint32_t nv = rows[r][lane] | (M0 & M1 & M2);
+                    rows[r][lane] = nv;
+                    if (nv == FULL) fullRows |= 1u << r;
+                }
+                if (fullRows == FULL) done = true;
+            }
+        }
+        if (active) {
+            int cnt = 0;
+            for (int r = 0; r < N; ++r) cnt += __popc(rows[r][lane]);
+            fr.shadow[local] = __fdiv_rn((float)cnt, (float)(N * N));
+            if (fr.masks) {
+                uint32_t *mo = fr.masks + (size_t)local * fr.maskWords;
+                uint32_t acc = 0u;
+                int bit = 0, wi = 0;
+                for (int r = 0; r < N; ++r) {
+                    const uint32_t v = rows[r][lane];
+                    acc |= v << bit;
+                    const int nb = bit + N;
+                    if (nb >= 32) {
+                        mo[wi++] = acc;
+                        acc = (nb > 32) ? (v >> (32 - bit)) : 0u;
+                        bit = nb - 32;
+                    } else {
+                        bit = nb;
+                    }
+                }
+                if (bit > 0) mo[wi] = acc;
+            }
+        }
+    }
+    unsigned long long t = tested;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFullWarp, t, o);
+    if (lane == 0 && t) atomicAdd(&ctr->pairTests, t);
+}
+
+// ---------------------------------------------------------------------------
+// k_move_model: FD::moveModel (K/moveModel.inl:6-30): xyz <- M * (xyz, 1) in
+// place, each component summed left to right.
+// ---------------------------------------------------------------------------
+static int grid_for_host(long long n, int threads, int cap)
+{
+    long long g = (n + threads - 1) / threads;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+struct Mat16 {
+    float m[16];
+};
+
+__global__ void k_move_model(float *vtx, int vstride, int V, Mat16 M)
+{
+    const float *m = M.m;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        float *p = vtx + (size_t)v * vstride;
+        const float x = p[0], y = p[1], z = p[2], w = 1.0f;
+        const float rx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], x), __fmul_rn(m[4], y)), __fmul_rn(m[8], z)), __fmul_rn(m[12], w));
+        const float ry = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[1], x), __fmul_rn(m[5], y)), __fmul_rn(m[9], z)), __fmul_rn(m[13], w));
+        const float rz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[2], x), __fmul_rn(m[6], y)), __fmul_rn(m[10], z)), __fmul_rn(m[14], w));
+        p[0] = rx;
+        p[1] = ry;
+        p[2] = rz;
+    }
+}
+
+cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t s)
+{
+    Mat16 M;
+    for (int i = 0; i < 16; ++i) M.m[i] = m[i];
+    if (V <= 0) return cudaSuccess;
+    k_move_model<<<grid_for_host(V, 256, 148 * 8), 256, 0, s>>>(vtx, vstride, V, M);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Host driver.
+// ---------------------------------------------------------------------------
+static_assert(kSortTileHost == kSortTile, "sort tile mismatch");
+static_assert(kTriTileHost == kTriThreads, "triangle tile mismatch");
+
+int sort_passes_for(long long keyRangeExclusive)
+{
+    int bits = 0;
+    while (bits < 32 && (1ll << bits) < keyRangeExclusive) ++bits;
+    if (bits == 0) bits = 1;
+    return (bits + 7) / 8;
+}
+
+static int grid_for(long long n, int threads, int cap)
+{
+    long long g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+// Sorts (kA, vA) with kB/vB as ping-pong buffers; `slot` selects the histogram
+// and ticket block (0 samples, 1 pairs).  Pass p uses epoch 8*launch + 4*slot + p.
+static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
+                     uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
+                     cudaStream_t s)
+{
+    uint32_t *hist = b.sortHist + slot * 4 * kRadix;
+    k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
+                                                                              cap, passes, hist);
+    uint32_t *ki = kA, *vi = vA, *ko = kB, *vo = vB;
+    const long long tiles = ((long long)cap + kSortTile - 1) / kSortTile;
+    const int passGrid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
+    for (int p = 0; p < passes; ++p) {
+        const uint32_t ep = b.epoch * 8u + (uint32_t)(slot * 4 + p);
+        k_radix_pass<<<passGrid, kSortThreads, 0, s>>>(ki, vi, ko, vo, n_dev, n_static, cap, 8 * p,
+                                                       hist + p * kRadix, b.sortStatus, ep,
+                                                       b.counters->sortTileCounter + slot * 4 + p,
+                                                       &b.counters->errorFlags);
+        uint32_t *t = ki;
+        ki = ko;
+        ko = t;
+        t = vi;
+        vi = vo;
+        vo = t;
+    }
+}
+
+static int g_smCount = 0;
+
+cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t s)
+{
+    if (g_smCount == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_smCount, cudaDevAttrMultiProcessorCount, dev);
+        if (g_smCount <= 0) g_smCount = 148;
+    }
+    const int sm = g_smCount;
+    const int nf = b.nframes;
+    k_init<<<grid_for(b.totalBins + 1, 256, sm * 8), 256, 0, s>>>(
+        b.states, nf, b.binStat, b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.totalBins);
+    {
+        const int gx = grid_for(maxS > maxV ? maxS : maxV, kReduceThreads, sm * 4);
+        k_reduce<<<dim3(gx, nf, 2), kReduceThreads, 0, s>>>(b.frames, b.states);
+    }
+    k_plan<<<(nf + 63) / 64, 64, 0, s>>>(b.frames, b.states, nf);
+    k_tri_setup<<<dim3(grid_for(maxT, 256, sm * 8), nf), 256, 0, s>>>(b.frames, b.states, b.triRec,
+                                                                      &b.counters->errorFlags);
+    k_sample_keys<<<dim3(grid_for(maxS, 256, sm * 8), nf), 256, 0, s>>>(
+        b.frames, b.states, b.keysA, b.valsA, b.binStat, b.totalBins);
+
+    if (b.dbgKeys) {
+        cudaMemcpyAsync(b.dbgKeys, b.keysA, 4ull * b.totalSamples, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(b.dbgVals, b.valsA, 4ull * b.totalSamples, cudaMemcpyDeviceToDevice, s);
+    }
+    run_sort(b, 0, b.keysA, b.valsA, b.keysB, b.valsB, nullptr, b.totalSamples, b.totalSamples,
+             b.samplePasses, sm, s);
+    uint32_t *sk = (b.samplePasses & 1) ? b.keysB : b.keysA;
+    uint32_t *sv = (b.samplePasses & 1) ? b.valsB : b.valsA;
+    k_find_start_end<<<grid_for(b.totalSamples, 256, sm * 8), 256, 0, s>>>(
+        sk, nullptr, b.totalSamples, b.totalSamples, b.binSampleStart, b.binSampleEnd,
+        (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
+
+    {
+        const int tiles = (b.totalTris + kTriThreads - 1) / kTriThreads;
+        const int grid = tiles < sm * 4 ? (tiles > 0 ? tiles : 1) : sm * 4;
+        k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
+                                                 b.triRec, b.binStat, b.triCount, b.triScanStatus,
+                                                 b.epoch, b.pkeysA, b.pvalsA, b.pairCapacity,
+                                                 b.counters);
+    }
+    if (b.dbgPKeys) {
+        cudaMemcpyAsync(b.dbgPKeys, b.pkeysA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(b.dbgPVals, b.pvalsA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
+    }
+    run_sort(b, 1, b.pkeysA, b.pvalsA, b.pkeysB, b.pvalsB, &b.counters->pairCount, 0, b.pairCapacity,
+             b.pairPasses, sm, s);
+    uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
+    uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
+    k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
+        pk, &b.counters->pairCount, 0, b.pairCapacity, b.binTriStart, b.binTriEnd,
+        (uint32_t)b.totalBins, &b.counters->errorFlags);
+    k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
+        b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
+        b.items, b.itemCapacity, b.counters);
+    k_occlusion<<<sm * 8, kOccThreads, 0, s>>>(b.frames, b.states, b.items, b.itemCapacity, b.counters,
+                                               sv, b.binSampleStart, b.binSampleEnd, b.binTriStart,
+                                               b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    return cudaGetLastError();
+}
+
+}  // namespace fdzb

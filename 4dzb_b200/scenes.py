@@ -1,0 +1,146 @@
+"""Seeded synthetic scenes for the FDZB soft-shadow path.
+
+The reference's demo meshes (dragon_1.obj, plane.obj) are not in its repository,
+so scenes are generated:
+
+* receiver: height field z = 0.3 sin(x) cos(y) over [-8, 8]^2 sampled on a W x H
+  grid with uniform +-0.5 cell jitter, analytic normals, positions pushed 1e-4
+  along the normal; row-major float4 (w = 1) positions and normals, the layout
+  of the reference's G-buffer textures (4DZB/Resources/shader/gatherData.shf);
+* occluders: a triangle soup, centroids uniform in [-6, 6]^2 x [zlo, zhi],
+  vertices = centroid + N(0, sigma^2) per axis, float4 vertices (stride 16 B),
+  int3 indices (3t, 3t+1, 3t+2);
+* light: square area light centred at (0, 0, 6) facing -z, up +y.
+
+Random numbers: splitmix64 counter streams (one stream per purpose) mapped to
+doubles in [0, 1); normal deviates by Box-Muller in double, cast to float32.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def _splitmix(seed: int, stream: int, n: int) -> np.ndarray:
+    """n uint64 outputs of the splitmix64 sequence for (seed, stream)."""
+    with np.errstate(over="ignore"):
+        base = np.uint64((seed * 0x100000001B3 + stream * 0x9E3779B1) & 0xFFFFFFFFFFFFFFFF)
+        z = base + (np.arange(1, n + 1, dtype=np.uint64) * _GOLDEN)
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform(seed: int, stream: int, n: int) -> np.ndarray:
+    return (_splitmix(seed, stream, n) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def normal(seed: int, stream: int, n: int) -> np.ndarray:
+    m = (n + 1) // 2
+    u1 = uniform(seed, stream, m)
+    u2 = uniform(seed, stream + 1000003, m)
+    u1 = np.maximum(u1, 1e-300)
+    r = np.sqrt(-2.0 * np.log(u1))
+    z = np.concatenate([r * np.cos(2.0 * np.pi * u2), r * np.sin(2.0 * np.pi * u2)])
+    return z[:n]
+
+
+@dataclass
+class Light:
+    right_radius: float = 1.0
+    top_radius: float = 1.0
+    position: tuple = (0.0, 0.0, 6.0)
+    view_dir: tuple = (0.0, 0.0, -1.0)
+    up_dir: tuple = (0.0, 1.0, 0.0)
+    n: int = 8
+
+
+@dataclass
+class Scene:
+    W: int
+    H: int
+    pos: np.ndarray          # float32 [H*W, 4]
+    nrm: np.ndarray          # float32 [H*W, 4]
+    vtx: np.ndarray          # float32 [V, 4]
+    idx: np.ndarray          # int32 [T, 3]
+    light: Light
+    bins: int
+    esp: float = 1e-3
+    cull: bool = False
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def S(self) -> int:
+        return self.W * self.H
+
+    @property
+    def T(self) -> int:
+        return int(self.idx.shape[0])
+
+    @property
+    def V(self) -> int:
+        return int(self.vtx.shape[0])
+
+
+def receiver(W: int, H: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    jx = uniform(seed, 1, W * H) - 0.5
+    jy = uniform(seed, 2, W * H) - 0.5
+    ii = np.tile(np.arange(W, dtype=np.float64), H)
+    jj = np.repeat(np.arange(H, dtype=np.float64), W)
+    x = -8.0 + (ii + 0.5 + jx) * (16.0 / W)
+    y = -8.0 + (jj + 0.5 + jy) * (16.0 / H)
+    z = 0.3 * np.sin(x) * np.cos(y)
+    n = np.stack([-0.3 * np.cos(x) * np.cos(y), 0.3 * np.sin(x) * np.sin(y), np.ones_like(x)], axis=1)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    p = np.stack([x, y, z], axis=1) + 1e-4 * n
+    pos = np.ones((W * H, 4), dtype=np.float32)
+    nrm = np.zeros((W * H, 4), dtype=np.float32)
+    pos[:, :3] = p.astype(np.float32)
+    nrm[:, :3] = n.astype(np.float32)
+    return pos, nrm
+
+
+def occluders(T: int, seed: int, sigma: float, zlo: float, zhi: float) -> tuple[np.ndarray, np.ndarray]:
+    cx = -6.0 + 12.0 * uniform(seed, 11, T)
+    cy = -6.0 + 12.0 * uniform(seed, 12, T)
+    cz = zlo + (zhi - zlo) * uniform(seed, 13, T)
+    c = np.stack([cx, cy, cz], axis=1)
+    d = normal(seed, 21, 9 * T).reshape(T, 3, 3) * sigma
+    v = (c[:, None, :] + d).reshape(3 * T, 3)
+    vtx = np.ones((3 * T, 4), dtype=np.float32)
+    vtx[:, :3] = v.astype(np.float32)
+    idx = np.arange(3 * T, dtype=np.int32).reshape(T, 3)
+    return vtx, idx
+
+
+def make_scene(W: int, H: int, T: int, n: int, bins: int, seed: int, sigma: float = 0.15,
+               zlo: float = 0.5, zhi: float = 3.0, radius: float = 1.0, esp: float = 1e-3,
+               cull: bool = False, name: str = "") -> Scene:
+    pos, nrm = receiver(W, H, seed)
+    vtx, idx = occluders(T, seed, sigma, zlo, zhi)
+    light = Light(right_radius=radius, top_radius=radius, n=n)
+    return Scene(W=W, H=H, pos=pos, nrm=nrm, vtx=vtx, idx=idx, light=light, bins=bins, esp=esp,
+                 cull=cull, name=name,
+                 meta=dict(seed=seed, sigma=sigma, zlo=zlo, zhi=zhi, radius=radius))
+
+
+# The workloads: small (CPU-oracle scale), HD single frame, large single frame.
+PRESETS = {
+    "small": dict(W=256, H=256, T=1024, n=8, bins=32, seed=1, sigma=0.15, zlo=0.5, zhi=3.0, radius=1.0),
+    "hd": dict(W=1920, H=1080, T=200_000, n=16, bins=128, seed=2, sigma=0.1, zlo=0.5, zhi=3.0, radius=1.0),
+    "large": dict(W=3840, H=2160, T=2_000_000, n=32, bins=256, seed=3, sigma=0.05, zlo=0.2, zhi=4.0,
+                  radius=2.0),
+}
+
+
+def preset(name: str, **over) -> Scene:
+    kw = dict(PRESETS[name])
+    kw.update(over)
+    return make_scene(name=name, **kw)

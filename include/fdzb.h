@@ -1,0 +1,194 @@
+/*
+ * fdzb.h -- C ABI of the B200 FDZB soft-shadow library (libfdzb.so).
+ *
+ * Drop-in boundary for the FD:: entry points of 4DZB's soft-shadow core
+ * (4DZB/FDZB_Soft_Shadow/api.h:10-56).  Each global-context function below keeps
+ * the shape of the reference function named beside it; GL object handles are
+ * replaced by caller-owned device pointers (the reference maps its GL VBO/IBO,
+ * G-buffer textures and PBO into exactly such pointers every frame,
+ * FS/api.cpp:413-420 and FS/util/OpenGLinteroperate.h:42-55,131-136).
+ *
+ * Conventions
+ *  - every entry point returns int status: 0 = FDZB_OK, negative = error;
+ *    fdzb_last_error() returns the message of the last failure on this thread;
+ *  - no C++ exceptions cross the ABI; no torch types appear in any signature;
+ *  - device pointers are CUDA global-memory pointers on the context's device;
+ *  - samples are row-major float4[W*H] positions and normals (xyz, w unused),
+ *    NaN position.x marks background (the reference's G-buffer clear value);
+ *  - outputs: shadow float[W*H] at index y*W+x (fraction of occluded light
+ *    samples, 1 - visibility) and, optionally, masks uint32[W*H][ceil(N*N/32)]
+ *    with light sample (row i along the light's width, column j along its
+ *    height) at bit i*N+j, least significant bit first.
+ *
+ * Reference-shaped global context: one process-wide context on the current CUDA
+ * device, single-threaded like FD:: (K/FourD.cu:47-136).  The fdzb_ctx_* handle
+ * API is the re-entrant form: one context per scene / host thread / stream.
+ */
+#ifndef FDZB_H
+#define FDZB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDZB_OK                   0
+#define FDZB_ERR_INVALID_ARG     -1
+#define FDZB_ERR_CUDA            -2
+#define FDZB_ERR_NOT_INITIALIZED -3
+#define FDZB_ERR_NO_MEMORY       -4
+#define FDZB_ERR_CAPACITY        -5   /* a device buffer overflowed and re-planning failed */
+#define FDZB_ERR_DEVICE_TIMEOUT  -6   /* a bounded device-side wait gave up */
+#define FDZB_ERR_UNSUPPORTED     -7
+#define FDZB_ERR_NOT_READY       -8   /* required inputs (view, samples, model, light, output) not set */
+
+/* Same 52-byte layout as AreaLightDes (4DZB/FDZB_Soft_Shadow/AreaLightDesc.h:3-14):
+ * two floats, three glm::vec3, two ints.  lightResWidth == lightResHeight = N, 1..32. */
+typedef struct fdzb_area_light_desc {
+    float rightRadius;      /* half width */
+    float topRadius;        /* half height */
+    float position[3];
+    float viewDir[3];
+    float upDir[3];
+    int32_t lightResWidth;
+    int32_t lightResHeight;
+} fdzb_area_light_desc;
+
+/* ---- reference-shaped global context (FD:: namespace, FS/api.h) ---------- */
+
+/* FD::FDinit (FS/api.h:15, FS/api.cpp:48-144). Creates the global context on the
+ * current device.  Calling it again resets the context. */
+int fdzb_init(void);
+/* FD::FDsetBackfaceCull (FS/api.h:18, FS/api.cpp:146-150).  Default 1, like
+ * m_enable_backfacecull (K/FourD.cu:61). */
+int fdzb_set_backface_cull(int enable);
+/* FD::FDaddModel (FS/api.h:21, FS/api.cpp:152-160).  d_vtx: n_vtx vertices of
+ * vtx_stride_bytes each (xyz first; stride a multiple of 4 bytes), d_idx: int3[n_tri].
+ * Like the reference (FS/api.cpp:430-445) only the first model added is shaded. */
+int fdzb_add_model(const float *d_vtx, size_t n_vtx, size_t vtx_stride_bytes,
+                   const int32_t *d_idx, size_t n_tri, const char *name);
+/* FD::FDsetSampleGLTex (FS/api.h:24, FS/api.cpp:162-166): the G-buffer position and
+ * normal images, as device float4[W*H] arrays. */
+int fdzb_set_sample_buffers(const float *d_pos, const float *d_nrm);
+/* FD::FDsetOutputGLBuffer (FS/api.h:27, FS/api.cpp:168-171): float[W*H] shadow
+ * fractions; d_masks (nullable) receives the per-sample occlusion bit masks. */
+int fdzb_set_output_buffer(float *d_shadow, uint32_t *d_masks);
+/* FD::FDregisterGLres / FDunregisterGLres (FS/api.h:30-33, FS/api.cpp:173-191).  No
+ * graphics interop here: these validate that the buffers set above are
+ * device-accessible and return 0. */
+int fdzb_register_resources(void);
+int fdzb_unregister_resources(void);
+/* FD::FDsetBinNum (FS/api.h:36; body commented out at FS/api.cpp:193-202, the
+ * reference fixes 16 at compile time, FS/constants.h:13).  Light-plane bins per
+ * side; power of two in [1, 512].  Default 16. */
+int fdzb_set_bin_num(size_t bin_num);
+/* FD::FDsetView (FS/api.h:39, FS/api.cpp:205-237). */
+int fdzb_set_view(int view_width, int view_height);
+/* FD::FDsetScenesEsp (FS/api.h:41, FS/api.cpp:238-241).  Default 1e-6 like
+ * K/FourD.cu:62 (the demo app sets 1e-3). */
+int fdzb_set_scenes_esp(float scenes_esp);
+/* FD::FDsetSceneParams (FS/api.h:44, FS/api.cpp:243-294): capacity hints used to
+ * pre-size per-triangle buffers. */
+int fdzb_set_scene_params(size_t max_triangle_num, size_t max_vertices_num);
+/* FD::FDsetAreaLight (FS/api.h:49, FS/api.cpp:303-400). */
+int fdzb_set_area_light(const fdzb_area_light_desc *light);
+/* FD::FDLaunch (FS/api.h:52, FS/api.cpp:402-582): computes one frame and returns its
+ * GPU time in milliseconds (CUDA events around the whole frame), or a negative
+ * FDZB_ERR_* value on failure. */
+float fdzb_launch(void);
+/* FD::moveModel (FS/api.h:12, K/moveModel.inl:31-51): applies the column-major
+ * 4x4 matrix m to the xyz of every vertex of model 0, in place. */
+int fdzb_move_model(const float m[16]);
+/* Message of the last failing call on this thread ("" if none). */
+const char *fdzb_last_error(void);
+
+/* ---- context handle API (re-entrant form) -------------------------------- */
+
+typedef struct fdzb_ctx fdzb_ctx;
+
+/* Per-frame counters of the last completed launch. */
+typedef struct fdzb_frame_stats {
+    int32_t state;             /* 0: no sample or vertex in front of the light;
+                                  1: only back-facing samples shaded (no light plane,
+                                     no valid sample or triangle); 2: full pipeline */
+    int32_t valid_samples;     /* samples with a light-plane bin */
+    int32_t valid_triangles;   /* triangles overlapping the light plane */
+    int32_t num_pairs;         /* triangle/bin pairs */
+    int32_t num_bins;
+    int32_t pair_capacity;
+    int64_t pair_tests;        /* sample/triangle pairs past the AABB pre-cull */
+    float f;                   /* far plane */
+    float sub[2];
+    float lp_begin[3], lp_end[3], lp_factor[2];
+    float sample_aabb[6], model_aabb[6];
+    int32_t replans;           /* pair-buffer regrowths in this launch */
+    int32_t quirk_key_range;   /* samples whose bin fell outside the grid (treated as unbinned) */
+} fdzb_frame_stats;
+
+/* device < 0: current device. */
+int fdzb_ctx_create(fdzb_ctx **out, int device);
+int fdzb_ctx_destroy(fdzb_ctx *ctx);
+/* Work is enqueued on `stream` (a cudaStream_t); NULL = the context's own stream. */
+int fdzb_ctx_set_stream(fdzb_ctx *ctx, void *stream);
+int fdzb_ctx_set_backface_cull(fdzb_ctx *ctx, int enable);
+int fdzb_ctx_add_model(fdzb_ctx *ctx, const float *d_vtx, size_t n_vtx, size_t vtx_stride_bytes,
+                       const int32_t *d_idx, size_t n_tri, const char *name);
+int fdzb_ctx_set_sample_buffers(fdzb_ctx *ctx, const float *d_pos, const float *d_nrm);
+int fdzb_ctx_set_output_buffer(fdzb_ctx *ctx, float *d_shadow, uint32_t *d_masks);
+int fdzb_ctx_set_bin_num(fdzb_ctx *ctx, size_t bin_num);
+int fdzb_ctx_set_view(fdzb_ctx *ctx, int view_width, int view_height);
+int fdzb_ctx_set_scenes_esp(fdzb_ctx *ctx, float scenes_esp);
+int fdzb_ctx_set_scene_params(fdzb_ctx *ctx, size_t max_triangle_num, size_t max_vertices_num);
+int fdzb_ctx_set_area_light(fdzb_ctx *ctx, const fdzb_area_light_desc *light);
+int fdzb_ctx_move_model(fdzb_ctx *ctx, const float m[16]);
+/* Synchronous frame (FDLaunch form); *ms_out (nullable) gets the GPU time. */
+int fdzb_ctx_launch(fdzb_ctx *ctx, float *ms_out);
+/* Enqueue the frame on the context stream without waiting.  Pair-buffer overflow
+ * is only detected (and the frame re-run) by fdzb_ctx_sync. */
+int fdzb_ctx_launch_async(fdzb_ctx *ctx);
+int fdzb_ctx_sync(fdzb_ctx *ctx);
+int fdzb_ctx_get_stats(fdzb_ctx *ctx, fdzb_frame_stats *out);
+
+/* Intermediate arrays of the last launch, for parity checks and debugging (the
+ * reference dumps the same data with saveBinImage / showBinTriPair,
+ * K/binRaster.inl:61-182, K/Step4_RasterizeTriangleToBin.inl:236-250).
+ * Copies `bytes` bytes of array `what` into host memory `dst`. */
+enum fdzb_array_id {
+    FDZB_ARR_SAMPLE_KEYS = 0,       /* int32[S] bin key per sample, y*W+x order (num_bins = unbinned) */
+    FDZB_ARR_SORTED_SAMPLE_KEYS,    /* int32[S] */
+    FDZB_ARR_SORTED_SAMPLE_IDS,     /* int32[S] y*W+x of each sorted entry */
+    FDZB_ARR_BIN_SAMPLE_START,      /* int32[num_bins+1] */
+    FDZB_ARR_BIN_SAMPLE_END,        /* int32[num_bins+1] */
+    FDZB_ARR_BIN_MAXZ,              /* float[num_bins] */
+    FDZB_ARR_BIN_RANGE,             /* float[4*num_bins] */
+    FDZB_ARR_TRI_COUNT,             /* int32[T] bins per triangle */
+    FDZB_ARR_PAIR_BIN,              /* int32[num_pairs] triangle order */
+    FDZB_ARR_PAIR_TRI,              /* int32[num_pairs] */
+    FDZB_ARR_SORTED_PAIR_BIN,       /* int32[num_pairs] */
+    FDZB_ARR_SORTED_PAIR_TRI,       /* int32[num_pairs] */
+    FDZB_ARR_BIN_TRI_START,         /* int32[num_bins] */
+    FDZB_ARR_BIN_TRI_END,           /* int32[num_bins] */
+    FDZB_ARR_TRI_AABB,              /* float[8*T] (min xyz,1, max xyz,1) */
+    FDZB_ARR_COUNT
+};
+int fdzb_ctx_export(fdzb_ctx *ctx, int what, void *dst, size_t bytes);
+/* flags bit 0: keep copies of the pre-sort key/value arrays (FDZB_ARR_SAMPLE_KEYS,
+ * FDZB_ARR_PAIR_BIN, FDZB_ARR_PAIR_TRI) at the cost of two extra device copies per
+ * sort.  Off by default. */
+int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
+
+/* Host-side light setup only (FS/api.cpp:303-400): fills the 16-float
+ * column-major light projection, RectangleFactor and the four light corners
+ * (upRight, upLeft, downLeft, downRight), x_delt and y_delt. */
+int fdzb_light_setup(const fdzb_area_light_desc *light, float mat[16], float rect_factor[2],
+                     float corners[12], float deltas[6]);
+
+/* Library version string. */
+const char *fdzb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDZB_H */

@@ -1,0 +1,118 @@
+/*
+ * fdzb_oracle.h -- CPU oracle for the FDZB soft-shadow path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the 4dzb_b200 package,
+ * libfdzb.so) links, loads or calls this code.  It is used by tests/ as the
+ * checker, by __graft_entry__.smoke() as the checker, and by bench.py for the
+ * timed CPU baseline leg.
+ *
+ * Three oracles live here:
+ *   O2  orc_frame()           FP32 restatement of the reference pipeline, stage by
+ *                             stage (light setup, rectangles, light plane, triangle
+ *                             setup, sample keys, stable sort, segments, bin stats,
+ *                             triangle/bin pairs, per-sample occlusion, popcount).
+ *                             Built with -ffp-contract=off: every + - * / is one IEEE
+ *                             binary32 operation in the reference's source order.
+ *   O3  orc_exhaustive_fp64() FP64 exhaustive per-light-sample edge test with no
+ *                             binning and no AABB pre-cull.
+ *   CPU orc_exhaustive_fp32() the O2 per-pair arithmetic run exhaustively (every
+ *                             valid sample x every valid triangle) with OpenMP: the
+ *                             reported CPU baseline.
+ *
+ * Parity is pinned against the reference's own kernel and host source compiled
+ * for the CPU (oracle/ref_emu, output in oracle/_ref/) and the golden fixtures it
+ * produced (tests/golden/).
+ */
+#ifndef FDZB_ORACLE_H
+#define FDZB_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same 52-byte layout as AreaLightDes (4DZB/FDZB_Soft_Shadow/AreaLightDesc.h:3-14). */
+typedef struct {
+    float rightRadius, topRadius;
+    float position[3], viewDir[3], upDir[3];
+    int32_t lightResWidth, lightResHeight;
+} orc_light_desc;
+
+/* Derived light block; mirrors AreaLight (4DZB/FDZB_Soft_Shadow/cuda/privateDefs.h:66-101). */
+typedef struct {
+    float rightRadius, topRadius;
+    float position[3], viewDir[3], upDir[3];
+    int32_t resW, resH, resNum;
+    uint32_t fullBits;
+    float rightDir[3], topDir[3], x_delt[3], y_delt[3];
+    float upRight[3], downLeft[3], upLeft[3], downRight[3];
+    float mat[16];
+    float RF[2];
+} orc_light;
+
+typedef struct {
+    int32_t W, H;
+    const float *pos, *nrm;      /* float4[W*H], row-major, NaN x = background */
+    const float *vtx;            /* vertex buffer, vtx_stride_floats floats per vertex, xyz first */
+    int32_t vtx_stride_floats, V;
+    const int32_t *idx;          /* int3[T] */
+    int32_t T;
+    int32_t bins;                /* light-plane bins per side (power of two) */
+    int32_t cull;                /* triangle back-face cull */
+    float esp;
+    const orc_light *light;
+    int32_t nthreads;            /* <= 0: OpenMP default */
+} orc_frame_in;
+
+typedef struct {
+    /* scalars */
+    int32_t state;               /* 0 no shadow work, 1 back-facing samples only, 2 full */
+    float f, sub[2];
+    float sample_aabb[6], model_aabb[6];  /* min xyz, max xyz */
+    float lp_begin[3], lp_end[3], lp_factor[2];
+    int32_t bins_log2, num_bins, view_log2up;
+    int32_t valid_samples, valid_tris, num_pairs, pair_overflow;
+    int64_t pairs_tested;        /* sample/triangle pairs that pass the AABB pre-cull */
+    int64_t quirk_rows_beyond_n; /* pairs whose row filter selects rows >= N (reference UB) */
+    int64_t quirk_high_bits;     /* samples whose reference mask would hold bits >= N */
+    int64_t quirk_key_range;     /* samples whose bin x/y fell outside the grid */
+    /* arrays, caller-allocated; NULL skips the copy */
+    int32_t *keys, *vals;                     /* [S] position order */
+    int32_t *sorted_keys, *sorted_vals;       /* [S] */
+    int32_t *bin_sample_start, *bin_sample_end; /* [num_bins + 1] */
+    float *bin_maxz;                          /* [num_bins] */
+    float *bin_range;                         /* [4 * num_bins] */
+    float *tri_aabb;                          /* [8 * T] */
+    int32_t *tri_count;                       /* [T] */
+    int32_t pair_capacity;
+    int32_t *pair_bin, *pair_tri;             /* [pair_capacity], triangle order */
+    int32_t *sorted_pair_bin, *sorted_pair_tri;
+    int32_t *bin_tri_start, *bin_tri_end;     /* [num_bins] */
+    uint32_t *masks;                          /* [S * words] */
+    float *shadow;                            /* [S] */
+} orc_frame_out;
+
+int32_t orc_mask_words(int32_t N);
+void orc_light_setup(const orc_light_desc *d, orc_light *out);
+/* returns 0 on success, negative on bad input / allocation failure */
+int32_t orc_frame(const orc_frame_in *in, orc_frame_out *out);
+
+/* Exhaustive FP32 per-pair loop (CPU baseline). Samples listed in `sample_ids`
+ * (row-major indices) are tested against every valid triangle.  Requires the
+ * frame scalars from a previous orc_frame() call on the same inputs (`fr`).
+ * Writes masks[n * words]; returns the number of pair tests executed. */
+int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
+                            const int32_t *sample_ids, int32_t n, uint32_t *masks);
+
+/* Exhaustive FP64 per-light-sample edge test (O3).  For each listed sample:
+ * masks[n * words] and min_dist[n * N * N] = min over edges of the FP64
+ * distance (light-grid units) from each light sample to the nearest projected
+ * edge of any triangle that decides it. */
+void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
+                         const int32_t *sample_ids, int32_t n, uint32_t *masks,
+                         double *edge_dist);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
