@@ -49,8 +49,12 @@ EXPORTED = [
     "fdzb_ctx_set_bin_num", "fdzb_ctx_set_view", "fdzb_ctx_set_scenes_esp",
     "fdzb_ctx_set_scene_params", "fdzb_ctx_set_area_light", "fdzb_ctx_move_model",
     "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
-    "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_light_setup", "fdzb_version",
+    "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_ctx_set_tri_order", "fdzb_light_setup",
+    "fdzb_version",
 ]
+
+TRI_ORDER_REFERENCE = 0
+TRI_ORDER_DEPTH = 1
 
 
 class FdzbError(RuntimeError):
@@ -135,6 +139,7 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_launch": ([vp, P(ctypes.c_float)], i32), "fdzb_ctx_launch_async": ([vp], i32),
         "fdzb_ctx_sync": ([vp], i32), "fdzb_ctx_get_stats": ([vp, P(FrameStats)], i32),
         "fdzb_ctx_export": ([vp, i32, vp, sz], i32), "fdzb_ctx_set_debug": ([vp, i32], i32),
+        "fdzb_ctx_set_tri_order": ([vp, i32], i32),
         "fdzb_light_setup": ([P(AreaLightDesc), P(ctypes.c_float), P(ctypes.c_float),
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
@@ -211,6 +216,10 @@ class Context:
     def set_debug(self, flags: int) -> None:
         """flags bit 0: keep pre-sort copies of the key arrays for export()."""
         _check(self._lib.fdzb_ctx_set_debug(self._h, int(flags)))
+
+    def set_tri_order(self, order: int) -> None:
+        """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_DEPTH."""
+        _check(self._lib.fdzb_ctx_set_tri_order(self._h, int(order)))
 
     def add_model(self, vtx, n_vtx: int, stride_bytes: int, idx, n_tri: int, name: str = "") -> None:
         self._keep += [vtx, idx]
@@ -361,7 +370,8 @@ def upload_scene(scene, device: str = "cuda"):
     return pos, nrm, vtx, idx
 
 
-def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bool = False):
+def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bool = False,
+                      tri_order: Optional[int] = None):
     """A Context with the scene's buffers uploaded and outputs allocated.
     Returns (ctx, tensors dict)."""
     import torch
@@ -371,6 +381,8 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
     ctx = Context()
     if debug:
         ctx.set_debug(1)
+    if tri_order is not None:
+        ctx.set_tri_order(tri_order)
     ctx.set_view(scene.W, scene.H)
     ctx.set_bin_num(scene.bins)
     ctx.set_scenes_esp(scene.esp)

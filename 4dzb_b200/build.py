@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfdzb.so")
 
 SOURCES = ["fdzb_pipeline.cu", "fdzb_api.cpp", "fdzb_light.cpp"]
-HEADERS = ["fdzb_internal.h", "fdzb_device.cuh", "fdzb_sort.cuh"]
+HEADERS = ["fdzb_internal.h", "fdzb_device.cuh", "fdzb_sort.cuh", "fdzb_occlusion.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -47,13 +47,18 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_library(force: bool = False, verbose: bool = False) -> str:
+def build_library(force: bool = False, verbose: bool = False, defines: tuple = (),
+                  out: str | None = None) -> str:
+    """Compile libfdzb.so; `defines` are extra -D macros (tuning switches of
+    fdzb_occlusion.cuh) and `out` an alternative output path."""
+    lib = out or LIB
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(ROOT, "include", "fdzb.h"))
-    if not force and not _stale(LIB, deps):
-        return LIB
-    tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", tmp, *[os.path.join(CSRC, f) for f in SOURCES]]
+    if not force and not defines and not _stale(lib, deps):
+        return lib
+    tmp = lib + ".tmp"
+    cmd = [_nvcc(), *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-o", tmp,
+           *[os.path.join(CSRC, f) for f in SOURCES]]
     env = dict(os.environ)
     # the host compiler must be the system g++ (an alternative gcc on PATH may
     # lack the runtime libraries)
@@ -64,10 +69,11 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         sys.stderr.write(res.stdout + res.stderr)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed ({res.returncode})")
-    os.replace(tmp, LIB)
-    with open(os.path.join(HERE, "ptxas_info.txt"), "w") as fh:
-        fh.write(res.stderr)
-    return LIB
+    os.replace(tmp, lib)
+    if out is None:
+        with open(os.path.join(HERE, "ptxas_info.txt"), "w") as fh:
+            fh.write(res.stderr)
+    return lib
 
 
 def build_oracle(verbose: bool = False) -> None:

@@ -80,6 +80,7 @@ struct fdzb_ctx {
     int pairCapacity = 0;
     uint32_t epoch = 0;
     int debug = 0;  // keep pre-sort copies for fdzb_ctx_export
+    int triOrder = FDZB_TRI_ORDER_DEPTH;
     // pinned host staging
     fdzb::FrameDesc *hFrame = nullptr;
     fdzb::Counters *hCounters = nullptr;
@@ -209,7 +210,22 @@ int enqueue(fdzb_ctx *c)
     if (rc) return rc;
     fdzb::DeviceBuffers &b = c->buf;
     b.samplePasses = fdzb::sort_passes_for((long long)NB + 1);
-    b.pairPasses = fdzb::sort_passes_for((long long)NB);
+    // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
+    // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
+    // order appends a depth bucket below the bin so each bin lists its lowest
+    // triangles first, which fills the masks in far fewer pair tests; it uses the
+    // key bits left over in the last radix pass, at least 4.
+    {
+        int binBits = 0;
+        while ((1ll << binBits) < (long long)NB) ++binBits;
+        if (c->triOrder == FDZB_TRI_ORDER_DEPTH) {
+            const int passes = (binBits + 4 + 7) / 8;
+            b.depthBits = std::min(10, passes * 8 - binBits);
+        } else {
+            b.depthBits = 0;
+        }
+        b.pairPasses = fdzb::sort_passes_for((long long)NB << b.depthBits);
+    }
     b.epoch = ++c->epoch;
 
     fdzb::FrameDesc &f = *c->hFrame;
@@ -394,6 +410,15 @@ int fdzb_ctx_set_debug(fdzb_ctx *c, int flags)
     return FDZB_OK;
 }
 
+int fdzb_ctx_set_tri_order(fdzb_ctx *c, int order)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_DEPTH)
+        return fail(FDZB_ERR_INVALID_ARG, "unknown triangle order");
+    c->triOrder = order;
+    return FDZB_OK;
+}
+
 int fdzb_ctx_set_backface_cull(fdzb_ctx *c, int enable)
 {
     if (int rc = ctx_check(c)) return rc;
@@ -572,10 +597,20 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
     }
     case FDZB_ARR_TRI_COUNT: src = b.triCount; avail = 4 * T; break;
     case FDZB_ARR_PAIR_BIN:
+    case FDZB_ARR_SORTED_PAIR_BIN: {
+        // pair keys carry the depth bucket below the bin; export the bin
+        const uint32_t *s2 = what == FDZB_ARR_PAIR_BIN ? b.dbgPKeys : (pOdd ? b.pkeysB : b.pkeysA);
+        if (!s2) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
+        if (bytes > 4 * P) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
+        std::vector<uint32_t> v(bytes / 4);
+        if (!v.empty()) FDZB_CUDA(cudaMemcpy(v.data(), s2, 4 * v.size(), cudaMemcpyDeviceToHost));
+        for (uint32_t &x : v) x >>= b.depthBits;
+        std::memcpy(dst, v.data(), 4 * v.size());
+        return FDZB_OK;
+    }
     case FDZB_ARR_PAIR_TRI:
-        if (!b.dbgPKeys) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
-        src = what == FDZB_ARR_PAIR_BIN ? b.dbgPKeys : b.dbgPVals; avail = 4 * P; break;
-    case FDZB_ARR_SORTED_PAIR_BIN: src = pOdd ? b.pkeysB : b.pkeysA; avail = 4 * P; break;
+        if (!b.dbgPVals) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
+        src = b.dbgPVals; avail = 4 * P; break;
     case FDZB_ARR_SORTED_PAIR_TRI: src = pOdd ? b.pvalsB : b.pvalsA; avail = 4 * P; break;
     case FDZB_ARR_BIN_TRI_START: src = b.binTriStart; avail = 4 * NB; break;
     case FDZB_ARR_BIN_TRI_END: src = b.binTriEnd; avail = 4 * NB; break;

@@ -78,8 +78,11 @@ void light_setup(const float rightRadius, const float topRadius, const float pos
     mv[3][2] = dot(f, ur);
 
     // infinitePerspectiveRH(fovy = 120 (radians in GLM 0.9.8), aspect 1, zNear 0.1)
+    // tan(fovy / 2) is taken correctly rounded to binary32 (evaluated in double):
+    // 0.32004037f.  C runtimes differ in the last bit here -- glibc's tanf(60.0f)
+    // returns 0.3200404f -- and this constant scales the whole projection.
     const float fovy = 120.0f, aspect = 1.0f, zNear = 0.1f;
-    const float range = std::tan(fovy / 2.0f) * zNear;
+    const float range = (float)std::tan((double)(fovy / 2.0f)) * zNear;
     const float left = -range * aspect, rgt = range * aspect, bottom = -range, tp = range;
     float P[4][4] = {};
     P[0][0] = (2.0f * zNear) / (rgt - left);

@@ -1,0 +1,360 @@
+// fdzb_occlusion.cuh -- per-bin occlusion and popcount shading (stages c + d).
+//
+// Reference: shadowCal_per_sample_kernel (K/Step5_2_shadowCalPerSample.inl:37-231),
+// one thread per sample walking its bin's triangle list through texture fetches.
+//
+// Here a warp owns a work item: up to kItemSamples samples of one bin.  The bin's
+// triangle records are staged into shared memory kOccChunk at a time, together
+// with the per-triangle values every pair test of the reference recomputes
+// (the face normal cross(v1-v0, v2-v1) and the edge vectors v0-v1, v1-v2,
+// v2-v0, each the same IEEE operation sequence).  Every lane tests its own
+// sample against the staged triangles.  A lane whose sample is done (all light
+// rows full -- the reference's early-out -- or every triangle seen) writes its
+// result and, at the next chunk boundary, takes the next sample of the item;
+// the warp streams the triangle list cyclically and each lane stops after
+// exactly one full cycle.  The final mask is the OR over the tested triangles,
+// so it is independent of the order and of where in the cycle a lane starts.
+#pragma once
+#include "fdzb_device.cuh"
+
+namespace fdzb {
+
+#ifndef FDZB_OCC_REFILL
+#define FDZB_OCC_REFILL 0
+#endif
+#ifndef FDZB_OCC_MINBLOCKS
+#define FDZB_OCC_MINBLOCKS 6
+#endif
+
+constexpr int kOccWarps = 4;
+constexpr int kOccThreads = kOccWarps * 32;
+constexpr int kOccChunk = 32;
+constexpr int kItemSamples = 256;
+
+// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(N-1) precomputed (the same
+// product) and the result limited to the N-bit light grid.
+__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full)
+{
+    const bool f1 = D >= 0.0f;
+    const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
+    if (f1 && f2) return full;
+    if (!f1 && !f2) return 0u;
+    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
+    const int k = __float2int_rz(ceilf(q));
+    uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
+    m -= 1u;
+    if (!f1) m = ~m;
+    return m & full;
+}
+
+// K/Step5_2_shadowCal.inl:213-222
+__device__ __forceinline__ bool point_in_tri(f3 A, f3 B, f3 C, f3 P)
+{
+    const f3 N1 = cross3(sub3(B, A), sub3(P, B));
+    const f3 N2 = cross3(sub3(C, B), sub3(P, C));
+    if (dot3(N1, N2) < 0.0f) return false;
+    const f3 N3 = cross3(sub3(A, C), sub3(P, A));
+    if (dot3(N2, N3) < 0.0f) return false;
+    return true;
+}
+
+// Staged triangle, 7 x float4:
+//  p0 = (aabb min x, min y, max x, max y)   p1 = (minz, v0)
+//  p2 = (v1, v2.x)   p3 = (v2.y, v2.z, n.x, n.y)   p4 = (n.z, e01)
+//  p5 = (e12, e20.x) p6 = (e20.y, e20.z, 0, 0)
+struct StagedTri {
+    float4 p[7];
+};
+
+__device__ __forceinline__ void stage_triangle(StagedTri &dst, const float4 *__restrict__ rec, int tri)
+{
+    const float4 q0 = __ldg(rec + 4 * (size_t)tri);
+    const float4 q1 = __ldg(rec + 4 * (size_t)tri + 1);
+    const float4 q2 = __ldg(rec + 4 * (size_t)tri + 2);
+    const float4 q3 = __ldg(rec + 4 * (size_t)tri + 3);
+    const f3 v0 = mk3(q0.x, q0.y, q0.z), v1 = mk3(q1.x, q1.y, q1.z), v2 = mk3(q2.x, q2.y, q2.z);
+    const f3 n = cross3(sub3(v1, v0), sub3(v2, v1));   // K/Step5_2_shadowCalPerSample.inl:130
+    const f3 e01 = sub3(v0, v1), e12 = sub3(v1, v2), e20 = sub3(v2, v0);  // a - b of :7
+    dst.p[0] = q3;
+    dst.p[1] = make_float4(q0.w, v0.x, v0.y, v0.z);
+    dst.p[2] = make_float4(v1.x, v1.y, v1.z, v2.x);
+    dst.p[3] = make_float4(v2.y, v2.z, n.x, n.y);
+    dst.p[4] = make_float4(n.z, e01.x, e01.y, e01.z);
+    dst.p[5] = make_float4(e12.x, e12.y, e12.z, e20.x);
+    dst.p[6] = make_float4(e20.y, e20.z, 0.0f, 0.0f);
+}
+
+struct LaneSample {
+    f3 Q, L0Q;
+    float spx, spy, spz, spw, spZ;
+};
+
+__device__ __forceinline__ void load_sample(LaneSample &s, const FrameDesc &fr, const FrameState &st,
+                                            int local)
+{
+    const float4 P = __ldg(fr.pos + local);
+    s.Q = mk3(P.x, P.y, P.z);
+    const f3 r = light_project(fr.light.mat, s.Q);
+    s.spx = r.x;
+    s.spy = r.y;
+    s.spz = __fsub_rn(__fadd_rn(r.x, __fdiv_rn(fr.light.RF[0], r.z)), st.subx);
+    s.spw = __fsub_rn(__fadd_rn(r.y, __fdiv_rn(fr.light.RF[1], r.z)), st.suby);
+    s.spZ = r.z;
+    s.L0Q = sub3(ld3(fr.light.ur), s.Q);
+}
+
+// One sample/triangle pair (K/Step5_2_shadowCalPerSample.inl:120-222).  Returns 1
+// if the pair passed the AABB pre-cull.
+__device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s, f3 xd, f3 yd,
+                                         float esp, float nm1, uint32_t FULL, uint32_t (*rows)[32],
+                                         int lane, uint32_t &fullRows)
+{
+    const float4 p0 = T.p[0];
+    const float4 p1 = T.p[1];
+    if (!(p0.x <= s.spx && p0.y <= s.spy && s.spz <= p0.z && s.spw <= p0.w && p1.x <= s.spZ)) return 0;
+    const float4 p2 = T.p[2], p3 = T.p[3], p4 = T.p[4], p5 = T.p[5], p6 = T.p[6];
+    const f3 v0 = mk3(p1.y, p1.z, p1.w), v1 = mk3(p2.x, p2.y, p2.z), v2 = mk3(p2.w, p3.x, p3.y);
+    const f3 n = mk3(p3.z, p3.w, p4.x);
+    const f3 e01 = mk3(p4.y, p4.z, p4.w), e12 = mk3(p5.x, p5.y, p5.z), e20 = mk3(p5.w, p6.x, p6.y);
+    const f3 Q = s.Q;
+    const float dir = dot3(sub3(Q, v0), n);
+    if (fabsf(dir) < esp && point_in_tri(v0, v1, v2, Q)) return 1;
+    // orientation: the reference negates t0, t1 and L0 - Q when dir < 0
+    const bool neg = dir < 0.0f;
+    const f3 t0 = neg ? mk3(-xd.x, -xd.y, -xd.z) : xd;
+    const f3 t1 = neg ? mk3(-yd.x, -yd.y, -yd.z) : yd;
+    const f3 lq = neg ? mk3(-s.L0Q.x, -s.L0Q.y, -s.L0Q.z) : s.L0Q;
+    // getPlaneDiscriminant for (v0,v1), (v1,v2), (v2,v0): n_k = cross(b - Q, a - b)
+    const f3 n0 = cross3(sub3(v1, Q), e01);
+    const f3 n1 = cross3(sub3(v2, Q), e12);
+    const f3 n2 = cross3(sub3(v0, Q), e20);
+    const float A0 = dot3(n0, t0), B0 = dot3(n0, t1), C0 = dot3(n0, lq);
+    const float A1 = dot3(n1, t0), B1 = dot3(n1, t1), C1 = dot3(n1, lq);
+    const float A2 = dot3(n2, t0), B2 = dot3(n2, t1), C2 = dot3(n2, lq);
+    const float An0 = __fmul_rn(A0, nm1), An1 = __fmul_rn(A1, nm1), An2 = __fmul_rn(A2, nm1);
+    const float Bn0 = __fmul_rn(B0, nm1), Bn1 = __fmul_rn(B1, nm1), Bn2 = __fmul_rn(B2, nm1);
+    // row filter (:176-191)
+    const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL);
+    const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL);
+    const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL);
+    uint32_t vr = N0 & N1 & N2 & ~fullRows;
+    // rows (:204-222)
+    while (vr) {
+        const int r = __ffs(vr) - 1;
+        vr &= vr - 1u;
+        const float fr = (float)r;
+        const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, FULL);
+        const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, FULL);
+        const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, FULL);
+        const uint32_t nv = rows[r][lane] | (M0 & M1 & M2);
+        rows[r][lane] = nv;
+        if (nv == FULL) fullRows |= 1u << r;
+    }
+    return 1;
+}
+
+__device__ __forceinline__ void write_result(const FrameDesc &fr, int local, int N, uint32_t (*rows)[32],
+                                             int lane)
+{
+    int cnt = 0;
+    for (int r = 0; r < N; ++r) cnt += __popc(rows[r][lane]);
+    fr.shadow[local] = __fdiv_rn((float)cnt, (float)(N * N));   // :226-231
+    if (fr.masks) {
+        uint32_t *mo = fr.masks + (size_t)local * fr.maskWords;
+        uint32_t acc = 0u;
+        int bit = 0, wi = 0;
+        for (int r = 0; r < N; ++r) {
+            const uint32_t v = rows[r][lane];
+            acc |= v << bit;
+            const int nb = bit + N;
+            if (nb >= 32) {
+                mo[wi++] = acc;
+                acc = (nb > 32) ? (v >> (32 - bit)) : 0u;
+                bit = nb - 32;
+            } else {
+                bit = nb;
+            }
+        }
+        if (bit > 0) mo[wi] = acc;
+    }
+}
+
+__device__ __forceinline__ void write_zero(const FrameDesc &fr, int local)
+{
+    fr.shadow[local] = 0.0f;
+    if (fr.masks) {
+        uint32_t *mo = fr.masks + (size_t)local * fr.maskWords;
+        for (int w = 0; w < fr.maskWords; ++w) mo[w] = 0u;
+    }
+}
+
+// k_items: one thread per bin; a bin with n samples yields ceil(n / kItemSamples)
+// items (bin, first sample offset, frame, triangle count).
+__global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
+                        const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
+                        const int *__restrict__ binBases, int nframes, int totalBins,
+                        int4 *__restrict__ items, int capacity, Counters *ctr)
+{
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < totalBins;
+         base += gridDim.x * blockDim.x) {
+        const int b = base + lane;
+        int n = 0;
+        if (b < totalBins) n = (bse[b] - bss[b] + kItemSamples - 1) / kItemSamples;
+        int x = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFullWarp, x, o);
+            if (lane >= o) x += y;
+        }
+        const int tot = __shfl_sync(kFullWarp, x, 31);
+        int wbase = 0;
+        if (lane == 0 && tot) wbase = atomicAdd(&ctr->itemCount, tot);
+        wbase = __shfl_sync(kFullWarp, wbase, 0);
+        if (n) {
+            const int f = frame_of(binBases, nframes, b);
+            const int nt = bte[b] - bts[b];
+            for (int k = 0; k < n; ++k) {
+                const int slot = wbase + x - n + k;
+                if (slot < capacity) items[slot] = make_int4(b, kItemSamples * k, f, nt);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
+    k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
+                const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
+                const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
+                const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
+                const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
+                const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
+{
+    __shared__ StagedTri s_tri[kOccWarps][kOccChunk];
+    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t(*rows)[32] = s_rows[warp];
+    StagedTri *tris = s_tri[warp];
+    unsigned long long tested = 0;
+    int nitems = *(volatile const int *)&ctr->itemCount;
+    if (nitems > itemCapacity) nitems = itemCapacity;
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(&ctr->itemCursor, 1);
+        it = __shfl_sync(kFullWarp, it, 0);
+        if (it >= nitems) break;
+        const int4 item = items[it];
+        const int bin = item.x, fi = item.z;
+        if ((unsigned)bin >= (unsigned)totalBins || (unsigned)fi >= (unsigned)nframes) {
+            if (lane == 0) atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+            continue;
+        }
+        const FrameDesc &fr = frames[fi];
+        const FrameState &st = states[fi];
+        const int S = fr.W * fr.H;
+        const int sLo = bss[bin] + item.y;
+        const int sHi = min(sLo + kItemSamples, bse[bin]);
+        const int tS = bts[bin];
+        const int nT = bte[bin] - tS;
+
+        if (nT <= 0) {
+            for (int k = sLo + lane; k < sHi; k += 32) {
+                const int local = (int)sortedVals[k] - fr.sampleBase;
+                if ((unsigned)local < (unsigned)S) write_zero(fr, local);
+                else atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+            }
+            continue;
+        }
+
+        const int N = fr.light.N;
+        const uint32_t FULL = fr.light.full;
+        const float nm1 = (float)(N - 1);
+        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd);
+        const float esp = fr.esp;
+
+        LaneSample smp;
+        int local = 0;
+        int remaining = 0;
+        uint32_t fullRows = 0u;
+        bool active = false;
+        int next = sLo;
+        // first fill
+        {
+            const int k = next + lane;
+            if (k < sHi) {
+                local = (int)sortedVals[k] - fr.sampleBase;
+                if ((unsigned)local >= (unsigned)S) {
+                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                } else {
+                    active = true;
+                    remaining = nT;
+                    load_sample(smp, fr, st, local);
+                    for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+                }
+            }
+            next += 32;
+        }
+        int cur = 0;  // offset of the next staged chunk within the bin's list
+        while (__any_sync(kFullWarp, active)) {
+            const int m = min(kOccChunk, nT);
+            __syncwarp();
+            if (lane < m) {
+                int off = cur + lane;
+                if (off >= nT) off -= nT;
+                int tri = (int)pairTri[tS + off];
+                if ((unsigned)tri >= (unsigned)totalTris) {
+                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                    tri = 0;
+                }
+                stage_triangle(tris[lane], rec, tri);
+            }
+            __syncwarp();
+            for (int t = 0; t < m; ++t) {
+                if (remaining > 0) {
+                    --remaining;
+                    tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows);
+                    if (fullRows == FULL) remaining = 0;
+                }
+            }
+            cur += m;
+            if (cur >= nT) cur -= nT;
+            // retire finished lanes, then refill them with the item's next samples
+            if (active && remaining == 0) {
+                write_result(fr, local, N, rows, lane);
+                active = false;
+            }
+            const unsigned freeLanes = __ballot_sync(kFullWarp, !active);
+#if FDZB_OCC_REFILL
+            const bool refill = next < sHi && freeLanes;
+#else
+            // refill only once the whole batch is done, restarting at the head of
+            // the (depth-ordered) list
+            const bool refill = next < sHi && freeLanes == kFullWarp;
+            if (refill) cur = 0;
+#endif
+            if (refill) {
+                const int k = next + __popc(freeLanes & lanemask_lt());
+                if (!active && k < sHi) {
+                    local = (int)sortedVals[k] - fr.sampleBase;
+                    if ((unsigned)local >= (unsigned)S) {
+                        atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                    } else {
+                        active = true;
+                        remaining = nT;
+                        fullRows = 0u;
+                        load_sample(smp, fr, st, local);
+                        for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+                    }
+                }
+                next += __popc(freeLanes);
+            }
+        }
+    }
+    unsigned long long t = tested;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFullWarp, t, o);
+    if (lane == 0 && t) atomicAdd(&ctr->pairTests, t);
+}
+
+}  // namespace fdzb

@@ -23,6 +23,7 @@
 //                 sample, OR-accumulating N-bit row masks.
 #include "fdzb_device.cuh"
 #include "fdzb_sort.cuh"
+#include "fdzb_occlusion.cuh"
 
 namespace fdzb {
 
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(kTriThreads)
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
                 int32_t *__restrict__ triCount, unsigned long long *scanStatus, uint32_t epoch,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
-                Counters *ctr)
+                int depthBits, Counters *ctr)
 {
     constexpr int WARPS = kTriThreads / 32;
     __shared__ int s_tile;
@@ -556,12 +557,23 @@ __global__ void __launch_bounds__(kTriThreads)
         if (cnt > 0) {
             unsigned long long pos = s_excl + mine_excl;
             const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
+            // Secondary key (depth order): bucket of the triangle's largest light
+            // depth, ascending bucket = lowest triangles first.  Bucket 0 in
+            // reference order, which keeps the reference's (bin, triangle) order.
+            uint32_t bucket = 0u;
+            if (depthBits > 0) {
+                const float f = states[fi].f;
+                const float maxz = __ldg(&rec[4 * (size_t)g + 1].w);
+                const float q = __fmul_rn(__fsub_rn(f, maxz), __fdiv_rn((float)(1 << depthBits), f));
+                const int bq = (int)fminf(fmaxf(q, 0.0f), (float)((1 << depthBits) - 1));
+                bucket = (uint32_t)bq;
+            }
             for (int j = c.cby; j < c.cey; ++j)
                 for (int i = c.cbx; i < c.cex; ++i) {
                     const int gb = bb + ((j << l2) | i);
                     if (bin_accepts(binStat, gb, c)) {
                         if (pos < (unsigned long long)capacity) {
-                            pkeys[pos] = (uint32_t)gb;
+                            pkeys[pos] = ((uint32_t)gb << depthBits) | bucket;
                             pvals[pos] = (uint32_t)g;
                         }
                         ++pos;
@@ -569,235 +581,6 @@ __global__ void __launch_bounds__(kTriThreads)
                 }
         }
     }
-}
-
-// ---------------------------------------------------------------------------
-// k_items: one thread per bin; a bin with n samples yields ceil(n/32) warp items.
-// ---------------------------------------------------------------------------
-__global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
-                        const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
-                        const int *__restrict__ binBases, int nframes, int totalBins,
-                        int4 *__restrict__ items, int capacity, Counters *ctr)
-{
-    const int lane = threadIdx.x & 31;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < totalBins;
-         base += gridDim.x * blockDim.x) {
-        const int b = base + lane;
-        int n = 0;
-        if (b < totalBins) n = (bse[b] - bss[b] + 31) >> 5;
-        int x = n;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(kFullWarp, x, o);
-            if (lane >= o) x += y;
-        }
-        const int tot = __shfl_sync(kFullWarp, x, 31);
-        int wbase = 0;
-        if (lane == 0 && tot) wbase = atomicAdd(&ctr->itemCount, tot);
-        wbase = __shfl_sync(kFullWarp, wbase, 0);
-        if (n) {
-            const int f = frame_of(binBases, nframes, b);
-            const int hasTris = bte[b] > bts[b] ? 1 : 0;
-            for (int k = 0; k < n; ++k) {
-                const int slot = wbase + x - n + k;
-                if (slot < capacity) items[slot] = make_int4(b, 32 * k, f, hasTris);
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Occlusion.  Per sample/triangle pair, exactly the reference arithmetic of
-// K/Step5_2_shadowCalPerSample.inl:120-222.  A, B, C are formed with the
-// unflipped light vectors and negated when dir < 0: with round-to-nearest,
-// dot(n, -t) == -dot(n, t) except for the sign of an exact zero, which no later
-// comparison, product or sum can observe.
-// ---------------------------------------------------------------------------
-
-// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(N-1) precomputed (same
-// product) and the result limited to the N-bit light grid.
-__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full)
-{
-    const bool f1 = D >= 0.0f;
-    const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
-    if (f1 && f2) return full;
-    if (!f1 && !f2) return 0u;
-    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
-    const int k = __float2int_rz(ceilf(q));
-    uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
-    m -= 1u;
-    if (!f1) m = ~m;
-    return m & full;
-}
-
-// K/Step5_2_shadowCal.inl:213-222
-__device__ __forceinline__ bool point_in_tri(f3 A, f3 B, f3 C, f3 P)
-{
-    const f3 N1 = cross3(sub3(B, A), sub3(P, B));
-    const f3 N2 = cross3(sub3(C, B), sub3(P, C));
-    if (dot3(N1, N2) < 0.0f) return false;
-    const f3 N3 = cross3(sub3(A, C), sub3(P, A));
-    if (dot3(N2, N3) < 0.0f) return false;
-    return true;
-}
-
-constexpr int kOccWarps = 4;
-constexpr int kOccThreads = kOccWarps * 32;
-
-__global__ void __launch_bounds__(kOccThreads)
-    k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
-                const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
-                const uint32_t *__restrict__ sortedVals,
-                const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
-                const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
-                const uint32_t *__restrict__ pairTri, const float4 *__restrict__ rec, int totalTris,
-                int totalBins, int nframes)
-{
-    __shared__ float4 s_tri[kOccWarps][32][4];
-    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t(*rows)[32] = s_rows[warp];
-    unsigned long long tested = 0;
-    int nitems = *(volatile const int *)&ctr->itemCount;
-    if (nitems > itemCapacity) nitems = itemCapacity;
-
-    for (;;) {
-        int it = 0;
-        if (lane == 0) it = atomicAdd(&ctr->itemCursor, 1);
-        it = __shfl_sync(kFullWarp, it, 0);
-        if (it >= nitems) break;
-        const int4 item = items[it];
-        const int bin = item.x, fi = item.z;
-        if ((unsigned)bin >= (unsigned)totalBins || (unsigned)fi >= (unsigned)nframes) {
-            if (lane == 0) atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
-            continue;
-        }
-        const FrameDesc &fr = frames[fi];
-        const FrameState &st = states[fi];
-        const int N = fr.light.N;
-        const uint32_t FULL = fr.light.full;
-        const float nm1 = (float)(N - 1);
-        const int sLo = bss[bin] + item.y;
-        const int sHi = min(sLo + 32, bse[bin]);
-        const int k = sLo + lane;
-        const bool active = k < sHi;
-
-        f3 Q = mk3(0.f, 0.f, 0.f);
-        float spx = 0.f, spy = 0.f, spz = 0.f, spw = 0.f, spZ = 0.f;
-        int local = 0;
-        if (active) {
-            local = (int)sortedVals[k] - fr.sampleBase;
-            if ((unsigned)local >= (unsigned)(fr.W * fr.H)) {
-                atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
-                local = 0;
-            }
-            const float4 P = __ldg(fr.pos + local);
-            Q = mk3(P.x, P.y, P.z);
-            const f3 r = light_project(fr.light.mat, Q);
-            spx = r.x;
-            spy = r.y;
-            spz = __fsub_rn(__fadd_rn(r.x, __fdiv_rn(fr.light.RF[0], r.z)), st.subx);
-            spw = __fsub_rn(__fadd_rn(r.y, __fdiv_rn(fr.light.RF[1], r.z)), st.suby);
-            spZ = r.z;
-        }
-        for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
-        uint32_t fullRows = 0u;
-        bool done = !active;
-
-        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd);
-        const f3 L0Q = sub3(ld3(fr.light.ur), Q);
-        const float esp = fr.esp;
-        const int tS = bts[bin], tE = bte[bin];
-        for (int c = tS; c < tE; c += 32) {
-            if (__all_sync(kFullWarp, done)) break;
-            const int m = min(32, tE - c);
-            __syncwarp();
-            if (lane < m) {
-                int tri = (int)pairTri[c + lane];
-                if ((unsigned)tri >= (unsigned)totalTris) {
-                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
-                    tri = 0;
-                }
-                const float4 *rp = rec + 4 * (size_t)tri;
-                s_tri[warp][lane][0] = __ldg(rp);
-                s_tri[warp][lane][1] = __ldg(rp + 1);
-                s_tri[warp][lane][2] = __ldg(rp + 2);
-                s_tri[warp][lane][3] = __ldg(rp + 3);
-            }
-            __syncwarp();
-            for (int t = 0; t < m; ++t) {
-                if (done) continue;
-                const float4 q3 = s_tri[warp][t][3];
-                const float4 q0 = s_tri[warp][t][0];
-                if (!(q3.x <= spx && q3.y <= spy && spz <= q3.z && spw <= q3.w && q0.w <= spZ))
-                    continue;
-                ++tested;
-                const float4 q1 = s_tri[warp][t][1];
-                const float4 q2 = s_tri[warp][t][2];
-                const f3 v0 = mk3(q0.x, q0.y, q0.z), v1 = mk3(q1.x, q1.y, q1.z),
-                         v2 = mk3(q2.x, q2.y, q2.z);
-                const f3 n = cross3(sub3(v1, v0), sub3(v2, v1));
-                const float dir = dot3(sub3(Q, v0), n);
-                if (fabsf(dir) < esp && point_in_tri(v0, v1, v2, Q)) continue;
-                const f3 n0 = cross3(sub3(v1, Q), sub3(v0, v1));
-                const f3 n1 = cross3(sub3(v2, Q), sub3(v1, v2));
-                const f3 n2 = cross3(sub3(v0, Q), sub3(v2, v0));
-                float A0 = dot3(n0, xd), B0 = dot3(n0, yd), C0 = dot3(n0, L0Q);
-                float A1 = dot3(n1, xd), B1 = dot3(n1, yd), C1 = dot3(n1, L0Q);
-                float A2 = dot3(n2, xd), B2 = dot3(n2, yd), C2 = dot3(n2, L0Q);
-                if (dir < 0.0f) {
-                    A0 = -A0; B0 = -B0; C0 = -C0;
-                    A1 = -A1; B1 = -B1; C1 = -C1;
-                    A2 = -A2; B2 = -B2; C2 = -C2;
-                }
-                const float An0 = __fmul_rn(A0, nm1), An1 = __fmul_rn(A1, nm1), An2 = __fmul_rn(A2, nm1);
-                const float Bn0 = __fmul_rn(B0, nm1), Bn1 = __fmul_rn(B1, nm1), Bn2 = __fmul_rn(B2, nm1);
-                const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL);
-                const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL);
-                const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL);
-                uint32_t vr = N0 & N1 & N2 & ~fullRows;
-                while (vr) {
-                    const int r = __ffs(vr) - 1;
-                    vr &= vr - 1u;
-                    const float fr_ = (float)r;
-                    const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr_), C0), Bn0, B0, FULL);
-                    const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr_), C1), Bn1, B1, FULL);
-                    const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr_), C2), Bn2, B2, FULL);
-                    const uint32_t nv = rows[r][lane] | (M0 & M1 & M2);
-                    rows[r][lane] = nv;
-                    if (nv == FULL) fullRows |= 1u << r;
-                }
-                if (fullRows == FULL) done = true;
-            }
-        }
-        if (active) {
-            int cnt = 0;
-            for (int r = 0; r < N; ++r) cnt += __popc(rows[r][lane]);
-            fr.shadow[local] = __fdiv_rn((float)cnt, (float)(N * N));
-            if (fr.masks) {
-                uint32_t *mo = fr.masks + (size_t)local * fr.maskWords;
-                uint32_t acc = 0u;
-                int bit = 0, wi = 0;
-                for (int r = 0; r < N; ++r) {
-                    const uint32_t v = rows[r][lane];
-                    acc |= v << bit;
-                    const int nb = bit + N;
-                    if (nb >= 32) {
-                        mo[wi++] = acc;
-                        acc = (nb > 32) ? (v >> (32 - bit)) : 0u;
-                        bit = nb - 32;
-                    } else {
-                        bit = nb;
-                    }
-                }
-                if (bit > 0) mo[wi] = acc;
-            }
-        }
-    }
-    unsigned long long t = tested;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFullWarp, t, o);
-    if (lane == 0 && t) atomicAdd(&ctr->pairTests, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -920,7 +703,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     uint32_t *sk = (b.samplePasses & 1) ? b.keysB : b.keysA;
     uint32_t *sv = (b.samplePasses & 1) ? b.valsB : b.valsA;
     k_find_start_end<<<grid_for(b.totalSamples, 256, sm * 8), 256, 0, s>>>(
-        sk, nullptr, b.totalSamples, b.totalSamples, b.binSampleStart, b.binSampleEnd,
+        sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
         (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
 
     {
@@ -929,7 +712,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epoch, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 b.counters);
+                                                 b.depthBits, b.counters);
     }
     if (b.dbgPKeys) {
         cudaMemcpyAsync(b.dbgPKeys, b.pkeysA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
@@ -940,7 +723,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
     uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
-        pk, &b.counters->pairCount, 0, b.pairCapacity, b.binTriStart, b.binTriEnd,
+        pk, &b.counters->pairCount, 0, b.pairCapacity, b.depthBits, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
         b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,

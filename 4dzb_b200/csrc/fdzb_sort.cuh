@@ -170,14 +170,15 @@ __global__ void __launch_bounds__(kSortThreads)
 
 // Segment bounds of a sorted key array (K/binRaster.inl:5-33): start[key] = first
 // index, end[key] = last index + 1, for keys present (arrays pre-zeroed).
+// The segment key is key >> shift (low bits may carry a secondary sort key).
 __global__ void k_find_start_end(const uint32_t *__restrict__ keys, const int *n_dev, int n_static,
-                                 int cap, int32_t *__restrict__ start, int32_t *__restrict__ end,
-                                 uint32_t nslots, int *err)
+                                 int cap, int shift, int32_t *__restrict__ start,
+                                 int32_t *__restrict__ end, uint32_t nslots, int *err)
 {
     const int n = sort_count(n_dev, n_static, cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        const uint32_t kp = i > 0 ? keys[i - 1] : 0u;
+        const uint32_t k = keys[i] >> shift;
+        const uint32_t kp = i > 0 ? (keys[i - 1] >> shift) : 0u;
         if (k >= nslots || kp >= nslots) {
             atomicOr(err, (int)ERR_INTERNAL);
             continue;

@@ -179,6 +179,17 @@ int fdzb_ctx_export(fdzb_ctx *ctx, int what, void *dst, size_t bytes);
  * sort.  Off by default. */
 int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
 
+/* Order of each bin's triangle list (no counterpart in the reference, whose
+ * thrust::sort_by_key leaves ascending triangle ids inside a bin,
+ * K/Step4_RasterizeTriangleToBin.inl:220-223).  Masks and shadows are identical in
+ * both orders -- a sample's mask is the OR over its bin's triangles -- only the
+ * number of pair tests before a sample's light is fully blocked changes.
+ *   FDZB_TRI_ORDER_REFERENCE: the reference's order (parity of the sorted lists);
+ *   FDZB_TRI_ORDER_DEPTH (default): lowest triangles first. */
+#define FDZB_TRI_ORDER_REFERENCE 0
+#define FDZB_TRI_ORDER_DEPTH     1
+int fdzb_ctx_set_tri_order(fdzb_ctx *ctx, int order);
+
 /* Host-side light setup only (FS/api.cpp:303-400): fills the 16-float
  * column-major light projection, RectangleFactor and the four light corners
  * (upRight, upLeft, downLeft, downRight), x_delt and y_delt. */

@@ -117,8 +117,10 @@ void orc_light_setup(const orc_light_desc *d, orc_light *L)
     MV[3][2] = dot3(fw, ur);
 
     /* infinitePerspectiveRH(120 [radians], 1, 0.1) */
+    /* tan(fovy/2) correctly rounded to binary32 (double evaluation); glibc's
+     * tanf(60.0f) is one ulp away from it. */
     float fovy = 120.0f, aspect = 1.0f, zNear = 0.1f;
-    float range = tanf(fovy / 2.0f) * zNear;
+    float range = (float)tan((double)(fovy / 2.0f)) * zNear;
     float left = -range * aspect, rightp = range * aspect, bottom = -range, topp = range;
     float P[4][4];
     memset(P, 0, sizeof(P));
@@ -190,12 +192,15 @@ static inline int f2i_sat(float q)
 }
 
 /* K/Step5_2_shadowCalPerSample.inl:14-33, unmasked (bits >= N may be set). */
+static _Thread_local int64_t tl_partial = 0, tl_rows = 0;
+
 static inline uint32_t row_mask_raw(float D, float s, unsigned nm1, uint32_t full)
 {
     int f1 = (D >= 0.0f);
     int f2 = (s * (float)nm1 + D >= 0.0f);
     if (f1 && f2) return full;
     if (!f1 && !f2) return 0u;
+    ++tl_partial;
     float q = (-1.0f * D) / s;
     uint32_t m = shl1(f2i_sat(ceilf(q)));
     m -= 1u;
@@ -250,6 +255,7 @@ static inline int pair_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint32_t 
     while (rows) {
         int r = __builtin_ctz(rows);
         rows &= rows - 1u;
+        ++tl_rows;
         uint32_t M0 = row_mask_raw(A0 * (float)r + C0, B0, nm1, FULL);
         uint32_t M1 = row_mask_raw(A1 * (float)r + C1, B1, nm1, FULL);
         uint32_t M2 = row_mask_raw(A2 * (float)r + C2, B2, nm1, FULL);
@@ -321,6 +327,7 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
     o->state = 0;
     o->valid_samples = o->valid_tris = o->num_pairs = o->pair_overflow = 0;
     o->pairs_tested = o->quirk_rows_beyond_n = o->quirk_high_bits = o->quirk_key_range = 0;
+    o->rows_evaluated = o->partial_masks = 0;
     o->view_log2up = ceil_log2_int(W);
     const int log2up = o->view_log2up;
     const int Wb = in->bins, Hb = in->bins;
@@ -507,10 +514,15 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
                     float cx = (e[0] + b[0]) / 2.0f, cy = (e[1] + b[1]) / 2.0f;
                     int bx = (int)floorf((cx - Bx) * fx);
                     int by = (int)floorf((cy - By) * fy);
-                    if (bx < 0 || bx >= Wb || by < 0 || by >= Hb) o->quirk_key_range++;
-                    key = (by << blog2) | bx;
-                    if (key < 0 || key > NB) key = NB; /* out-of-grid guard */
-                    ++nv;
+                    if (bx < 0 || bx >= Wb || by < 0 || by >= Hb) {
+                        /* A centre on the far edge of the light plane rounds to bin
+                         * Wb (or Hb); the reference then forms an aliased or
+                         * out-of-range key.  Such samples stay unbinned here. */
+                        o->quirk_key_range++;
+                    } else {
+                        key = (by << blog2) | bx;
+                        ++nv;
+                    }
                 }
                 keys[s] = key;
                 vals[s] = (y << log2up) | x;
@@ -615,9 +627,13 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
         c.full = L->fullBits;
         c.esp = in->esp;
         const int Sv = o->valid_samples;
-        int64_t tested = 0, qrows = 0, qhigh = 0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : tested, qrows, qhigh)
+        const int stride = in->occ_stride > 1 ? in->occ_stride : 1;
+        int64_t tested = 0, qrows = 0, qhigh = 0, nrows = 0, npart = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : tested, qrows, qhigh, nrows, npart)
         for (int k = 0; k < Sv; ++k) {
+            if (k % stride) continue;
+            tl_rows = 0;
+            tl_partial = 0;
             int sv = svals[k], bin = skeys[k];
             size_t s = (size_t)(sv >> log2up) * W + (sv & ((1 << log2up) - 1));
             v3 Q = ld3(in->pos + 4 * s);
@@ -636,6 +652,8 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
                 pair_test(&c, Q, t, rows, &full_rows, &qrows, &high);
             }
             qhigh += high;
+            nrows += tl_rows;
+            npart += tl_partial;
             int cnt = 0;
             for (int i = 0; i < N; ++i) cnt += __builtin_popcount(rows[i]);
             if (o->shadow) o->shadow[s] = (float)cnt / (float)(N * N);
@@ -644,6 +662,8 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
         o->pairs_tested = tested;
         o->quirk_rows_beyond_n = qrows;
         o->quirk_high_bits = qhigh;
+        o->rows_evaluated = nrows;
+        o->partial_masks = npart;
     }
 
 free2:

@@ -62,6 +62,8 @@ typedef struct {
     float esp;
     const orc_light *light;
     int32_t nthreads;            /* <= 0: OpenMP default */
+    int32_t occ_stride;          /* occlusion only for sorted samples k with k % occ_stride == 0
+                                    (<= 1: all); others keep mask 0 / shadow 0 */
 } orc_frame_in;
 
 typedef struct {
@@ -76,6 +78,8 @@ typedef struct {
     int64_t quirk_rows_beyond_n; /* pairs whose row filter selects rows >= N (reference UB) */
     int64_t quirk_high_bits;     /* samples whose reference mask would hold bits >= N */
     int64_t quirk_key_range;     /* samples whose bin x/y fell outside the grid */
+    int64_t rows_evaluated;      /* light-grid rows evaluated (3 row masks each) */
+    int64_t partial_masks;       /* row masks that needed the ceil(-D/B) threshold */
     /* arrays, caller-allocated; NULL skips the copy */
     int32_t *keys, *vals;                     /* [S] position order */
     int32_t *sorted_keys, *sorted_vals;       /* [S] */

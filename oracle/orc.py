@@ -39,7 +39,8 @@ class FrameIn(ctypes.Structure):
     _fields_ = [("W", ctypes.c_int32), ("H", ctypes.c_int32), ("pos", f32p), ("nrm", f32p),
                 ("vtx", f32p), ("vtx_stride_floats", ctypes.c_int32), ("V", ctypes.c_int32),
                 ("idx", i32p), ("T", ctypes.c_int32), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
-                ("esp", ctypes.c_float), ("light", ctypes.POINTER(Light)), ("nthreads", ctypes.c_int32)]
+                ("esp", ctypes.c_float), ("light", ctypes.POINTER(Light)), ("nthreads", ctypes.c_int32),
+                ("occ_stride", ctypes.c_int32)]
 
 
 class FrameOut(ctypes.Structure):
@@ -52,6 +53,7 @@ class FrameOut(ctypes.Structure):
                 ("num_pairs", ctypes.c_int32), ("pair_overflow", ctypes.c_int32),
                 ("pairs_tested", ctypes.c_int64), ("quirk_rows_beyond_n", ctypes.c_int64),
                 ("quirk_high_bits", ctypes.c_int64), ("quirk_key_range", ctypes.c_int64),
+                ("rows_evaluated", ctypes.c_int64), ("partial_masks", ctypes.c_int64),
                 ("keys", i32p), ("vals", i32p), ("sorted_keys", i32p), ("sorted_vals", i32p),
                 ("bin_sample_start", i32p), ("bin_sample_end", i32p), ("bin_maxz", f32p),
                 ("bin_range", f32p), ("tri_aabb", f32p), ("tri_count", i32p),
@@ -126,7 +128,7 @@ class OrcFrame:
     _keep: list
 
 
-def _frame_in(scene, light: Light, nthreads: int, keep: list) -> FrameIn:
+def _frame_in(scene, light: Light, nthreads: int, keep: list, occ_stride: int = 1) -> FrameIn:
     pos = np.ascontiguousarray(scene.pos, dtype=np.float32)
     nrm = np.ascontiguousarray(scene.nrm, dtype=np.float32)
     vtx = np.ascontiguousarray(scene.vtx, dtype=np.float32)
@@ -145,15 +147,17 @@ def _frame_in(scene, light: Light, nthreads: int, keep: list) -> FrameIn:
     fi.esp = scene.esp
     fi.light = ctypes.pointer(light)
     fi.nthreads = nthreads
+    fi.occ_stride = occ_stride
     return fi
 
 
-def frame(scene, nthreads: int = 0, pair_capacity: int | None = None) -> OrcFrame:
-    """Run the FP32 restatement (O2) on a scenes.Scene."""
+def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride: int = 1) -> OrcFrame:
+    """Run the FP32 restatement (O2) on a scenes.Scene.  occ_stride > 1 runs the
+    occlusion stage only for every occ_stride-th sorted valid sample."""
     lib = load()
     keep: list = []
     light = light_setup(scene.light)
-    fi = _frame_in(scene, light, nthreads, keep)
+    fi = _frame_in(scene, light, nthreads, keep, occ_stride)
     S, T, NB = scene.W * scene.H, scene.T, scene.bins * scene.bins
     words = mask_words(scene.light.n)
     # first a counting run to size the pair buffers
@@ -194,6 +198,14 @@ def frame(scene, nthreads: int = 0, pair_capacity: int | None = None) -> OrcFram
         out[k] = arrs[k][:P].copy()
     out["tri_aabb"] = arrs["tri_aabb"][:8 * T]
     out["tri_count"] = arrs["tri_count"][:T]
+    stride = max(occ_stride, 1)
+    Sv = fo.valid_samples
+    if fo.state == 2:
+        sv = out["sorted_vals"][:Sv:stride]
+        l2 = fo.view_log2up
+        out["occ_samples"] = ((sv >> l2) * scene.W + (sv & ((1 << l2) - 1))).astype(np.int64)
+    else:
+        out["occ_samples"] = np.zeros(0, np.int64)
     return OrcFrame(scalars=sc, arrays=out, _in=fi, _out=fo, _keep=keep)
 
 

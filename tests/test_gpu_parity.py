@@ -4,35 +4,43 @@ Bar: bin keys, sorted sample order, per-bin segments and statistics, triangle
 footprints, per-triangle bin counts, triangle/bin pairs (before and after the
 sort), per-bin triangle segments, N^2-bit masks and shadow values all equal the
 FP32 restatement bit for bit (both sides compute with unfused IEEE binary32
-operations in the reference's order).
+operations in the reference's order).  In depth order the per-bin triangle
+lists are a permutation of the reference's (checked as sets); masks and shadows
+must still match bit for bit.
 """
 import numpy as np
 import pytest
 
+import oracle
 from tests import parity
 
 pytestmark = pytest.mark.gpu
 
+ORDERS = [0, 1]
 
-def _check(scene):
-    errs = parity.compare(scene)
+
+def _check(scene, tri_order=0, occ_stride=1):
+    orc = oracle.frame(scene, occ_stride=occ_stride)
+    errs = parity.compare(scene, gpu=parity.run_gpu(scene, tri_order=tri_order), orc=orc)
     assert not errs, "\n".join(errs)
 
 
 @pytest.mark.parametrize("cull", [False, True])
-def test_small_preset(cuda_ok, scenes, cull):
-    _check(scenes.preset("small", cull=cull))
+@pytest.mark.parametrize("order", ORDERS)
+def test_small_preset(cuda_ok, scenes, cull, order):
+    _check(scenes.preset("small", cull=cull), order)
 
 
-@pytest.mark.parametrize("n,bins", [(8, 16), (16, 32), (32, 64), (4, 8), (12, 32), (1, 16)])
+@pytest.mark.parametrize("n,bins", [(8, 16), (16, 32), (32, 64), (4, 8), (12, 32), (1, 16), (2, 1)])
 def test_light_grid_and_bins(cuda_ok, scenes, n, bins):
-    _check(scenes.make_scene(160, 128, 700, n=n, bins=bins, seed=7, name=f"n{n}b{bins}"))
+    _check(scenes.make_scene(160, 128, 700, n=n, bins=bins, seed=7, name=f"n{n}b{bins}"), 1)
 
 
-def test_non_power_of_two_view(cuda_ok, scenes):
+@pytest.mark.parametrize("order", ORDERS)
+def test_non_power_of_two_view(cuda_ok, scenes, order):
     # 1920-wide views hit the reference's padded output index (y<<ceil(log2 W)|x);
     # the library writes y*W+x.
-    _check(scenes.make_scene(300, 170, 2000, n=16, bins=64, seed=11, sigma=0.1))
+    _check(scenes.make_scene(300, 170, 2000, n=16, bins=64, seed=11, sigma=0.1), order)
 
 
 def test_background_samples(cuda_ok, scenes):
@@ -40,14 +48,21 @@ def test_background_samples(cuda_ok, scenes):
     rng = np.random.default_rng(0)
     bg = rng.random(s.S) < 0.3
     s.pos[bg, 0] = np.nan
-    _check(s)
+    _check(s, 1)
 
 
 def test_backfacing_samples(cuda_ok, scenes):
     s = scenes.make_scene(128, 128, 800, n=8, bins=16, seed=9)
     s.nrm[: s.S // 3, :3] *= -1.0   # a third of the receiver faces away from the light
-    _check(s)
+    _check(s, 1)
 
 
-def test_medium_scene(cuda_ok, scenes):
-    _check(scenes.make_scene(640, 480, 20000, n=16, bins=64, seed=21, sigma=0.1))
+@pytest.mark.parametrize("order", ORDERS)
+def test_medium_scene(cuda_ok, scenes, order):
+    _check(scenes.make_scene(640, 480, 20000, n=16, bins=64, seed=21, sigma=0.1), order)
+
+
+def test_hd_preset_sampled(cuda_ok, scenes):
+    """1920x1080 x 200k triangles x 16x16 light, 128^2 bins: every stage exact;
+    masks checked on every 97th binned sample."""
+    _check(scenes.preset("hd"), 1, occ_stride=97)

@@ -1,0 +1,176 @@
+"""CPU tests of the oracle (the checker) and of the scene generator.
+
+Hand-derived cases pin the restatement's semantics; the FP64 exhaustive oracle
+and the unbinned FP32 loop cross-check the binned FP32 pipeline.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+
+def _flat_receiver(scenes, W, H, z=0.0, half=1.0):
+    """W x H samples on the plane z over [-half, half]^2, normals +z."""
+    xs = -half + (np.arange(W) + 0.5) * (2 * half / W)
+    ys = -half + (np.arange(H) + 0.5) * (2 * half / H)
+    X, Y = np.meshgrid(xs, ys)
+    pos = np.ones((W * H, 4), np.float32)
+    pos[:, 0], pos[:, 1], pos[:, 2] = X.ravel(), Y.ravel(), z
+    nrm = np.zeros((W * H, 4), np.float32)
+    nrm[:, 2] = 1.0
+    return pos, nrm
+
+
+def _scene(scenes, tris, W=16, H=16, n=8, bins=8, z=0.0, cull=False, esp=1e-3):
+    pos, nrm = _flat_receiver(scenes, W, H, z)
+    tris = np.asarray(tris, np.float32).reshape(-1, 3, 3)
+    vtx = np.ones((3 * len(tris), 4), np.float32)
+    vtx[:, :3] = tris.reshape(-1, 3)
+    idx = np.arange(3 * len(tris), dtype=np.int32).reshape(-1, 3)
+    return scenes.Scene(W=W, H=H, pos=pos, nrm=nrm, vtx=vtx, idx=idx, light=scenes.Light(n=n),
+                        bins=bins, esp=esp, cull=cull, name="hand")
+
+
+BIG = [[-20, -20, 3], [20, -20, 3], [0, 30, 3]]   # covers every sample's view of the light
+
+
+def test_generator_is_deterministic(scenes):
+    a = scenes.preset("small")
+    b = scenes.preset("small")
+    for k in ("pos", "nrm", "vtx", "idx"):
+        assert np.array_equal(getattr(a, k), getattr(b, k))
+    c = scenes.make_scene(256, 256, 1024, n=8, bins=32, seed=99)
+    assert not np.array_equal(a.vtx, c.vtx)
+    assert a.pos.dtype == np.float32 and a.pos.shape == (65536, 4)
+    assert np.all(a.idx == np.arange(3 * 1024).reshape(1024, 3))
+    # receiver on z = 0.3 sin x cos y (+1e-4 along the normal)
+    x, y, z = a.pos[:, 0].astype(np.float64), a.pos[:, 1], a.pos[:, 2]
+    assert np.max(np.abs(z - 0.3 * np.sin(x) * np.cos(y))) < 2e-4
+    cz = a.vtx[:, 2].reshape(-1, 3).mean(axis=1)
+    assert cz.min() > 0.0 and cz.max() < 3.6
+
+
+def test_one_big_triangle_blocks_the_whole_light(scenes):
+    s = _scene(scenes, BIG)
+    fr = oracle.frame(s)
+    assert fr.scalars["state"] == 2
+    sh = fr.arrays["shadow"]
+    # interior samples are fully occluded; samples whose rectangle touches the
+    # light-plane border get no pair (strict bin test on the clamped AABB)
+    assert (sh == 1.0).mean() > 0.7
+    assert set(np.unique(sh)) <= {0.0, 1.0}
+    m = fr.arrays["masks"].reshape(s.S, -1)
+    assert np.all(m[sh == 1.0] == 0xFFFFFFFF)
+    # FP64 exhaustive agrees for every sample the binned pipeline tested
+    ids = np.flatnonzero(sh == 1.0).astype(np.int32)
+    m64, _ = oracle.exhaustive_fp64(s, fr, ids)
+    assert np.array_equal(m64, m[ids])
+
+
+def test_triangle_off_to_the_side_gives_no_light_plane(scenes):
+    s = _scene(scenes, [[50, 50, 3], [60, 50, 3], [55, 60, 3]])
+    fr = oracle.frame(s)
+    assert fr.scalars["state"] == 1       # light plane empty (FS/.../Step2_3_defineFDbuffer.inl:62)
+    assert np.all(fr.arrays["shadow"] == 0)
+
+
+def test_back_facing_samples_are_fully_shadowed(scenes):
+    s = _scene(scenes, BIG)
+    s.nrm[:, 2] = -1.0
+    fr = oracle.frame(s)
+    assert fr.scalars["state"] == 1       # no front-facing sample
+    assert np.all(fr.arrays["shadow"] == 1.0)
+    assert np.all(fr.arrays["masks"] == 0xFFFFFFFF)
+
+
+def test_nothing_in_front_of_the_light(scenes):
+    s = _scene(scenes, [[-1, -1, 9], [1, -1, 9], [0, 1, 9]], z=7.0)  # all behind the light plane
+    fr = oracle.frame(s)
+    assert fr.scalars["state"] == 0
+    assert np.all(fr.arrays["shadow"] == 0)
+
+
+def test_coplanar_triangle_containing_the_sample_is_skipped(scenes):
+    """|dir| < esp and point in triangle: the reference skips the pair
+    (K/Step5_2_shadowCalPerSample.inl:134-135)."""
+    tri = [[-20, -20, 0.0], [20, -20, 0.0], [0, 30, 0.0]]
+    fr = oracle.frame(_scene(scenes, tri + BIG[:0], z=0.0))
+    lifted = oracle.frame(_scene(scenes, [[-20, -20, 0.01], [20, -20, 0.01], [0, 30, 0.01]], z=0.0))
+    if fr.scalars["state"] == 2:
+        assert np.all(fr.arrays["shadow"] == 0)
+    assert (lifted.arrays["shadow"] == 1).any()
+
+
+def test_full_rows_stop_the_triangle_loop(scenes):
+    one = oracle.frame(_scene(scenes, BIG))
+    two = oracle.frame(_scene(scenes, BIG + BIG))
+    assert np.array_equal(one.arrays["masks"], two.arrays["masks"])
+    assert one.scalars["pairs_tested"] == two.scalars["pairs_tested"]   # 2nd copy never tested
+
+
+def test_light_sample_exactly_on_an_edge_is_occluded(scenes):
+    """Edge plane through the sample and light column x = 0.125 (row i = 3 for
+    N = 8: x = 0.875 - 0.25 i); dyadic coordinates make E = 0 exactly, and the
+    row mask keeps E >= 0 (K/Step5_2_shadowCalPerSample.inl:19-31)."""
+    W = H = 8
+    tri = [[0.0625, -40.0, 3.0], [0.0625, 40.0, 3.0], [-40.0, 0.0, 3.0]]
+    s = _scene(scenes, tri, W=W, H=H, bins=4)
+    s.pos[:] = 0.0
+    s.pos[:, 3] = 1.0
+    # spread the receiver so the light plane is not a single rectangle
+    xs = (np.arange(W * H) % W - W / 2) * 0.0
+    s.pos[:, 0] = xs
+    fr = oracle.frame(s)
+    if fr.scalars["state"] != 2:
+        pytest.skip("degenerate light plane")
+    ids = np.arange(s.S, dtype=np.int32)
+    m64, dist = oracle.exhaustive_fp64(s, fr, ids)
+    m32, _ = oracle.exhaustive_fp32(s, fr, ids)
+    assert np.array_equal(m32, m64)
+
+
+@pytest.mark.parametrize("cull", [False, True])
+def test_binned_fp32_equals_unbinned_fp32(scenes, cull):
+    """The bin filter and AABB pre-cull only drop pairs that cannot occlude, so
+    the binned pipeline equals the exhaustive FP32 loop on the same samples."""
+    s = scenes.preset("small", cull=cull)
+    fr = oracle.frame(s)
+    rng = np.random.default_rng(1)
+    ids = rng.choice(s.S, 512, replace=False).astype(np.int32)
+    m32, n = oracle.exhaustive_fp32(s, fr, ids)
+    binned = fr.arrays["masks"].reshape(s.S, -1)[ids]
+    diff = np.flatnonzero((m32 != binned).any(axis=1))
+    assert diff.size <= 1, f"{diff.size} samples differ"
+    assert n > 0
+
+
+def test_fp32_masks_within_tolerance_of_fp64(scenes):
+    """O2 (FP32, closed-form row masks) vs O3 (FP64 per light sample): at most
+    1e-5 of the mask bits may differ, and only at light samples within a small
+    distance (light-grid units) of a projected edge."""
+    s = scenes.preset("small")
+    fr = oracle.frame(s)
+    rng = np.random.default_rng(2)
+    ids = rng.choice(s.S, 2048, replace=False).astype(np.int32)
+    m64, dist = oracle.exhaustive_fp64(s, fr, ids)
+    m32 = fr.arrays["masks"].reshape(s.S, -1)[ids]
+    N = s.light.n
+    bits32 = np.unpackbits(m32.view(np.uint8), bitorder="little").reshape(len(ids), -1)[:, :N * N]
+    bits64 = np.unpackbits(m64.view(np.uint8), bitorder="little").reshape(len(ids), -1)[:, :N * N]
+    flip = bits32 != bits64
+    assert flip.mean() <= 1e-5
+    if flip.any():
+        assert dist[flip].max() <= 1e-3
+    vis32 = 1 - bits32.mean(axis=1)
+    vis64 = 1 - bits64.mean(axis=1)
+    assert np.abs(vis32 - vis64).max() <= 2.0 / (N * N)
+
+
+def test_sampled_occlusion_matches_full_run(scenes):
+    s = scenes.preset("small")
+    full = oracle.frame(s)
+    part = oracle.frame(s, occ_stride=7)
+    idx = part.arrays["occ_samples"]
+    assert len(idx) == (full.scalars["valid_samples"] + 6) // 7
+    assert np.array_equal(part.arrays["shadow"][idx], full.arrays["shadow"][idx])
+    assert np.array_equal(part.arrays["sorted_keys"], full.arrays["sorted_keys"])
