@@ -50,8 +50,10 @@ EXPORTED = [
     "fdzb_ctx_set_scene_params", "fdzb_ctx_set_area_light", "fdzb_ctx_move_model",
     "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
     "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_ctx_set_tri_order", "fdzb_light_setup",
-    "fdzb_version",
+    "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate",
 ]
+
+STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
 
 TRI_ORDER_REFERENCE = 0
 TRI_ORDER_DEPTH = 1
@@ -91,7 +93,10 @@ class FrameStats(ctypes.Structure):
                 ("lp_begin", ctypes.c_float * 3), ("lp_end", ctypes.c_float * 3),
                 ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 6),
                 ("model_aabb", ctypes.c_float * 6), ("replans", ctypes.c_int32),
-                ("quirk_key_range", ctypes.c_int32)]
+                ("quirk_key_range", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
+                ("pad0", ctypes.c_int32), ("rows_evaluated", ctypes.c_int64),
+                ("partial_masks", ctypes.c_int64), ("stage_ms", ctypes.c_float * 5),
+                ("pad1", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         out = {}
@@ -139,7 +144,8 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_launch": ([vp, P(ctypes.c_float)], i32), "fdzb_ctx_launch_async": ([vp], i32),
         "fdzb_ctx_sync": ([vp], i32), "fdzb_ctx_get_stats": ([vp, P(FrameStats)], i32),
         "fdzb_ctx_export": ([vp, i32, vp, sz], i32), "fdzb_ctx_set_debug": ([vp, i32], i32),
-        "fdzb_ctx_set_tri_order": ([vp, i32], i32),
+        "fdzb_ctx_set_tri_order": ([vp, i32], i32), "fdzb_ctx_set_profiling": ([vp, i32], i32),
+        "fdzb_measure_alu_rate": ([P(ctypes.c_double)], i32),
         "fdzb_light_setup": ([P(AreaLightDesc), P(ctypes.c_float), P(ctypes.c_float),
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
@@ -182,6 +188,13 @@ def light_setup(light) -> dict:
                 deltas=np.array(deltas, dtype=np.float32).reshape(2, 3))
 
 
+def measure_alu_rate() -> float:
+    """FP32 lane operations per second of the current device (issue-rate probe)."""
+    v = ctypes.c_double()
+    _check(load().fdzb_measure_alu_rate(ctypes.byref(v)))
+    return float(v.value)
+
+
 def mask_words(n: int) -> int:
     return (n * n + 31) // 32
 
@@ -216,6 +229,10 @@ class Context:
     def set_debug(self, flags: int) -> None:
         """flags bit 0: keep pre-sort copies of the key arrays for export()."""
         _check(self._lib.fdzb_ctx_set_debug(self._h, int(flags)))
+
+    def set_profiling(self, enable: bool) -> None:
+        """Per-stage CUDA-event timing, reported in stats()['stage_ms']."""
+        _check(self._lib.fdzb_ctx_set_profiling(self._h, int(bool(enable))))
 
     def set_tri_order(self, order: int) -> None:
         """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_DEPTH."""

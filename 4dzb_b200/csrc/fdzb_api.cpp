@@ -87,6 +87,9 @@ struct fdzb_ctx {
     fdzb::FrameState *hState = nullptr;
     int *hBases = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool profile = false;  // record events at the stage boundaries
+    cudaEvent_t stageEv[fdzb::STAGE_COUNT + 1] = {};
+    int launches = 0;
     bool pending = false;
     fdzb_frame_stats stats{};
     float lastMs = 0.f;
@@ -261,7 +264,8 @@ int enqueue(fdzb_ctx *c)
     FDZB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(fdzb::Counters), c->stream));
     FDZB_CUDA(cudaMemsetAsync(b.sortHist, 0, 8 * 256 * sizeof(uint32_t), c->stream));
     FDZB_CUDA(cudaEventRecord(c->ev0, c->stream));
-    FDZB_CUDA(fdzb::run_pipeline(b, (int)S, T, V, c->stream));
+    FDZB_CUDA(fdzb::run_pipeline(b, (int)S, T, V, c->stream, c->profile ? c->stageEv : nullptr,
+                                 &c->launches));
     FDZB_CUDA(cudaEventRecord(c->ev1, c->stream));
     FDZB_CUDA(cudaMemcpyAsync(c->hCounters, b.counters, sizeof(fdzb::Counters), cudaMemcpyDeviceToHost, c->stream));
     FDZB_CUDA(cudaMemcpyAsync(c->hState, b.states, sizeof(fdzb::FrameState), cudaMemcpyDeviceToHost, c->stream));
@@ -320,6 +324,14 @@ int sync_frame(fdzb_ctx *c)
     }
     o.replans = replans;
     o.quirk_key_range = s.quirkKeyRange;
+    o.kernel_launches = c->launches;
+    o.rows_evaluated = (int64_t)k.rowsEvaluated;
+    o.partial_masks = (int64_t)k.partialMasks;
+    for (int i = 0; i < fdzb::STAGE_COUNT; ++i) {
+        float t = 0.f;
+        if (c->profile) cudaEventElapsedTime(&t, c->stageEv[i], c->stageEv[i + 1]);
+        o.stage_ms[i] = t;
+    }
     return FDZB_OK;
 }
 
@@ -335,6 +347,7 @@ int ctx_init_resources(fdzb_ctx *c, int device)
     c->stream = c->ownStream;
     FDZB_CUDA(cudaEventCreate(&c->ev0));
     FDZB_CUDA(cudaEventCreate(&c->ev1));
+    for (auto &e : c->stageEv) FDZB_CUDA(cudaEventCreate(&e));
     FDZB_CUDA(cudaMallocHost(&c->hFrame, sizeof(fdzb::FrameDesc)));
     FDZB_CUDA(cudaMallocHost(&c->hCounters, sizeof(fdzb::Counters)));
     FDZB_CUDA(cudaMallocHost(&c->hState, sizeof(fdzb::FrameState)));
@@ -353,6 +366,8 @@ void ctx_release(fdzb_ctx *c)
     if (c->hBases) cudaFreeHost(c->hBases);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto &e : c->stageEv)
+        if (e) cudaEventDestroy(e);
     if (c->ownStream) cudaStreamDestroy(c->ownStream);
     delete c;
 }
@@ -407,6 +422,20 @@ int fdzb_ctx_set_debug(fdzb_ctx *c, int flags)
 {
     if (int rc = ctx_check(c)) return rc;
     c->debug = flags & 1;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_profiling(fdzb_ctx *c, int enable)
+{
+    if (int rc = ctx_check(c)) return rc;
+    c->profile = enable != 0;
+    return FDZB_OK;
+}
+
+int fdzb_measure_alu_rate(double *lane_ops_per_second)
+{
+    if (!lane_ops_per_second) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    FDZB_CUDA(fdzb::measure_alu_rate(lane_ops_per_second));
     return FDZB_OK;
 }
 

@@ -78,7 +78,13 @@ struct Counters {
     int errorFlags;         // bit 0: look-back wait gave up, bit 1: mbarrier wait gave up
     unsigned long long pairTests;
     int sortTileCounter[8]; // one ticket per radix pass (4 sample + 4 pair)
+    unsigned long long rowsEvaluated;   // light rows evaluated by pair tests
+    unsigned long long partialMasks;    // row masks that needed the ceil(-D/B) threshold
 };
+
+// Stage boundaries recorded when per-stage timing is on.
+enum StageId { STAGE_SETUP = 0, STAGE_SAMPLE_SORT, STAGE_TRI_PAIRS, STAGE_PAIR_SORT, STAGE_OCCLUSION,
+               STAGE_COUNT };
 
 enum ErrorBits { ERR_LOOKBACK_TIMEOUT = 1, ERR_MBAR_TIMEOUT = 2, ERR_BAD_INPUT = 4, ERR_INTERNAL = 8 };
 
@@ -124,7 +130,12 @@ void light_setup(const float rightRadius, const float topRadius, const float pos
 
 // Kernel drivers (fdzb_pipeline.cu).  All enqueue on `stream`, no host syncs.
 // maxS / maxT / maxV: largest per-frame sample / triangle / vertex counts.
-cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t stream);
+// stageEvents: nullptr, or STAGE_COUNT + 1 events recorded at the stage
+// boundaries.  *launches receives the number of kernels enqueued.
+cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t stream,
+                         cudaEvent_t *stageEvents, int *launches);
+// Issue-rate probe: lane FP32 adds per second of a kernel with independent chains.
+cudaError_t measure_alu_rate(double *laneOpsPerSecond);
 int sort_passes_for(long long keyRangeExclusive);
 cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t stream);
 constexpr int kSortTileHost = 4096;   // keys per radix-sort tile (fdzb_sort.cuh)

@@ -26,19 +26,31 @@ namespace fdzb {
 #define FDZB_OCC_MINBLOCKS 6
 #endif
 
+#ifndef FDZB_OCC_ITEM
+#define FDZB_OCC_ITEM 32
+#endif
+#ifndef FDZB_OCC_CHUNK
+#define FDZB_OCC_CHUNK 32
+#endif
+#ifndef FDZB_OCC_VOTE
+#define FDZB_OCC_VOTE 1
+#endif
+
 constexpr int kOccWarps = 4;
 constexpr int kOccThreads = kOccWarps * 32;
-constexpr int kOccChunk = 32;
-constexpr int kItemSamples = 256;
+constexpr int kOccChunk = FDZB_OCC_CHUNK;
+constexpr int kItemSamples = FDZB_OCC_ITEM;
 
 // K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(N-1) precomputed (the same
 // product) and the result limited to the N-bit light grid.
-__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full)
+__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full,
+                                             uint32_t &npart)
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
     if (f1 && f2) return full;
     if (!f1 && !f2) return 0u;
+    ++npart;
     const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
     const int k = __float2int_rz(ceilf(q));
     uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
@@ -107,7 +119,7 @@ __device__ __forceinline__ void load_sample(LaneSample &s, const FrameDesc &fr, 
 // if the pair passed the AABB pre-cull.
 __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s, f3 xd, f3 yd,
                                          float esp, float nm1, uint32_t FULL, uint32_t (*rows)[32],
-                                         int lane, uint32_t &fullRows)
+                                         int lane, uint32_t &fullRows, uint32_t &nrows, uint32_t &npart)
 {
     const float4 p0 = T.p[0];
     const float4 p1 = T.p[1];
@@ -134,18 +146,19 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
     const float An0 = __fmul_rn(A0, nm1), An1 = __fmul_rn(A1, nm1), An2 = __fmul_rn(A2, nm1);
     const float Bn0 = __fmul_rn(B0, nm1), Bn1 = __fmul_rn(B1, nm1), Bn2 = __fmul_rn(B2, nm1);
     // row filter (:176-191)
-    const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL);
-    const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL);
-    const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL);
+    const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL, npart);
+    const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL, npart);
+    const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL, npart);
     uint32_t vr = N0 & N1 & N2 & ~fullRows;
     // rows (:204-222)
     while (vr) {
         const int r = __ffs(vr) - 1;
         vr &= vr - 1u;
+        ++nrows;
         const float fr = (float)r;
-        const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, FULL);
-        const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, FULL);
-        const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, FULL);
+        const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, FULL, npart);
+        const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, FULL, npart);
+        const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, FULL, npart);
         const uint32_t nv = rows[r][lane] | (M0 & M1 & M2);
         rows[r][lane] = nv;
         if (nv == FULL) fullRows |= 1u << r;
@@ -236,6 +249,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
     uint32_t(*rows)[32] = s_rows[warp];
     StagedTri *tris = s_tri[warp];
     unsigned long long tested = 0;
+    uint32_t nrows = 0, npart = 0;
     int nitems = *(volatile const int *)&ctr->itemCount;
     if (nitems > itemCapacity) nitems = itemCapacity;
 
@@ -311,9 +325,13 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
             }
             __syncwarp();
             for (int t = 0; t < m; ++t) {
+#if FDZB_OCC_VOTE
+                if (!__any_sync(kFullWarp, remaining > 0)) break;
+#endif
                 if (remaining > 0) {
                     --remaining;
-                    tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows);
+                    tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows, nrows,
+                                        npart);
                     if (fullRows == FULL) remaining = 0;
                 }
             }
@@ -351,10 +369,18 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
             }
         }
     }
-    unsigned long long t = tested;
+    unsigned long long t = tested, tr = nrows, tp = npart;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFullWarp, t, o);
-    if (lane == 0 && t) atomicAdd(&ctr->pairTests, t);
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_xor_sync(kFullWarp, t, o);
+        tr += __shfl_xor_sync(kFullWarp, tr, o);
+        tp += __shfl_xor_sync(kFullWarp, tp, o);
+    }
+    if (lane == 0 && t) {
+        atomicAdd(&ctr->pairTests, t);
+        atomicAdd(&ctr->rowsEvaluated, tr);
+        atomicAdd(&ctr->partialMasks, tp);
+    }
 }
 
 }  // namespace fdzb

@@ -672,7 +672,7 @@ static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *v
 
 static int g_smCount = 0;
 
-cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t s)
+static int sm_count()
 {
     if (g_smCount == 0) {
         int dev = 0;
@@ -680,8 +680,17 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         cudaDeviceGetAttribute(&g_smCount, cudaDevAttrMultiProcessorCount, dev);
         if (g_smCount <= 0) g_smCount = 148;
     }
-    const int sm = g_smCount;
+    return g_smCount;
+}
+
+cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, cudaStream_t s,
+                         cudaEvent_t *ev, int *launches)
+{
+    const int sm = sm_count();
     const int nf = b.nframes;
+    int nl = 0;
+    if (ev) cudaEventRecord(ev[STAGE_SETUP], s);
+    // (a) samples, vertices, triangles
     k_init<<<grid_for(b.totalBins + 1, 256, sm * 8), 256, 0, s>>>(
         b.states, nf, b.binStat, b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.totalBins);
     {
@@ -693,11 +702,13 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
                                                                       &b.counters->errorFlags);
     k_sample_keys<<<dim3(grid_for(maxS, 256, sm * 8), nf), 256, 0, s>>>(
         b.frames, b.states, b.keysA, b.valsA, b.binStat, b.totalBins);
-
+    nl += 5;
     if (b.dbgKeys) {
         cudaMemcpyAsync(b.dbgKeys, b.keysA, 4ull * b.totalSamples, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(b.dbgVals, b.valsA, 4ull * b.totalSamples, cudaMemcpyDeviceToDevice, s);
     }
+    // (b) sample sort and segments
+    if (ev) cudaEventRecord(ev[STAGE_SAMPLE_SORT], s);
     run_sort(b, 0, b.keysA, b.valsA, b.keysB, b.valsB, nullptr, b.totalSamples, b.totalSamples,
              b.samplePasses, sm, s);
     uint32_t *sk = (b.samplePasses & 1) ? b.keysB : b.keysA;
@@ -705,7 +716,9 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     k_find_start_end<<<grid_for(b.totalSamples, 256, sm * 8), 256, 0, s>>>(
         sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
         (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
-
+    nl += 2 + b.samplePasses;
+    // (a) triangle/bin pairs
+    if (ev) cudaEventRecord(ev[STAGE_TRI_PAIRS], s);
     {
         const int tiles = (b.totalTris + kTriThreads - 1) / kTriThreads;
         const int grid = tiles < sm * 4 ? (tiles > 0 ? tiles : 1) : sm * 4;
@@ -713,11 +726,14 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epoch, b.pkeysA, b.pvalsA, b.pairCapacity,
                                                  b.depthBits, b.counters);
+        nl += 1;
     }
     if (b.dbgPKeys) {
         cudaMemcpyAsync(b.dbgPKeys, b.pkeysA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(b.dbgPVals, b.pvalsA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
     }
+    // (b) pair sort and segments
+    if (ev) cudaEventRecord(ev[STAGE_PAIR_SORT], s);
     run_sort(b, 1, b.pkeysA, b.pvalsA, b.pkeysB, b.pvalsB, &b.counters->pairCount, 0, b.pairCapacity,
              b.pairPasses, sm, s);
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
@@ -725,13 +741,63 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
         pk, &b.counters->pairCount, 0, b.pairCapacity, b.depthBits, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
+    nl += 2 + b.pairPasses;
+    // (c) + (d) occlusion and shading
+    if (ev) cudaEventRecord(ev[STAGE_OCCLUSION], s);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
         b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
         b.items, b.itemCapacity, b.counters);
-    k_occlusion<<<sm * 8, kOccThreads, 0, s>>>(b.frames, b.states, b.items, b.itemCapacity, b.counters,
-                                               sv, b.binSampleStart, b.binSampleEnd, b.binTriStart,
-                                               b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    k_occlusion<<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
+        b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
+        b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    nl += 2;
+    if (ev) cudaEventRecord(ev[STAGE_COUNT], s);
+    if (launches) *launches = nl;
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Issue-rate probe for the roofline of the occlusion kernel: 8 independent
+// FP32 add chains per thread, enough warps per SM to hide the add latency.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_alu_probe(float *out, int iters, float step)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = (float)(threadIdx.x + k) * 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = __fadd_rn(a[k], step);
+    }
+    float r = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r = __fadd_rn(r, a[k]);
+    if (r == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = r;  // keeps the chains live
+}
+
+cudaError_t measure_alu_rate(double *rate)
+{
+    const int sm = sm_count();
+    float *out = nullptr;
+    cudaError_t e = cudaMalloc(&out, 4);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sm * 8, threads = 256, iters = 4096;
+    k_alu_probe<<<blocks, threads>>>(out, 64, 1.0f);  // warm-up
+    cudaEventRecord(a);
+    k_alu_probe<<<blocks, threads>>>(out, iters, 1.0f);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    *rate = ms > 0 ? (double)blocks * threads * iters * 8.0 / (ms * 1e-3) : 0.0;
+    return e;
 }
 
 }  // namespace fdzb

@@ -1,0 +1,341 @@
+#!/usr/bin/env python3
+"""Benchmark of the FDZB soft-shadow path on B200.
+
+Workload (default, --config hd): one frame = 1920x1080 view samples x 200,000
+occluder triangles x 16x16 light grid, 128x128 light-plane bins, fp32, seeded
+synthetic scene (no public dataset; the reference's own meshes are absent).
+A step is one frame through the library's public context API.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fdzb|reference]
+
+N > 1 runs under torchrun: one process per GPU, each rendering its own frames
+(replicas, weak scaling); timing is the max over ranks.
+
+Metric: shadow frames/s (whole job).  Also reported: sample-triangle pair
+tests/s (executed, and brute-force-equivalent S*T/t), the occlusion kernel's
+operation rate against the measured FP32 issue rate, the end-to-end rate with
+host buffers, and the CPU baseline (the exhaustive per-pair test as an OpenMP
+loop on this host's cores, on a bounded random sample of the frame's samples).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic operation count of one sample/triangle pair test, as written in the
+# reference's per-pair code (K/Step5_2_shadowCalPerSample.inl:120-222): pre-cull
+# compares, face normal, orientation, the three plane discriminants, the row
+# filter; per evaluated light row: three row masks and the mask update; per
+# partial row mask: the ceil(-D/B) threshold (negate, divide, ceil, convert,
+# shift, decrement, invert).
+OPS_PER_PAIR = 164
+OPS_PER_ROW = 31
+OPS_PER_PARTIAL = 7
+
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except OSError:
+        return {}
+
+
+def profile_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_hd.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(scene, seconds_target: float = 15.0) -> dict:
+    """Exhaustive per-pair FP32 loop (OpenMP, all host threads) on a random
+    sample of the frame's samples; extrapolated to frames/s."""
+    import numpy as np
+    import oracle
+    fr = oracle.frame(scene, occ_stride=1 << 30)          # light plane / records only
+    rng = np.random.default_rng(12345)
+    threads = os.cpu_count() or 1
+    n = 256
+    t0 = time.time()
+    ids = rng.choice(scene.S, n, replace=False).astype(np.int32)
+    _, tests = oracle.exhaustive_fp32(scene, fr, ids, nthreads=threads)
+    dt = time.time() - t0
+    # grow the sample to fill the time budget
+    if dt < seconds_target / 4:
+        n = int(min(scene.S, n * max(1.0, seconds_target / max(dt, 1e-3))))
+        ids = rng.choice(scene.S, n, replace=False).astype(np.int32)
+        t0 = time.time()
+        _, tests = oracle.exhaustive_fp32(scene, fr, ids, nthreads=threads)
+        dt = time.time() - t0
+    per_sample = dt / n
+    frame_s = per_sample * scene.S
+    return {"value": 1.0 / frame_s, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{n} random samples of the {scene.W}x{scene.H} frame x all {scene.T} triangles, "
+                      f"exhaustive per-pair FP32 test (OpenMP), {dt:.1f} s, extrapolated to the full frame",
+            "pair_tests_per_s": tests / dt, "effective_gpairs_per_s": n * scene.T / dt / 1e9}
+
+
+def reference_arm(args, scene) -> dict:
+    """The reference algorithm on the host cores: the oracle's port of the binned
+    pipeline (light plane, binning, sorts, per-sample occlusion), with the
+    occlusion stage on every `stride`-th sample, extrapolated to the full frame."""
+    import oracle
+    threads = os.cpu_count() or 1
+    stride = 64
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.time()
+        fr = oracle.frame(scene, nthreads=threads, occ_stride=stride)
+        dt = time.time() - t0
+        t_occ = fr.scalars.get("t_occ_ms", 0.0) / 1e3
+        t_frame = (dt - t_occ) + t_occ * stride
+        if i >= args.warmup:
+            times.append(t_frame)
+    ms = 1e3 * statistics.mean(times)
+    v = 1e3 / ms
+    return {"metric": "shadow frames/s", "value": v, "unit": "frames/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.config, "W": scene.W, "H": scene.H, "triangles": scene.T,
+                       "light_grid": scene.light.n, "bins": scene.bins},
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": f"binned FP32 port of the reference pipeline; occlusion on every "
+                                       f"{stride}th binned sample, extrapolated"},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fdzb", choices=["fdzb", "reference"])
+    ap.add_argument("--config", default="hd", choices=["small", "hd", "large"])
+    ap.add_argument("--tri-order", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    ws, rank, local = _dist()
+    scenes = importlib.import_module("4dzb_b200.scenes")
+
+    if args.impl == "reference":
+        if rank == 0:
+            scene = scenes.preset(args.config)
+            print(json.dumps(reference_arm(args, scene)), flush=True)
+        return
+
+    import torch
+    fdzb = importlib.import_module("4dzb_b200")
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    scene = scenes.preset(args.config)
+    stream = torch.cuda.Stream()
+    ctx, t = fdzb.context_for_scene(scene, masks=True, tri_order=args.tri_order)
+    ctx.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up (also grows the pair buffer to the scene's needs)
+    for _ in range(args.warmup):
+        ctx.launch()
+
+    # device-timed frames, inputs resident, L2 flushed before each frame
+    def timed(profile: bool):
+        ctx.set_profiling(profile)
+        evs = []
+        stats = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.launch_async()
+            b.record(stream)
+            ctx.sync()
+            evs.append((a, b))
+            stats.append(ctx.stats())
+        stream.synchronize()
+        return [a.elapsed_time(b) for a, b in evs], stats
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        frame_ms, stats = timed(False)
+    torch.cuda.synchronize()
+    total_ms = sum(frame_ms)
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_step = total_ms / args.steps
+    value = args.gpus * 1e3 / ms_step
+    st = stats[-1]
+    assert all(s["replans"] == 0 for s in stats), "pair buffer regrown inside the timed region"
+
+    # per-stage times (separate pass with stage events) for the roofline
+    prof_ms, pstats = timed(True)
+    stage = [statistics.mean(s["stage_ms"][i] for s in pstats) for i in range(5)]
+    occ_ms = stage[4]
+    ops = (pstats[-1]["pair_tests"] * OPS_PER_PAIR + pstats[-1]["rows_evaluated"] * OPS_PER_ROW
+           + pstats[-1]["partial_masks"] * OPS_PER_PARTIAL)
+    alu_peak = fdzb.measure_alu_rate()
+    achieved = ops / (occ_ms * 1e-3)
+
+    # end to end through the public API with host buffers: H2D of the frame's
+    # G-buffer (positions + normals) from pinned memory, the frame, D2H of the
+    # shadow buffer
+    pos_h = torch.from_numpy(scene.pos).pin_memory()
+    nrm_h = torch.from_numpy(scene.nrm).pin_memory()
+    sh_h = torch.empty(scene.S, dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        with torch.cuda.stream(stream):
+            t["pos"].copy_(pos_h, non_blocking=True)
+            t["nrm"].copy_(nrm_h, non_blocking=True)
+        ctx.launch_async()
+        with torch.cuda.stream(stream):
+            sh_h.copy_(t["shadow"], non_blocking=True)
+        b.record(stream)
+        ctx.sync()
+        stream.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = sum(e2e_ms)
+    if dist:
+        tt = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = args.gpus * 1e3 * args.steps / e2e_total
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(scene)
+
+    peaks = measured_peaks()
+    clocks = clk.summary()
+    out = {
+        "metric": "shadow frames/s", "value": value, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {scene.W}x{scene.H} samples x {scene.T} triangles x "
+                               f"{scene.light.n}x{scene.light.n} light, {scene.bins}^2 bins",
+                   "W": scene.W, "H": scene.H, "triangles": scene.T, "light_grid": scene.light.n,
+                   "bins": scene.bins, "tri_order": "depth" if args.tri_order else "reference",
+                   "l2": "flushed (256 MB write) before every timed frame", "parallelism": f"replicas{args.gpus}"},
+        "pair_tests_per_s": st["pair_tests"] * 1e3 / ms_step * args.gpus,
+        "effective_gpairs_per_s": scene.S * scene.T * 1e3 / ms_step * args.gpus / 1e9,
+        "stage_ms": dict(zip(fdzb.STAGES, stage)),
+        "roofline": {"kernel": "k_occlusion", "bound": "alu", "achieved": achieved / 1e9,
+                     "peak": alu_peak / 1e9, "unit": "Gop/s", "frac": achieved / alu_peak,
+                     "traffic": profile_traffic("k_occlusion"),
+                     "ops_per_launch": ops, "launch_ms": occ_ms,
+                     "note": "algorithmic FP32/INT32 ops of the reference per-pair code / measured FP32 "
+                             "issue rate (lane ops/s) of this GPU"},
+        "e2e": {"value": e2e_value, "unit": "frames/s",
+                "h2d_bytes_per_step": int(scene.pos.nbytes + scene.nrm.nbytes),
+                "d2h_bytes_per_step": int(scene.S * 4)},
+        "gpu_launches": st["kernel_launches"] * args.steps,
+        "clocks": clocks,
+        "frame_stats": {"valid_samples": st["valid_samples"], "pairs": st["num_pairs"],
+                        "pair_tests": st["pair_tests"], "rows_evaluated": st["rows_evaluated"],
+                        "partial_masks": st["partial_masks"]},
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

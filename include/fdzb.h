@@ -125,6 +125,13 @@ typedef struct fdzb_frame_stats {
     float sample_aabb[6], model_aabb[6];
     int32_t replans;           /* pair-buffer regrowths in this launch */
     int32_t quirk_key_range;   /* samples whose bin fell outside the grid (treated as unbinned) */
+    int32_t kernel_launches;   /* kernels enqueued by the frame */
+    int32_t pad0;
+    int64_t rows_evaluated;    /* light-grid rows evaluated by pair tests */
+    int64_t partial_masks;     /* row masks that needed the ceil(-D/B) threshold */
+    float stage_ms[5];         /* with profiling on: setup, sample sort, triangle pairs,
+                                  pair sort, occlusion+shading (CUDA events) */
+    float pad1;
 } fdzb_frame_stats;
 
 /* device < 0: current device. */
@@ -189,6 +196,16 @@ int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
 #define FDZB_TRI_ORDER_REFERENCE 0
 #define FDZB_TRI_ORDER_DEPTH     1
 int fdzb_ctx_set_tri_order(fdzb_ctx *ctx, int order);
+
+/* Per-stage GPU timing (CUDA events between stages, read back in
+ * fdzb_frame_stats.stage_ms); off by default.  The reference times only the whole
+ * frame (FS/api.cpp:405-409,574-581). */
+int fdzb_ctx_set_profiling(fdzb_ctx *ctx, int enable);
+
+/* Measures the FP32 issue rate of the current device (lane operations per second
+ * of a kernel of independent FP32 add chains): the peak against which the
+ * occlusion kernel's operation rate is reported.  No counterpart in the reference. */
+int fdzb_measure_alu_rate(double *lane_ops_per_second);
 
 /* Host-side light setup only (FS/api.cpp:303-400): fills the 16-float
  * column-major light projection, RectangleFactor and the four light corners

@@ -281,6 +281,15 @@ static void pack_mask(const uint32_t *rows, int N, uint32_t *out)
 
 static int ceil_log2_int(int v) { return (int)ceilf(log2f((float)v)); }
 
+static double wall_s(void)
+{
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
+
 /* Stable counting sort of (key, val) by key in [0, nkeys). */
 static int stable_sort_pairs(const int32_t *k, const int32_t *v, int64_t n, int32_t nkeys,
                              int32_t *ko, int32_t *vo)
@@ -328,6 +337,8 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
     o->valid_samples = o->valid_tris = o->num_pairs = o->pair_overflow = 0;
     o->pairs_tested = o->quirk_rows_beyond_n = o->quirk_high_bits = o->quirk_key_range = 0;
     o->rows_evaluated = o->partial_masks = 0;
+    o->t_total_ms = o->t_occ_ms = 0.0;
+    const double t_begin = wall_s();
     o->view_log2up = ceil_log2_int(W);
     const int log2up = o->view_log2up;
     const int Wb = in->bins, Hb = in->bins;
@@ -619,6 +630,7 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
 
     /* A14 + A15: K/Step5_2_shadowCalPerSample.inl:37-231 */
     {
+        const double t_occ0 = wall_s();
         pair_ctx c;
         memcpy(c.ur, L->upRight, sizeof(c.ur));
         memcpy(c.xd, L->x_delt, sizeof(c.xd));
@@ -664,6 +676,7 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
         o->quirk_high_bits = qhigh;
         o->rows_evaluated = nrows;
         o->partial_masks = npart;
+        o->t_occ_ms = 1e3 * (wall_s() - t_occ0);
     }
 
 free2:
@@ -672,6 +685,7 @@ free2:
     free(pbin); free(ptri); free(spbin); free(sptri);
 done:
     free(rb); free(re); free(backface); free(rec); free(taabb);
+    o->t_total_ms = 1e3 * (wall_s() - t_begin);
     return ret;
 }
 

@@ -80,6 +80,7 @@ typedef struct {
     int64_t quirk_key_range;     /* samples whose bin x/y fell outside the grid */
     int64_t rows_evaluated;      /* light-grid rows evaluated (3 row masks each) */
     int64_t partial_masks;       /* row masks that needed the ceil(-D/B) threshold */
+    double t_total_ms, t_occ_ms; /* wall time of the call and of the occlusion stage */
     /* arrays, caller-allocated; NULL skips the copy */
     int32_t *keys, *vals;                     /* [S] position order */
     int32_t *sorted_keys, *sorted_vals;       /* [S] */

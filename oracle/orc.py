@@ -54,6 +54,7 @@ class FrameOut(ctypes.Structure):
                 ("pairs_tested", ctypes.c_int64), ("quirk_rows_beyond_n", ctypes.c_int64),
                 ("quirk_high_bits", ctypes.c_int64), ("quirk_key_range", ctypes.c_int64),
                 ("rows_evaluated", ctypes.c_int64), ("partial_masks", ctypes.c_int64),
+                ("t_total_ms", ctypes.c_double), ("t_occ_ms", ctypes.c_double),
                 ("keys", i32p), ("vals", i32p), ("sorted_keys", i32p), ("sorted_vals", i32p),
                 ("bin_sample_start", i32p), ("bin_sample_end", i32p), ("bin_maxz", f32p),
                 ("bin_range", f32p), ("tri_aabb", f32p), ("tri_count", i32p),
