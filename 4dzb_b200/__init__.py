@@ -50,7 +50,7 @@ EXPORTED = [
     "fdzb_ctx_set_scene_params", "fdzb_ctx_set_area_light", "fdzb_ctx_move_model",
     "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
     "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_ctx_set_tri_order", "fdzb_light_setup",
-    "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate",
+    "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate", "fdzb_sort_pairs_noalloc",
 ]
 
 STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]

@@ -386,6 +386,8 @@ bool is_device_pointer(const void *p)
 
 }  // namespace
 
+int fdzb::set_error(int code, const std::string &msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char *fdzb_last_error(void) { return g_err.c_str(); }

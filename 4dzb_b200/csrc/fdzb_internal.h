@@ -7,6 +7,7 @@
 // key is the total bin count.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace fdzb {
@@ -136,6 +137,9 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
                          cudaEvent_t *stageEvents, int *launches);
 // Issue-rate probe: lane FP32 adds per second of a kernel with independent chains.
 cudaError_t measure_alu_rate(double *laneOpsPerSecond);
+
+// Records `msg` as this thread's fdzb_last_error() and returns `code`.
+int set_error(int code, const std::string &msg);
 int sort_passes_for(long long keyRangeExclusive);
 cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t stream);
 constexpr int kSortTileHost = 4096;   // keys per radix-sort tile (fdzb_sort.cuh)

@@ -216,6 +216,33 @@ int fdzb_light_setup(const fdzb_area_light_desc *light, float mat[16], float rec
 /* Library version string. */
 const char *fdzb_version(void);
 
+/* ---- allocation-free sort ------------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- an allocator or pool that forbids cudaMalloc/cudaFree on the hot
+ * path, a host process that owns every allocation, a real-time loop that may
+ * not synchronise for cudaFree -- this sorts n (key, value) uint32 pairs by key,
+ * stably (equal keys keep their input order), keys < key_range, using only a
+ * fixed scratch area built into the library (about 8.5 MB of device memory on
+ * every GPU that loads libfdzb.so, held until the process exits).  It is the
+ * same radix sort the frame pipeline runs on its own arena.
+ *  - n at most FDZB_NOALLOC_SORT_MAX_PAIRS; larger n is rejected
+ *    (FDZB_ERR_INVALID_ARG) before any work is enqueued;
+ *  - inputs are not modified; outputs must not alias inputs or each other;
+ *  - work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ *    stream) and the call returns without waiting; d_status (device int32,
+ *    nullable) receives 0, or nonzero if a bounded device wait gave up;
+ *  - the first call on a device looks up the scratch area's device address
+ *    with cudaGetSymbolAddress, so make it before any stream capture;
+ *  - every call reuses the same scratch area: calls that overlap on the GPU
+ *    (other streams or threads on the same device) race and must be ordered by
+ *    the caller;
+ *  - no cudaMalloc, cudaFree or other allocating routine is called. */
+#define FDZB_NOALLOC_SORT_MAX_PAIRS (1 << 20)
+int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t *d_vals_in,
+                            uint32_t *d_keys_out, uint32_t *d_vals_out, int32_t n,
+                            uint32_t key_range, void *stream, int32_t *d_status);
+
 #ifdef __cplusplus
 }
 #endif
