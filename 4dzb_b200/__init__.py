@@ -51,6 +51,10 @@ EXPORTED = [
     "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
     "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_ctx_set_tri_order", "fdzb_light_setup",
     "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate", "fdzb_sort_pairs_noalloc",
+    "fdzb_ctx_set_graph", "fdzb_batch_create", "fdzb_batch_destroy", "fdzb_batch_set_stream",
+    "fdzb_batch_set_graph", "fdzb_batch_set_profiling", "fdzb_batch_set_tri_order",
+    "fdzb_batch_launch_async", "fdzb_batch_sync", "fdzb_batch_launch", "fdzb_batch_get_frame_stats",
+    "fdzb_batch_get_stats", "fdzb_batch_frame_bins", "fdzb_batch_autotune",
 ]
 
 STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
@@ -106,6 +110,27 @@ class FrameStats(ctypes.Structure):
         return out
 
 
+class FrameDesc(ctypes.Structure):
+    """fdzb_frame_desc: one frame of a batch."""
+    _fields_ = [("d_pos", ctypes.c_void_p), ("d_nrm", ctypes.c_void_p), ("W", ctypes.c_int32),
+                ("H", ctypes.c_int32), ("d_vtx", ctypes.c_void_p), ("n_vtx", ctypes.c_size_t),
+                ("vtx_stride_bytes", ctypes.c_size_t), ("d_idx", ctypes.c_void_p), ("n_tri", ctypes.c_size_t),
+                ("light", AreaLightDesc), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
+                ("esp", ctypes.c_float), ("d_shadow", ctypes.c_void_p), ("d_masks", ctypes.c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("totals", FrameStats), ("frames", ctypes.c_int32), ("from_graph", ctypes.c_int32),
+                ("graph_captures", ctypes.c_int64), ("graph_replays", ctypes.c_int64),
+                ("tuned_classes", ctypes.c_int32), ("pad0", ctypes.c_int32), ("tune_launches", ctypes.c_int64),
+                ("ms", ctypes.c_float), ("pad1", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        out = {n: getattr(self, n) for n, _ in self._fields_ if n != "totals"}
+        out["totals"] = self.totals.as_dict()
+        return out
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -149,6 +174,16 @@ def load() -> ctypes.CDLL:
         "fdzb_light_setup": ([P(AreaLightDesc), P(ctypes.c_float), P(ctypes.c_float),
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
+        "fdzb_ctx_set_graph": ([vp, i32], i32),
+        "fdzb_batch_create": ([P(vp), i32], i32), "fdzb_batch_destroy": ([vp], i32),
+        "fdzb_batch_set_stream": ([vp, vp], i32), "fdzb_batch_set_graph": ([vp, i32], i32),
+        "fdzb_batch_set_profiling": ([vp, i32], i32), "fdzb_batch_set_tri_order": ([vp, i32], i32),
+        "fdzb_batch_launch_async": ([vp, P(FrameDesc), i32], i32),
+        "fdzb_batch_sync": ([vp, P(ctypes.c_float)], i32),
+        "fdzb_batch_launch": ([vp, P(FrameDesc), i32, P(ctypes.c_float)], i32),
+        "fdzb_batch_get_frame_stats": ([vp, i32, P(FrameStats)], i32),
+        "fdzb_batch_get_stats": ([vp, P(BatchStats)], i32), "fdzb_batch_frame_bins": ([vp, i32], i32),
+        "fdzb_batch_autotune": ([vp, P(FrameDesc), i32, vp, sz], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -237,6 +272,10 @@ class Context:
     def set_tri_order(self, order: int) -> None:
         """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_DEPTH."""
         _check(self._lib.fdzb_ctx_set_tri_order(self._h, int(order)))
+
+    def set_graph(self, enable: bool) -> None:
+        """Capture launches in a CUDA graph and replay it while the shape holds (default on)."""
+        _check(self._lib.fdzb_ctx_set_graph(self._h, int(bool(enable))))
 
     def add_model(self, vtx, n_vtx: int, stride_bytes: int, idx, n_tri: int, name: str = "") -> None:
         self._keep += [vtx, idx]
@@ -409,3 +448,94 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
     ctx.set_output_buffer(shadow, mk)
     ctx.set_area_light(scene.light)
     return ctx, dict(pos=pos, nrm=nrm, vtx=vtx, idx=idx, shadow=shadow, masks=mk)
+
+
+# ---- batches ---------------------------------------------------------------
+
+
+def frame_desc(pos, nrm, W: int, H: int, vtx, n_vtx: int, idx, n_tri: int, light, shadow, masks=None,
+               bins: int = 0, cull: bool = False, esp: float = 1e-3, stride_bytes: int = 16) -> FrameDesc:
+    """An fdzb_frame_desc from device tensors (or int pointers); bins 0 = autotuned."""
+    d = FrameDesc()
+    d.d_pos, d.d_nrm = _ptr(pos), _ptr(nrm)
+    d.W, d.H = W, H
+    d.d_vtx, d.n_vtx, d.vtx_stride_bytes = _ptr(vtx), n_vtx, stride_bytes
+    d.d_idx, d.n_tri = _ptr(idx), n_tri
+    d.light = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+    d.bins, d.cull, d.esp = bins, int(bool(cull)), esp
+    d.d_shadow, d.d_masks = _ptr(shadow), _ptr(masks)
+    return d
+
+
+class Batch:
+    """Many independent frames per launch (the fdzb_batch_* API)."""
+
+    def __init__(self, device: int = -1):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        _check(self._lib.fdzb_batch_create(ctypes.byref(h), device))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fdzb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _array(frames):
+        arr = (FrameDesc * len(frames))(*frames)
+        return arr
+
+    def set_graph(self, enable: bool) -> None:
+        _check(self._lib.fdzb_batch_set_graph(self._h, int(bool(enable))))
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(self._lib.fdzb_batch_set_profiling(self._h, int(bool(enable))))
+
+    def set_tri_order(self, order: int) -> None:
+        _check(self._lib.fdzb_batch_set_tri_order(self._h, int(order)))
+
+    def set_stream(self, stream) -> None:
+        _check(self._lib.fdzb_batch_set_stream(self._h, ctypes.c_void_p(stream)))
+
+    def launch(self, frames) -> float:
+        arr = self._array(frames)
+        ms = ctypes.c_float()
+        _check(self._lib.fdzb_batch_launch(self._h, arr, len(frames), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def launch_async(self, frames) -> None:
+        self._pending = self._array(frames)
+        _check(self._lib.fdzb_batch_launch_async(self._h, self._pending, len(frames)))
+
+    def sync(self) -> float:
+        ms = ctypes.c_float()
+        _check(self._lib.fdzb_batch_sync(self._h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def autotune(self, frames, scratch) -> None:
+        """scratch: device float tensor with at least max(W*H) elements."""
+        arr = self._array(frames)
+        _check(self._lib.fdzb_batch_autotune(self._h, arr, len(frames), _ptr(scratch), scratch.numel()))
+
+    def frame_stats(self, i: int) -> dict:
+        st = FrameStats()
+        _check(self._lib.fdzb_batch_get_frame_stats(self._h, i, ctypes.byref(st)))
+        return st.as_dict()
+
+    def stats(self) -> dict:
+        st = BatchStats()
+        _check(self._lib.fdzb_batch_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def frame_bins(self, i: int) -> int:
+        rc = self._lib.fdzb_batch_frame_bins(self._h, i)
+        if rc <= 0:
+            _check(rc if rc < 0 else -1)
+        return rc

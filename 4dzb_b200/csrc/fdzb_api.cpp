@@ -1,20 +1,24 @@
-// fdzb_api.cpp -- contexts, device arena and the extern "C" entry points.
+// fdzb_api.cpp -- engine, contexts, batches and the extern "C" entry points.
 //
-// A context owns one scene (model 0), one view and one light, plus every
-// scratch buffer of the pipeline, carved from a single grow-only device arena
-// (the reference allocates the same buffers with FD::Buffer<T>,
-// FS/api.cpp:48-144,205-294).  A frame is enqueued with no host round trip;
-// fdzb_ctx_sync() reads back one small counter block, checks the device error
-// word and, if the triangle/bin pair buffer overflowed, grows it and re-runs
-// the frame (the reference has no such check, FS/constants.h:15).
+// An Engine owns every scratch buffer of the pipeline, carved from a single
+// grow-only device arena (the reference allocates the same buffers with
+// FD::Buffer<T>, FS/api.cpp:48-144,205-294), plus the pinned staging blocks and
+// the CUDA graph of its last launch shape.  A launch processes a list of
+// frames laid end to end in HBM (one frame for the FD-shaped context API, up to
+// thousands for a batch) with no host round trip; sync reads back one small
+// counter block, checks the device error word and, if the triangle/bin pair
+// buffer overflowed, grows it and re-runs the launch (the reference has no such
+// check, FS/constants.h:15).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fdzb.h"
@@ -39,12 +43,22 @@ int fail(int code, const std::string &msg)
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-int ceil_log2(int v)
+int ceil_log2(long long v)
 {
     int l = 0;
-    while ((1 << l) < v) ++l;
+    while ((1ll << l) < v) ++l;
     return l;
 }
+
+// ABI layouts mirrored by the ctypes binding
+static_assert(sizeof(fdzb_area_light_desc) == 52, "fdzb_area_light_desc layout");
+static_assert(sizeof(fdzb_frame_stats) == 184, "fdzb_frame_stats layout");
+static_assert(sizeof(fdzb_frame_desc) == 144, "fdzb_frame_desc layout");
+static_assert(sizeof(fdzb_batch_stats) == 232, "fdzb_batch_stats layout");
+
+constexpr long long kMaxPairCapacity = 1ll << 29;
+constexpr long long kMaxTotalSamples = 0x7fffffffll / 2;
+constexpr long long kMaxTotalBins = 1ll << 27;   // leaves >= 5 depth bits in a 32-bit pair key
 
 struct Model {
     const float *vtx = nullptr;
@@ -54,57 +68,69 @@ struct Model {
     std::string name;
 };
 
-}  // namespace
+// Host copy of one frame's inputs.
+struct FrameSpec {
+    const float4 *pos = nullptr, *nrm = nullptr;
+    int W = 0, H = 0;
+    const float *vtx = nullptr;
+    size_t nv = 0, strideBytes = 16;
+    const int32_t *idx = nullptr;
+    size_t nt = 0;
+    fdzb::LightParams light{};
+    int bins = 16;
+    int cull = 1;
+    float esp = 1e-6f;
+    float *shadow = nullptr;
+    uint32_t *masks = nullptr;
+};
 
-struct fdzb_ctx {
+// Host-side parameters that a captured graph bakes in; a launch whose key
+// differs re-captures.
+struct GraphKey {
+    int nf = -1, S = 0, T = 0, NB = 0, P = 0, sp = 0, pp = 0, db = 0, maxS = 0, maxT = 0, maxV = 0;
+    const void *arena = nullptr, *hFrames = nullptr;
+    cudaStream_t stream = nullptr;
+    auto tie() const { return std::tie(nf, S, T, NB, P, sp, pp, db, maxS, maxT, maxV, arena, hFrames, stream); }
+    bool operator==(const GraphKey &o) const { return tie() == o.tie(); }
+};
+
+struct Engine {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t ownStream = nullptr;
-    // knobs (defaults of K/FourD.cu:61-62 and FS/constants.h:13)
-    int cull = 1;
-    float esp = 1e-6f;
-    int bins = 16;
-    int W = 0, H = 0;
-    size_t maxTri = 0, maxVert = 0;
-    const float4 *pos = nullptr, *nrm = nullptr;
-    float *shadow = nullptr;
-    uint32_t *masks = nullptr;
-    std::vector<Model> models;
-    bool lightSet = false;
-    fdzb_area_light_desc lightDesc{};
-    fdzb::LightParams light{};
-    // device arena
     void *arena = nullptr;
     size_t arenaBytes = 0;
     fdzb::DeviceBuffers buf{};
-    int pairCapacity = 0;
-    uint32_t epoch = 0;
-    int debug = 0;  // keep pre-sort copies for fdzb_ctx_export
+    long long pairCapacity = 0;
+    int debug = 0;  // keep pre-sort copies for export
     int triOrder = FDZB_TRI_ORDER_DEPTH;
-    // pinned host staging
-    fdzb::FrameDesc *hFrame = nullptr;
-    fdzb::Counters *hCounters = nullptr;
-    fdzb::FrameState *hState = nullptr;
-    int *hBases = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool profile = false;  // record events at the stage boundaries
+    bool useGraph = true;
+    // pinned host staging, grown to the largest frame list
+    fdzb::FrameDesc *hFrames = nullptr;
+    fdzb::FrameState *hStates = nullptr;
+    int *hBases = nullptr;
+    int hCap = 0;
+    fdzb::Counters *hCounters = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t stageEv[fdzb::STAGE_COUNT + 1] = {};
+    // the frame list of the pending / last launch
+    std::vector<FrameSpec> frames;
+    int maxS = 0, maxT = 0, maxV = 0;
     int launches = 0;
     bool pending = false;
-    fdzb_frame_stats stats{};
+    int replans = 0;
     float lastMs = 0.f;
+    // graph of the last launch shape
+    cudaGraphExec_t graph = nullptr;
+    GraphKey graphKey{};
+    bool lastFromGraph = false;
+    long long graphCaptures = 0, graphReplays = 0;
 };
 
-namespace {
-
-int ctx_check(fdzb_ctx *c)
-{
-    if (!c) return fail(FDZB_ERR_NOT_INITIALIZED, "context not initialised (call fdzb_init)");
-    return FDZB_OK;
-}
-
-// Lays out every buffer of a launch of one frame inside the arena; returns bytes.
-size_t layout(fdzb::DeviceBuffers &b, char *base, int S, int T, int NB, int P, bool debug)
+// Lays out every buffer of a launch of nf frames inside the arena; returns bytes.
+size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long T, long long NB, long long P,
+              bool debug)
 {
     size_t off = 0;
     auto take = [&](size_t bytes) -> char * {
@@ -113,20 +139,20 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int S, int T, int NB, int P, b
         off += bytes;
         return p;
     };
-    const int nf = 1;
     b.nframes = nf;
-    b.totalSamples = S;
-    b.totalTris = T;
-    b.totalBins = NB;
-    b.pairCapacity = P;
+    b.totalSamples = (int)S;
+    b.totalTris = (int)T;
+    b.totalBins = (int)NB;
+    b.pairCapacity = (int)P;
     b.frames = (fdzb::FrameDesc *)take(sizeof(fdzb::FrameDesc) * nf);
     b.states = (fdzb::FrameState *)take(sizeof(fdzb::FrameState) * nf);
     b.counters = (fdzb::Counters *)take(sizeof(fdzb::Counters));
+    b.epochWord = (uint32_t *)take(sizeof(uint32_t));
     b.sortHist = (uint32_t *)take(sizeof(uint32_t) * 8 * 256);
     b.sampleBases = (int *)take(sizeof(int) * 3 * nf);
     b.triBases = b.sampleBases ? b.sampleBases + nf : nullptr;
     b.binBases = b.sampleBases ? b.sampleBases + 2 * nf : nullptr;
-    const size_t Ss = (size_t)std::max(S, 1), Ts = (size_t)std::max(T, 1), Ps = (size_t)std::max(P, 1);
+    const size_t Ss = (size_t)std::max(S, 1ll), Ts = (size_t)std::max(T, 1ll), Ps = (size_t)std::max(P, 1ll);
     b.keysA = (uint32_t *)take(4 * Ss);
     b.valsA = (uint32_t *)take(4 * Ss);
     b.keysB = (uint32_t *)take(4 * Ss);
@@ -146,7 +172,7 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int S, int T, int NB, int P, b
     const size_t tiles = (std::max(Ss, Ps) + fdzb::kSortTileHost - 1) / fdzb::kSortTileHost;
     b.sortStatusTiles = tiles;
     b.sortStatus = (unsigned long long *)take(8 * 256 * tiles);
-    b.itemCapacity = (int)(Ss / 32 + (size_t)NB + 1);
+    b.itemCapacity = (int)(Ss / 32 + (size_t)NB + (size_t)nf + 1);
     b.items = (int4 *)take(16 * (size_t)b.itemCapacity);
     b.dbgKeys = b.dbgVals = b.dbgPKeys = b.dbgPVals = nullptr;
     if (debug) {
@@ -158,129 +184,272 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int S, int T, int NB, int P, b
     return align_up(off, 256);
 }
 
-int ensure_arena(fdzb_ctx *c, int S, int T, int NB, int P)
+void drop_graph(Engine &e)
+{
+    if (e.graph) cudaGraphExecDestroy(e.graph);
+    e.graph = nullptr;
+    e.graphKey = GraphKey{};
+}
+
+int ensure_arena(Engine &e, int nf, long long S, long long T, long long NB, long long P)
 {
     fdzb::DeviceBuffers probe{};
-    const size_t need = layout(probe, nullptr, S, T, NB, P, c->debug != 0);
-    if (need > c->arenaBytes) {
-        if (c->arena) {
-            cudaStreamSynchronize(c->stream);
-            cudaFree(c->arena);
-            c->arena = nullptr;
-            c->arenaBytes = 0;
+    const size_t need = layout(probe, nullptr, nf, S, T, NB, P, e.debug != 0);
+    if (need > e.arenaBytes) {
+        if (e.arena) {
+            cudaStreamSynchronize(e.stream);
+            drop_graph(e);
+            cudaFree(e.arena);
+            e.arena = nullptr;
+            e.arenaBytes = 0;
         }
         const size_t bytes = align_up(need + need / 8, 1 << 20);
-        cudaError_t e = cudaMalloc(&c->arena, bytes);
-        if (e != cudaSuccess) {
-            c->arena = nullptr;
+        cudaError_t err = cudaMalloc(&e.arena, bytes);
+        if (err != cudaSuccess) {
+            e.arena = nullptr;
             cudaGetLastError();
             return fail(FDZB_ERR_NO_MEMORY, "device arena of " + std::to_string(bytes) +
-                                                " bytes: " + cudaGetErrorString(e));
+                                                " bytes: " + cudaGetErrorString(err));
         }
-        c->arenaBytes = bytes;
-        // look-back status words are epoch-tagged; start from a clean slate
-        FDZB_CUDA(cudaMemsetAsync(c->arena, 0, bytes, c->stream));
+        e.arenaBytes = bytes;
+        // look-back status words are tagged with the launch number; start clean
+        FDZB_CUDA(cudaMemsetAsync(e.arena, 0, bytes, e.stream));
     }
-    layout(c->buf, (char *)c->arena, S, T, NB, P, c->debug != 0);
+    layout(e.buf, (char *)e.arena, nf, S, T, NB, P, e.debug != 0);
     return FDZB_OK;
 }
 
-int ready(fdzb_ctx *c)
+int ensure_host(Engine &e, int nf)
 {
-    if (c->W <= 0 || c->H <= 0) return fail(FDZB_ERR_NOT_READY, "view size not set (fdzb_set_view)");
-    if (!c->pos || !c->nrm) return fail(FDZB_ERR_NOT_READY, "sample buffers not set");
-    if (!c->shadow) return fail(FDZB_ERR_NOT_READY, "output buffer not set");
-    if (c->models.empty()) return fail(FDZB_ERR_NOT_READY, "no model added");
-    if (!c->lightSet) return fail(FDZB_ERR_NOT_READY, "area light not set");
+    if (nf <= e.hCap) return FDZB_OK;
+    if (e.pending) cudaStreamSynchronize(e.stream);
+    drop_graph(e);
+    if (e.hFrames) cudaFreeHost(e.hFrames);
+    if (e.hStates) cudaFreeHost(e.hStates);
+    if (e.hBases) cudaFreeHost(e.hBases);
+    e.hFrames = nullptr;
+    e.hStates = nullptr;
+    e.hBases = nullptr;
+    e.hCap = 0;
+    const int cap = std::max(nf, 1);
+    FDZB_CUDA(cudaMallocHost(&e.hFrames, sizeof(fdzb::FrameDesc) * cap));
+    FDZB_CUDA(cudaMallocHost(&e.hStates, sizeof(fdzb::FrameState) * cap));
+    FDZB_CUDA(cudaMallocHost(&e.hBases, sizeof(int) * 3 * cap));
+    e.hCap = cap;
     return FDZB_OK;
 }
 
-int enqueue(fdzb_ctx *c)
+int engine_init(Engine &e, int device)
 {
-    int rc = ready(c);
-    if (rc) return rc;
-    const Model &m = c->models[0];
-    const long long S = (long long)c->W * c->H;
-    if (S > 0x7fffffffll / 2) return fail(FDZB_ERR_INVALID_ARG, "view too large");
-    if (m.nt > 0x3fffffffull || m.nv > 0x3fffffffull) return fail(FDZB_ERR_INVALID_ARG, "model too large");
-    const int T = (int)m.nt, V = (int)m.nv;
-    const int NB = c->bins * c->bins;
-    if (c->pairCapacity <= 0) {
-        long long guess = std::max<long long>(1 << 20, (long long)T * 64);
-        c->pairCapacity = (int)std::min<long long>(guess, 1ll << 29);
+    if (device < 0) {
+        FDZB_CUDA(cudaGetDevice(&e.device));
+    } else {
+        e.device = device;
     }
-    rc = ensure_arena(c, (int)S, T, NB, c->pairCapacity);
-    if (rc) return rc;
-    fdzb::DeviceBuffers &b = c->buf;
-    b.samplePasses = fdzb::sort_passes_for((long long)NB + 1);
+    FDZB_CUDA(cudaSetDevice(e.device));
+    FDZB_CUDA(cudaStreamCreateWithFlags(&e.ownStream, cudaStreamNonBlocking));
+    e.stream = e.ownStream;
+    FDZB_CUDA(cudaEventCreate(&e.ev0));
+    FDZB_CUDA(cudaEventCreate(&e.ev1));
+    for (auto &ev : e.stageEv) FDZB_CUDA(cudaEventCreate(&ev));
+    FDZB_CUDA(cudaMallocHost(&e.hCounters, sizeof(fdzb::Counters)));
+    return ensure_host(e, 1);
+}
+
+void engine_release(Engine &e)
+{
+    if (e.stream) cudaStreamSynchronize(e.stream);
+    drop_graph(e);
+    if (e.arena) cudaFree(e.arena);
+    if (e.hFrames) cudaFreeHost(e.hFrames);
+    if (e.hStates) cudaFreeHost(e.hStates);
+    if (e.hBases) cudaFreeHost(e.hBases);
+    if (e.hCounters) cudaFreeHost(e.hCounters);
+    if (e.ev0) cudaEventDestroy(e.ev0);
+    if (e.ev1) cudaEventDestroy(e.ev1);
+    for (auto &ev : e.stageEv)
+        if (ev) cudaEventDestroy(ev);
+    if (e.ownStream) cudaStreamDestroy(e.ownStream);
+    e = Engine{};
+}
+
+// Checks one frame's inputs (the conditions FD:: assumes of its callers).
+int check_frame(const FrameSpec &f, int i)
+{
+    const std::string at = "frame " + std::to_string(i) + ": ";
+    if (f.W <= 0 || f.H <= 0 || (long long)f.W * f.H > (1ll << 30)) return fail(FDZB_ERR_INVALID_ARG, at + "bad view size");
+    if (!f.pos || !f.nrm) return fail(FDZB_ERR_NOT_READY, at + "sample buffers not set");
+    if (((uintptr_t)f.pos & 15) || ((uintptr_t)f.nrm & 15))
+        return fail(FDZB_ERR_INVALID_ARG, at + "sample buffers must be 16-byte aligned float4 arrays");
+    if (!f.shadow) return fail(FDZB_ERR_NOT_READY, at + "output buffer not set");
+    if ((f.nv && !f.vtx) || (f.nt && !f.idx)) return fail(FDZB_ERR_INVALID_ARG, at + "NULL model buffer");
+    if (f.strideBytes < 12 || f.strideBytes % 4)
+        return fail(FDZB_ERR_INVALID_ARG, at + "vertex stride must be >= 12 and a multiple of 4 bytes");
+    if (f.nt > 0x3fffffffull || f.nv > 0x3fffffffull) return fail(FDZB_ERR_INVALID_ARG, at + "model too large");
+    if (f.bins < 1 || f.bins > fdzb::kMaxBins || (f.bins & (f.bins - 1)))
+        return fail(FDZB_ERR_INVALID_ARG, at + "bin number must be a power of two in [1, 512]");
+    if (f.light.N < 1 || f.light.N > fdzb::kMaxLightN) return fail(FDZB_ERR_UNSUPPORTED, at + "light grid N out of [1, 32]");
+    return FDZB_OK;
+}
+
+// Fills the pinned frame table and enqueues copies, the pipeline and the
+// read-back of counters and frame states (captured into a graph or not).
+cudaError_t enqueue_body(Engine &e, int nf)
+{
+    fdzb::DeviceBuffers &b = e.buf;
+    cudaStream_t s = e.stream;
+    cudaError_t err;
+    if ((err = cudaMemcpyAsync(b.frames, e.hFrames, sizeof(fdzb::FrameDesc) * nf, cudaMemcpyHostToDevice, s))) return err;
+    if ((err = cudaMemcpyAsync(b.sampleBases, e.hBases, 3 * sizeof(int) * nf, cudaMemcpyHostToDevice, s))) return err;
+    if ((err = cudaMemsetAsync(b.counters, 0, sizeof(fdzb::Counters), s))) return err;
+    if ((err = cudaMemsetAsync(b.sortHist, 0, 8 * 256 * sizeof(uint32_t), s))) return err;
+    if ((err = fdzb::run_pipeline(b, e.maxS, e.maxT, e.maxV, s, e.profile ? e.stageEv : nullptr, &e.launches))) return err;
+    if ((err = cudaMemcpyAsync(e.hCounters, b.counters, sizeof(fdzb::Counters), cudaMemcpyDeviceToHost, s))) return err;
+    return cudaMemcpyAsync(e.hStates, b.states, sizeof(fdzb::FrameState) * nf, cudaMemcpyDeviceToHost, s);
+}
+
+int engine_enqueue(Engine &e)
+{
+    const int nf = (int)e.frames.size();
+    if (nf <= 0) return fail(FDZB_ERR_INVALID_ARG, "no frames");
+    long long S = 0, T = 0, NB = 0;
+    int maxS = 0, maxT = 0, maxV = 0;
+    for (int i = 0; i < nf; ++i) {
+        const FrameSpec &f = e.frames[i];
+        if (int rc = check_frame(f, i)) return rc;
+        const long long s = (long long)f.W * f.H;
+        S += s;
+        T += (long long)f.nt;
+        NB += (long long)f.bins * f.bins;
+        maxS = std::max<int>(maxS, (int)s);
+        maxT = std::max<int>(maxT, (int)f.nt);
+        maxV = std::max<int>(maxV, (int)f.nv);
+    }
+    if (S > kMaxTotalSamples) return fail(FDZB_ERR_INVALID_ARG, "too many samples in one launch");
+    if (T > 0x3fffffffll) return fail(FDZB_ERR_INVALID_ARG, "too many triangles in one launch");
+    if (NB > kMaxTotalBins) return fail(FDZB_ERR_INVALID_ARG, "too many light-plane bins in one launch");
+    if (nf > 65535) return fail(FDZB_ERR_INVALID_ARG, "too many frames in one launch (max 65535)");
+    if (e.pairCapacity <= 0) e.pairCapacity = std::min(std::max<long long>(1 << 20, T * 64), kMaxPairCapacity);
+    if (int rc = ensure_host(e, nf)) return rc;
+    if (int rc = ensure_arena(e, nf, S, T, NB, e.pairCapacity)) return rc;
+    e.maxS = maxS;
+    e.maxT = maxT;
+    e.maxV = maxV;
+    fdzb::DeviceBuffers &b = e.buf;
+    b.samplePasses = fdzb::sort_passes_for(NB + 1);
     // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
     // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
     // order appends a depth bucket below the bin so each bin lists its lowest
     // triangles first, which fills the masks in far fewer pair tests; it uses the
     // key bits left over in the last radix pass, at least 4.
     {
-        int binBits = 0;
-        while ((1ll << binBits) < (long long)NB) ++binBits;
-        if (c->triOrder == FDZB_TRI_ORDER_DEPTH) {
+        const int binBits = ceil_log2(NB);
+        if (e.triOrder == FDZB_TRI_ORDER_DEPTH) {
             const int passes = (binBits + 4 + 7) / 8;
             b.depthBits = std::min(10, passes * 8 - binBits);
         } else {
             b.depthBits = 0;
         }
-        b.pairPasses = fdzb::sort_passes_for((long long)NB << b.depthBits);
+        b.pairPasses = fdzb::sort_passes_for(NB << b.depthBits);
     }
-    b.epoch = ++c->epoch;
-
-    fdzb::FrameDesc &f = *c->hFrame;
-    std::memset(&f, 0, sizeof(f));
-    f.pos = c->pos;
-    f.nrm = c->nrm;
-    f.vtx = m.vtx;
-    f.idx = m.idx;
-    f.shadow = c->shadow;
-    f.masks = c->masks;
-    f.W = c->W;
-    f.H = c->H;
-    f.log2up = ceil_log2(c->W);
-    f.V = V;
-    f.vstride = (int)(m.strideBytes / 4);
-    f.T = T;
-    f.Wb = c->bins;
-    f.log2Wb = ceil_log2(c->bins);
-    f.numBins = NB;
-    f.cull = c->cull;
-    f.esp = c->esp;
-    f.maskWords = (c->light.N * c->light.N + 31) / 32;
-    f.sampleBase = 0;
-    f.triBase = 0;
-    f.binBase = 0;
-    f.light = c->light;
-    c->hBases[0] = 0;
-    c->hBases[1] = 0;
-    c->hBases[2] = 0;
-
-    FDZB_CUDA(cudaMemcpyAsync(b.frames, c->hFrame, sizeof(fdzb::FrameDesc), cudaMemcpyHostToDevice, c->stream));
-    FDZB_CUDA(cudaMemcpyAsync(b.sampleBases, c->hBases, 3 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    FDZB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(fdzb::Counters), c->stream));
-    FDZB_CUDA(cudaMemsetAsync(b.sortHist, 0, 8 * 256 * sizeof(uint32_t), c->stream));
-    FDZB_CUDA(cudaEventRecord(c->ev0, c->stream));
-    FDZB_CUDA(fdzb::run_pipeline(b, (int)S, T, V, c->stream, c->profile ? c->stageEv : nullptr,
-                                 &c->launches));
-    FDZB_CUDA(cudaEventRecord(c->ev1, c->stream));
-    FDZB_CUDA(cudaMemcpyAsync(c->hCounters, b.counters, sizeof(fdzb::Counters), cudaMemcpyDeviceToHost, c->stream));
-    FDZB_CUDA(cudaMemcpyAsync(c->hState, b.states, sizeof(fdzb::FrameState), cudaMemcpyDeviceToHost, c->stream));
-    c->pending = true;
+    int sb = 0, tb = 0, bb = 0;
+    for (int i = 0; i < nf; ++i) {
+        const FrameSpec &s = e.frames[i];
+        fdzb::FrameDesc &f = e.hFrames[i];
+        std::memset(&f, 0, sizeof(f));
+        f.pos = s.pos;
+        f.nrm = s.nrm;
+        f.vtx = s.vtx;
+        f.idx = s.idx;
+        f.shadow = s.shadow;
+        f.masks = s.masks;
+        f.W = s.W;
+        f.H = s.H;
+        f.log2up = ceil_log2(s.W);
+        f.V = (int)s.nv;
+        f.vstride = (int)(s.strideBytes / 4);
+        f.T = (int)s.nt;
+        f.Wb = s.bins;
+        f.log2Wb = ceil_log2(s.bins);
+        f.numBins = s.bins * s.bins;
+        f.cull = s.cull;
+        f.esp = s.esp;
+        f.maskWords = (s.light.N * s.light.N + 31) / 32;
+        f.sampleBase = sb;
+        f.triBase = tb;
+        f.binBase = bb;
+        f.light = s.light;
+        e.hBases[i] = sb;
+        e.hBases[nf + i] = tb;
+        e.hBases[2 * nf + i] = bb;
+        sb += s.W * s.H;
+        tb += (int)s.nt;
+        bb += s.bins * s.bins;
+    }
+    const bool legacy = e.stream == nullptr || e.stream == cudaStreamLegacy || e.stream == cudaStreamPerThread;
+    const bool graphable = e.useGraph && !e.profile && !e.debug && !legacy;
+    if (graphable) {
+        GraphKey k;
+        k.nf = nf;
+        k.S = (int)S;
+        k.T = (int)T;
+        k.NB = (int)NB;
+        k.P = (int)e.pairCapacity;
+        k.sp = b.samplePasses;
+        k.pp = b.pairPasses;
+        k.db = b.depthBits;
+        k.maxS = maxS;
+        k.maxT = maxT;
+        k.maxV = maxV;
+        k.arena = e.arena;
+        k.hFrames = e.hFrames;
+        k.stream = e.stream;
+        if (!e.graph || !(k == e.graphKey)) {
+            drop_graph(e);
+            FDZB_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t body = enqueue_body(e, nf);
+            cudaGraph_t g = nullptr;
+            cudaError_t end = cudaStreamEndCapture(e.stream, &g);
+            if (body != cudaSuccess || end != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return fail(FDZB_ERR_CUDA, std::string("graph capture: ") +
+                                               cudaGetErrorString(body != cudaSuccess ? body : end));
+            }
+            cudaError_t inst = cudaGraphInstantiate(&e.graph, g, 0);
+            cudaGraphDestroy(g);
+            if (inst != cudaSuccess) {
+                e.graph = nullptr;
+                return fail(FDZB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(inst));
+            }
+            e.graphKey = k;
+            ++e.graphCaptures;
+        } else {
+            ++e.graphReplays;
+        }
+        FDZB_CUDA(cudaEventRecord(e.ev0, e.stream));
+        FDZB_CUDA(cudaGraphLaunch(e.graph, e.stream));
+        FDZB_CUDA(cudaEventRecord(e.ev1, e.stream));
+        e.lastFromGraph = true;
+    } else {
+        FDZB_CUDA(cudaEventRecord(e.ev0, e.stream));
+        FDZB_CUDA(enqueue_body(e, nf));
+        FDZB_CUDA(cudaEventRecord(e.ev1, e.stream));
+        e.lastFromGraph = false;
+    }
+    e.pending = true;
     return FDZB_OK;
 }
 
-int sync_frame(fdzb_ctx *c)
+int engine_sync(Engine &e)
 {
-    if (!c->pending) return FDZB_OK;
-    int replans = 0;
+    if (!e.pending) return FDZB_OK;
+    e.replans = 0;
     for (;;) {
-        FDZB_CUDA(cudaStreamSynchronize(c->stream));
-        c->pending = false;
-        const fdzb::Counters &k = *c->hCounters;
+        cudaError_t w = cudaStreamSynchronize(e.stream);
+        e.pending = false;
+        if (w != cudaSuccess) return fail(FDZB_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(w));
+        const fdzb::Counters &k = *e.hCounters;
         if (k.errorFlags & fdzb::ERR_LOOKBACK_TIMEOUT)
             return fail(FDZB_ERR_DEVICE_TIMEOUT, "a look-back wait exceeded its spin limit");
         if (k.errorFlags & fdzb::ERR_MBAR_TIMEOUT)
@@ -290,88 +459,230 @@ int sync_frame(fdzb_ctx *c)
         if (k.errorFlags & fdzb::ERR_INTERNAL)
             return fail(FDZB_ERR_CUDA, "internal consistency check failed on the device");
         if (!k.pairOverflow) break;
-        if (replans >= 3 || k.pairCount >= (1 << 29))
-            return fail(FDZB_ERR_CAPACITY, "triangle/bin pair buffer overflow (" +
-                                               std::to_string(k.pairCount) + " pairs)");
-        c->pairCapacity = (int)std::min<long long>((long long)k.pairCount + k.pairCount / 4 + 1024, 1ll << 29);
-        ++replans;
-        int rc = enqueue(c);
-        if (rc) return rc;
+        if (e.replans >= 3 || k.pairCount >= kMaxPairCapacity)
+            return fail(FDZB_ERR_CAPACITY, "triangle/bin pair buffer overflow (" + std::to_string(k.pairCount) +
+                                               " pairs)");
+        e.pairCapacity = std::min<long long>((long long)k.pairCount + k.pairCount / 4 + 1024, kMaxPairCapacity);
+        ++e.replans;
+        const int replans = e.replans;
+        if (int rc = engine_enqueue(e)) return rc;
+        e.replans = replans;
     }
     float ms = 0.f;
-    FDZB_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    c->lastMs = ms;
-    const fdzb::FrameState &s = *c->hState;
-    const fdzb::Counters &k = *c->hCounters;
-    fdzb_frame_stats &o = c->stats;
+    FDZB_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
+    e.lastMs = ms;
+    return FDZB_OK;
+}
+
+// Statistics of frame i of the last completed launch.
+void frame_stats(const Engine &e, int i, fdzb_frame_stats &o)
+{
+    const fdzb::FrameState &s = e.hStates[i];
+    const fdzb::Counters &k = *e.hCounters;
+    const FrameSpec &f = e.frames[i];
+    const bool single = e.frames.size() == 1;
     std::memset(&o, 0, sizeof(o));
     o.state = (s.state == 2 && s.nValidTris == 0) ? 1 : s.state;
     o.valid_samples = o.state == 2 ? s.nValidSamples : 0;
     o.valid_triangles = s.state == 2 ? s.nValidTris : 0;
-    o.num_pairs = o.state == 2 ? k.pairCount : 0;
-    o.num_bins = c->bins * c->bins;
-    o.pair_capacity = c->pairCapacity;
-    o.pair_tests = (int64_t)k.pairTests;
+    // launch-wide counters: per frame only when the launch holds one frame
+    o.num_pairs = single ? (o.state == 2 ? k.pairCount : 0) : -1;
+    o.num_bins = f.bins * f.bins;
+    o.pair_capacity = (int)e.pairCapacity;
+    o.pair_tests = single ? (int64_t)k.pairTests : -1;
     o.f = s.f;
     o.sub[0] = s.subx;
     o.sub[1] = s.suby;
     o.lp_begin[0] = s.Bx; o.lp_begin[1] = s.By; o.lp_begin[2] = s.Bz;
     o.lp_end[0] = s.Ex; o.lp_end[1] = s.Ey; o.lp_end[2] = s.Ez;
     o.lp_factor[0] = s.fx; o.lp_factor[1] = s.fy;
-    for (int i = 0; i < 6; ++i) {
-        o.sample_aabb[i] = s.sampleAabb[i];
-        o.model_aabb[i] = s.modelAabb[i];
+    for (int j = 0; j < 6; ++j) {
+        o.sample_aabb[j] = s.sampleAabb[j];
+        o.model_aabb[j] = s.modelAabb[j];
     }
-    o.replans = replans;
+    o.replans = e.replans;
     o.quirk_key_range = s.quirkKeyRange;
-    o.kernel_launches = c->launches;
+    o.kernel_launches = e.launches;
+    o.rows_evaluated = single ? (int64_t)k.rowsEvaluated : -1;
+    o.partial_masks = single ? (int64_t)k.partialMasks : -1;
+    for (int j = 0; j < fdzb::STAGE_COUNT; ++j) {
+        float t = 0.f;
+        if (e.profile) cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
+        o.stage_ms[j] = t;
+    }
+}
+
+void launch_stats(const Engine &e, fdzb_frame_stats &o)
+{
+    const fdzb::Counters &k = *e.hCounters;
+    std::memset(&o, 0, sizeof(o));
+    o.state = 2;
+    long long vs = 0, vt = 0, nb = 0;
+    for (size_t i = 0; i < e.frames.size(); ++i) {
+        const fdzb::FrameState &s = e.hStates[i];
+        if (s.state == 2 && s.nValidTris > 0) {
+            vs += s.nValidSamples;
+            vt += s.nValidTris;
+        }
+        o.quirk_key_range += s.quirkKeyRange;
+        nb += (long long)e.frames[i].bins * e.frames[i].bins;
+    }
+    o.valid_samples = (int32_t)std::min<long long>(vs, 0x7fffffff);
+    o.valid_triangles = (int32_t)std::min<long long>(vt, 0x7fffffff);
+    o.num_pairs = k.pairCount;
+    o.num_bins = (int32_t)nb;
+    o.pair_capacity = (int)e.pairCapacity;
+    o.pair_tests = (int64_t)k.pairTests;
+    o.replans = e.replans;
+    o.kernel_launches = e.launches;
     o.rows_evaluated = (int64_t)k.rowsEvaluated;
     o.partial_masks = (int64_t)k.partialMasks;
-    for (int i = 0; i < fdzb::STAGE_COUNT; ++i) {
+    for (int j = 0; j < fdzb::STAGE_COUNT; ++j) {
         float t = 0.f;
-        if (c->profile) cudaEventElapsedTime(&t, c->stageEv[i], c->stageEv[i + 1]);
-        o.stage_ms[i] = t;
+        if (e.profile) cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
+        o.stage_ms[j] = t;
     }
+}
+
+}  // namespace
+
+// ---- FD-shaped context: one scene, one view, one light -----------------------
+
+struct fdzb_ctx {
+    Engine eng;
+    // knobs (defaults of K/FourD.cu:61-62 and FS/constants.h:13)
+    int cull = 1;
+    float esp = 1e-6f;
+    int bins = 16;
+    int W = 0, H = 0;
+    size_t maxTri = 0, maxVert = 0;
+    const float4 *pos = nullptr, *nrm = nullptr;
+    float *shadow = nullptr;
+    uint32_t *masks = nullptr;
+    std::vector<Model> models;
+    bool lightSet = false;
+    fdzb_area_light_desc lightDesc{};
+    fdzb::LightParams light{};
+    fdzb_frame_stats stats{};
+};
+
+// ---- batch: a list of independent frames per launch --------------------------
+
+namespace {
+
+// Autotuner table: bins per side for a size class (log2 samples, log2
+// triangles, light grid N).
+using TuneKey = std::tuple<int, int, int>;
+
+TuneKey tune_key(long long S, long long T, int N)
+{
+    return TuneKey(ceil_log2(std::max(S, 1ll)), ceil_log2(std::max(T, 1ll)), N);
+}
+
+// Starting point of the autotuner: about 128 samples per bin on the light plane
+// (the HD frame's 1920x1080 samples over 128 x 128 bins), clamped to [8, 256].
+int heuristic_bins(long long S)
+{
+    const double side = std::sqrt((double)std::max(S, 1ll) / 128.0);
+    int b = 8;
+    while (b < 256 && b * 2 <= side * 1.41421356) b *= 2;
+    return b;
+}
+
+}  // namespace
+
+struct fdzb_batch {
+    Engine eng;
+    int triOrder = FDZB_TRI_ORDER_DEPTH;
+    std::map<TuneKey, int> tuned;
+    std::vector<int> chosenBins;
+    long long tuneLaunches = 0;
+};
+
+namespace {
+
+int ctx_check(fdzb_ctx *c)
+{
+    if (!c) return fail(FDZB_ERR_NOT_INITIALIZED, "context not initialised (call fdzb_init)");
     return FDZB_OK;
 }
 
-int ctx_init_resources(fdzb_ctx *c, int device)
+int batch_check(fdzb_batch *b)
 {
-    if (device < 0) {
-        FDZB_CUDA(cudaGetDevice(&c->device));
-    } else {
-        c->device = device;
-    }
-    FDZB_CUDA(cudaSetDevice(c->device));
-    FDZB_CUDA(cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking));
-    c->stream = c->ownStream;
-    FDZB_CUDA(cudaEventCreate(&c->ev0));
-    FDZB_CUDA(cudaEventCreate(&c->ev1));
-    for (auto &e : c->stageEv) FDZB_CUDA(cudaEventCreate(&e));
-    FDZB_CUDA(cudaMallocHost(&c->hFrame, sizeof(fdzb::FrameDesc)));
-    FDZB_CUDA(cudaMallocHost(&c->hCounters, sizeof(fdzb::Counters)));
-    FDZB_CUDA(cudaMallocHost(&c->hState, sizeof(fdzb::FrameState)));
-    FDZB_CUDA(cudaMallocHost(&c->hBases, 4 * sizeof(int)));
+    if (!b) return fail(FDZB_ERR_NOT_INITIALIZED, "batch is NULL");
     return FDZB_OK;
 }
 
-void ctx_release(fdzb_ctx *c)
+int ctx_frame(fdzb_ctx *c, FrameSpec &f)
 {
-    if (!c) return;
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->arena) cudaFree(c->arena);
-    if (c->hFrame) cudaFreeHost(c->hFrame);
-    if (c->hCounters) cudaFreeHost(c->hCounters);
-    if (c->hState) cudaFreeHost(c->hState);
-    if (c->hBases) cudaFreeHost(c->hBases);
-    if (c->ev0) cudaEventDestroy(c->ev0);
-    if (c->ev1) cudaEventDestroy(c->ev1);
-    for (auto &e : c->stageEv)
-        if (e) cudaEventDestroy(e);
-    if (c->ownStream) cudaStreamDestroy(c->ownStream);
-    delete c;
+    if (c->W <= 0 || c->H <= 0) return fail(FDZB_ERR_NOT_READY, "view size not set (fdzb_set_view)");
+    if (!c->pos || !c->nrm) return fail(FDZB_ERR_NOT_READY, "sample buffers not set");
+    if (!c->shadow) return fail(FDZB_ERR_NOT_READY, "output buffer not set");
+    if (c->models.empty()) return fail(FDZB_ERR_NOT_READY, "no model added");
+    if (!c->lightSet) return fail(FDZB_ERR_NOT_READY, "area light not set");
+    const Model &m = c->models[0];  // only scene 0 / model 0 is drawn (FS/api.cpp:430-445)
+    f.pos = c->pos;
+    f.nrm = c->nrm;
+    f.W = c->W;
+    f.H = c->H;
+    f.vtx = m.vtx;
+    f.nv = m.nv;
+    f.strideBytes = m.strideBytes;
+    f.idx = m.idx;
+    f.nt = m.nt;
+    f.light = c->light;
+    f.bins = c->bins;
+    f.cull = c->cull;
+    f.esp = c->esp;
+    f.shadow = c->shadow;
+    f.masks = c->masks;
+    return FDZB_OK;
 }
 
+int ctx_sync(fdzb_ctx *c)
+{
+    if (!c->eng.pending) return FDZB_OK;
+    if (int rc = engine_sync(c->eng)) return rc;
+    frame_stats(c->eng, 0, c->stats);
+    return FDZB_OK;
+}
+
+int desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
+{
+    const fdzb_area_light_desc &L = d.light;
+    if (L.lightResWidth != L.lightResHeight || L.lightResWidth < 1 || L.lightResWidth > fdzb::kMaxLightN)
+        return fail(FDZB_ERR_UNSUPPORTED, "frame " + std::to_string(i) + ": light grid must be square with N in [1, 32]");
+    f.pos = (const float4 *)d.d_pos;
+    f.nrm = (const float4 *)d.d_nrm;
+    f.W = d.W;
+    f.H = d.H;
+    f.vtx = d.d_vtx;
+    f.nv = d.n_vtx;
+    f.strideBytes = d.vtx_stride_bytes;
+    f.idx = d.d_idx;
+    f.nt = d.n_tri;
+    fdzb::light_setup(L.rightRadius, L.topRadius, L.position, L.viewDir, L.upDir, L.lightResWidth,
+                      L.lightResHeight, &f.light);
+    f.bins = d.bins;
+    f.cull = d.cull;
+    f.esp = d.esp;
+    f.shadow = d.d_shadow;
+    f.masks = d.d_masks;
+    return FDZB_OK;
+}
+
+int batch_bins_for(fdzb_batch *b, const FrameSpec &f)
+{
+    const long long S = (long long)f.W * f.H;
+    auto it = b->tuned.find(tune_key(S, (long long)f.nt, f.light.N));
+    return it != b->tuned.end() ? it->second : heuristic_bins(S);
+}
+
+}  // namespace
+
+int fdzb::set_error(int code, const std::string &msg) { return fail(code, msg); }
+
+namespace {
 fdzb_ctx *g_ctx = nullptr;
 
 bool is_device_pointer(const void *p)
@@ -383,24 +694,22 @@ bool is_device_pointer(const void *p)
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
-
 }  // namespace
-
-int fdzb::set_error(int code, const std::string &msg) { return fail(code, msg); }
 
 extern "C" {
 
 const char *fdzb_last_error(void) { return g_err.c_str(); }
-const char *fdzb_version(void) { return "fdzb-b200 0.1 (sm_100a)"; }
+const char *fdzb_version(void) { return "fdzb-b200 0.2 (sm_100a)"; }
 
 int fdzb_ctx_create(fdzb_ctx **out, int device)
 {
     if (!out) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
     fdzb_ctx *c = new (std::nothrow) fdzb_ctx();
     if (!c) return fail(FDZB_ERR_NO_MEMORY, "host allocation failed");
-    int rc = ctx_init_resources(c, device);
+    int rc = engine_init(c->eng, device);
     if (rc) {
-        ctx_release(c);
+        engine_release(c->eng);
+        delete c;
         return rc;
     }
     *out = c;
@@ -409,28 +718,40 @@ int fdzb_ctx_create(fdzb_ctx **out, int device)
 
 int fdzb_ctx_destroy(fdzb_ctx *c)
 {
-    ctx_release(c);
+    if (!c) return FDZB_OK;
+    engine_release(c->eng);
+    delete c;
     return FDZB_OK;
 }
 
 int fdzb_ctx_set_stream(fdzb_ctx *c, void *stream)
 {
     if (int rc = ctx_check(c)) return rc;
-    c->stream = stream ? (cudaStream_t)stream : c->ownStream;
+    if (int rc = ctx_sync(c)) return rc;
+    c->eng.stream = stream ? (cudaStream_t)stream : c->eng.ownStream;
     return FDZB_OK;
 }
 
 int fdzb_ctx_set_debug(fdzb_ctx *c, int flags)
 {
     if (int rc = ctx_check(c)) return rc;
-    c->debug = flags & 1;
+    c->eng.debug = flags & 1;
     return FDZB_OK;
 }
 
 int fdzb_ctx_set_profiling(fdzb_ctx *c, int enable)
 {
     if (int rc = ctx_check(c)) return rc;
-    c->profile = enable != 0;
+    c->eng.profile = enable != 0;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_graph(fdzb_ctx *c, int enable)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (int rc = ctx_sync(c)) return rc;
+    c->eng.useGraph = enable != 0;
+    if (!c->eng.useGraph) drop_graph(c->eng);
     return FDZB_OK;
 }
 
@@ -446,7 +767,7 @@ int fdzb_ctx_set_tri_order(fdzb_ctx *c, int order)
     if (int rc = ctx_check(c)) return rc;
     if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_DEPTH)
         return fail(FDZB_ERR_INVALID_ARG, "unknown triangle order");
-    c->triOrder = order;
+    c->eng.triOrder = order;
     return FDZB_OK;
 }
 
@@ -543,36 +864,37 @@ int fdzb_ctx_move_model(fdzb_ctx *c, const float m[16])
     if (int rc = ctx_check(c)) return rc;
     if (!m) return fail(FDZB_ERR_INVALID_ARG, "matrix is NULL");
     if (c->models.empty()) return fail(FDZB_ERR_NOT_READY, "no model added");
-    if (int rc = sync_frame(c)) return rc;
+    if (int rc = ctx_sync(c)) return rc;
     const Model &md = c->models[0];
-    FDZB_CUDA(fdzb::run_move_model(const_cast<float *>(md.vtx), (int)(md.strideBytes / 4), (int)md.nv, m, c->stream));
-    FDZB_CUDA(cudaStreamSynchronize(c->stream));
+    FDZB_CUDA(fdzb::run_move_model(const_cast<float *>(md.vtx), (int)(md.strideBytes / 4), (int)md.nv, m,
+                                   c->eng.stream));
+    FDZB_CUDA(cudaStreamSynchronize(c->eng.stream));
     return FDZB_OK;
 }
 
 int fdzb_ctx_launch_async(fdzb_ctx *c)
 {
     if (int rc = ctx_check(c)) return rc;
-    if (c->pending) {
-        int rc = sync_frame(c);
-        if (rc) return rc;
-    }
-    return enqueue(c);
+    if (int rc = ctx_sync(c)) return rc;
+    FrameSpec f;
+    if (int rc = ctx_frame(c, f)) return rc;
+    c->eng.frames.assign(1, f);
+    return engine_enqueue(c->eng);
 }
 
 int fdzb_ctx_sync(fdzb_ctx *c)
 {
     if (int rc = ctx_check(c)) return rc;
-    return sync_frame(c);
+    return ctx_sync(c);
 }
 
 int fdzb_ctx_launch(fdzb_ctx *c, float *ms)
 {
     int rc = fdzb_ctx_launch_async(c);
     if (rc) return rc;
-    rc = sync_frame(c);
+    rc = ctx_sync(c);
     if (rc) return rc;
-    if (ms) *ms = c->lastMs;
+    if (ms) *ms = c->eng.lastMs;
     return FDZB_OK;
 }
 
@@ -588,11 +910,11 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
 {
     if (int rc = ctx_check(c)) return rc;
     if (!dst) return fail(FDZB_ERR_INVALID_ARG, "dst is NULL");
-    if (!c->arena) return fail(FDZB_ERR_NOT_READY, "no launch yet");
-    if (int rc = sync_frame(c)) return rc;
-    const fdzb::DeviceBuffers &b = c->buf;
+    if (!c->eng.arena) return fail(FDZB_ERR_NOT_READY, "no launch yet");
+    if (int rc = ctx_sync(c)) return rc;
+    const fdzb::DeviceBuffers &b = c->eng.buf;
     const size_t S = (size_t)b.totalSamples, T = (size_t)b.totalTris, NB = (size_t)b.totalBins;
-    const size_t P = (size_t)std::min(c->hCounters->pairCount, b.pairCapacity);
+    const size_t P = (size_t)std::min(c->eng.hCounters->pairCount, b.pairCapacity);
     const bool sOdd = b.samplePasses & 1, pOdd = b.pairPasses & 1;
     const void *src = nullptr;
     size_t avail = 0;
@@ -688,12 +1010,198 @@ int fdzb_light_setup(const fdzb_area_light_desc *d, float mat[16], float rf[2], 
     return FDZB_OK;
 }
 
+// ---- batches -----------------------------------------------------------------
+
+int fdzb_batch_create(fdzb_batch **out, int device)
+{
+    if (!out) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    fdzb_batch *b = new (std::nothrow) fdzb_batch();
+    if (!b) return fail(FDZB_ERR_NO_MEMORY, "host allocation failed");
+    int rc = engine_init(b->eng, device);
+    if (rc) {
+        engine_release(b->eng);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return FDZB_OK;
+}
+
+int fdzb_batch_destroy(fdzb_batch *b)
+{
+    if (!b) return FDZB_OK;
+    engine_release(b->eng);
+    delete b;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_stream(fdzb_batch *b, void *stream)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (int rc = engine_sync(b->eng)) return rc;
+    b->eng.stream = stream ? (cudaStream_t)stream : b->eng.ownStream;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_graph(fdzb_batch *b, int enable)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (int rc = engine_sync(b->eng)) return rc;
+    b->eng.useGraph = enable != 0;
+    if (!b->eng.useGraph) drop_graph(b->eng);
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_profiling(fdzb_batch *b, int enable)
+{
+    if (int rc = batch_check(b)) return rc;
+    b->eng.profile = enable != 0;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_tri_order(fdzb_batch *b, int order)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_DEPTH)
+        return fail(FDZB_ERR_INVALID_ARG, "unknown triangle order");
+    b->eng.triOrder = order;
+    return FDZB_OK;
+}
+
+int fdzb_batch_launch_async(fdzb_batch *b, const fdzb_frame_desc *frames, int n)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (!frames || n <= 0) return fail(FDZB_ERR_INVALID_ARG, "empty frame list");
+    if (int rc = engine_sync(b->eng)) return rc;
+    std::vector<FrameSpec> specs((size_t)n);
+    b->chosenBins.assign((size_t)n, 0);
+    for (int i = 0; i < n; ++i) {
+        if (int rc = desc_to_spec(frames[i], specs[i], i)) return rc;
+        if (specs[i].bins == 0) specs[i].bins = batch_bins_for(b, specs[i]);
+        b->chosenBins[i] = specs[i].bins;
+    }
+    b->eng.frames.swap(specs);
+    return engine_enqueue(b->eng);
+}
+
+int fdzb_batch_sync(fdzb_batch *b, float *ms)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (int rc = engine_sync(b->eng)) return rc;
+    if (ms) *ms = b->eng.lastMs;
+    return FDZB_OK;
+}
+
+int fdzb_batch_launch(fdzb_batch *b, const fdzb_frame_desc *frames, int n, float *ms)
+{
+    if (int rc = fdzb_batch_launch_async(b, frames, n)) return rc;
+    return fdzb_batch_sync(b, ms);
+}
+
+int fdzb_batch_get_frame_stats(fdzb_batch *b, int i, fdzb_frame_stats *out)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (!out) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    if (b->eng.pending) return fail(FDZB_ERR_NOT_READY, "launch not synchronised (fdzb_batch_sync)");
+    if (i < 0 || i >= (int)b->eng.frames.size()) return fail(FDZB_ERR_INVALID_ARG, "frame index out of range");
+    frame_stats(b->eng, i, *out);
+    return FDZB_OK;
+}
+
+int fdzb_batch_get_stats(fdzb_batch *b, fdzb_batch_stats *out)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (!out) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    if (b->eng.pending) return fail(FDZB_ERR_NOT_READY, "launch not synchronised (fdzb_batch_sync)");
+    std::memset(out, 0, sizeof(*out));
+    launch_stats(b->eng, out->totals);
+    out->frames = (int32_t)b->eng.frames.size();
+    out->from_graph = b->eng.lastFromGraph ? 1 : 0;
+    out->graph_captures = b->eng.graphCaptures;
+    out->graph_replays = b->eng.graphReplays;
+    out->tuned_classes = (int32_t)b->tuned.size();
+    out->tune_launches = b->tuneLaunches;
+    out->ms = b->eng.lastMs;
+    return FDZB_OK;
+}
+
+int fdzb_batch_frame_bins(fdzb_batch *b, int i)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (i < 0 || i >= (int)b->chosenBins.size()) return fail(FDZB_ERR_INVALID_ARG, "frame index out of range");
+    return b->chosenBins[i];
+}
+
+// Times candidate bin resolutions for every size class present in `frames`
+// (frames with bins == 0 only) and keeps the fastest.  Each candidate runs as a
+// launch of `reps` copies of the class's first frame (so that it is timed as
+// it runs inside a batch: the GPU full), writing into `d_scratch`
+// (float[scratch_floats]), twice; the faster of the two counts.
+int fdzb_batch_autotune(fdzb_batch *b, const fdzb_frame_desc *frames, int n, float *d_scratch,
+                        size_t scratch_floats)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (!frames || n <= 0) return fail(FDZB_ERR_INVALID_ARG, "empty frame list");
+    if (!d_scratch) return fail(FDZB_ERR_INVALID_ARG, "scratch buffer is NULL");
+    if (int rc = engine_sync(b->eng)) return rc;
+    std::map<TuneKey, int> firstOf;
+    for (int i = 0; i < n; ++i) {
+        if (frames[i].bins != 0) continue;
+        FrameSpec f;
+        if (int rc = desc_to_spec(frames[i], f, i)) return rc;
+        const TuneKey k = tune_key((long long)f.W * f.H, (long long)f.nt, f.light.N);
+        if (!b->tuned.count(k) && !firstOf.count(k)) firstOf[k] = i;
+    }
+    const bool savedGraph = b->eng.useGraph;
+    b->eng.useGraph = false;  // one-off shapes: no point capturing them
+    int rc = FDZB_OK;
+    for (const auto &kv : firstOf) {
+        FrameSpec f;
+        desc_to_spec(frames[kv.second], f, kv.second);
+        const long long S = (long long)f.W * f.H;
+        if ((size_t)S > scratch_floats) {
+            rc = fail(FDZB_ERR_INVALID_ARG, "autotune scratch smaller than a frame");
+            break;
+        }
+        const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, (long long)(scratch_floats / S)}));
+        const int h = heuristic_bins(S);
+        int best = h;
+        float bestMs = 1e30f;
+        for (int cand : {h / 2, h, h * 2}) {
+            if (cand < 4 || cand > fdzb::kMaxBins) continue;
+            std::vector<FrameSpec> specs((size_t)reps, f);
+            for (int r = 0; r < reps; ++r) {
+                specs[r].bins = cand;
+                specs[r].shadow = d_scratch + (size_t)r * S;
+                specs[r].masks = nullptr;
+            }
+            float t = 1e30f;
+            for (int trial = 0; trial < 2 && rc == FDZB_OK; ++trial) {
+                b->eng.frames = specs;
+                rc = engine_enqueue(b->eng);
+                if (rc == FDZB_OK) rc = engine_sync(b->eng);
+                ++b->tuneLaunches;
+                if (rc == FDZB_OK) t = std::min(t, b->eng.lastMs);
+            }
+            if (rc) break;
+            if (t < bestMs) {
+                bestMs = t;
+                best = cand;
+            }
+        }
+        if (rc) break;
+        b->tuned[kv.first] = best;
+    }
+    b->eng.useGraph = savedGraph;
+    return rc;
+}
+
 // ---- reference-shaped global context -----------------------------------------
 
 int fdzb_init(void)
 {
     if (g_ctx) {
-        ctx_release(g_ctx);
+        fdzb_ctx_destroy(g_ctx);
         g_ctx = nullptr;
     }
     return fdzb_ctx_create(&g_ctx, -1);

@@ -119,7 +119,8 @@ struct DeviceBuffers {
     // sorted data lands in the A buffers after an even number of passes, B after odd
     int samplePasses, pairPasses;
     int depthBits;                              // secondary (depth-bucket) bits of the pair key
-    uint32_t epoch;                             // launch sequence number (look-back tags)
+    uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
+                                                // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays
     uint32_t *dbgKeys, *dbgVals, *dbgPKeys, *dbgPVals;
 };

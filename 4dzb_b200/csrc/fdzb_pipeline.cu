@@ -35,9 +35,10 @@ namespace fdzb {
 // segment tables (K/binRaster.inl:39-40, 52-53).
 // ---------------------------------------------------------------------------
 __global__ void k_init(FrameState *states, int nframes, uint32_t *binStat, int32_t *bss,
-                       int32_t *bse, int32_t *bts, int32_t *bte, int totalBins)
+                       int32_t *bse, int32_t *bts, int32_t *bte, int totalBins, uint32_t *epochWord)
 {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) *epochWord += 1u;  // launch number: look-back tags of this launch
     const int stride = gridDim.x * blockDim.x;
     const uint32_t neg = f2o(-kF32Max), pos = f2o(kF32Max);
     for (int b = gid; b < totalBins; b += stride) {
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(kTriThreads)
     k_tri_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int *__restrict__ triBases, int nframes, int totalTris,
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
-                int32_t *__restrict__ triCount, unsigned long long *scanStatus, uint32_t epoch,
+                int32_t *__restrict__ triCount, unsigned long long *scanStatus, const uint32_t *epochWord,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
                 int depthBits, Counters *ctr)
 {
@@ -480,6 +481,7 @@ __global__ void __launch_bounds__(kTriThreads)
     __shared__ unsigned long long s_excl;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (totalTris + kTriThreads - 1) / kTriThreads;
+    const uint32_t epoch = *epochWord;
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&ctr->triTileCounter, 1);
@@ -647,7 +649,7 @@ static int grid_for(long long n, int threads, int cap)
 }
 
 // Sorts (kA, vA) with kB/vB as ping-pong buffers; `slot` selects the histogram
-// and ticket block (0 samples, 1 pairs).  Pass p uses epoch 8*launch + 4*slot + p.
+// and ticket block (0 samples, 1 pairs).  Pass p uses tag 8*launch + 4*slot + p.
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
                      cudaStream_t s)
@@ -659,9 +661,9 @@ static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *v
     const long long tiles = ((long long)cap + kSortTile - 1) / kSortTile;
     const int passGrid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
     for (int p = 0; p < passes; ++p) {
-        const uint32_t ep = b.epoch * 8u + (uint32_t)(slot * 4 + p);
         k_radix_pass<<<passGrid, kSortThreads, 0, s>>>(ki, vi, ko, vo, n_dev, n_static, cap, 8 * p,
-                                                       hist + p * kRadix, b.sortStatus, ep,
+                                                       hist + p * kRadix, b.sortStatus, b.epochWord,
+                                                       (uint32_t)(slot * 4 + p),
                                                        b.counters->sortTileCounter + slot * 4 + p,
                                                        &b.counters->errorFlags);
         uint32_t *t = ki;
@@ -695,7 +697,8 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     if (ev) cudaEventRecord(ev[STAGE_SETUP], s);
     // (a) samples, vertices, triangles
     k_init<<<grid_for(b.totalBins + 1, 256, sm * 8), 256, 0, s>>>(
-        b.states, nf, b.binStat, b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.totalBins);
+        b.states, nf, b.binStat, b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.totalBins,
+        b.epochWord);
     {
         const int gx = grid_for(maxS > maxV ? maxS : maxV, kReduceThreads, sm * 4);
         k_reduce<<<dim3(gx, nf, 2), kReduceThreads, 0, s>>>(b.frames, b.states);
@@ -727,7 +730,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         const int grid = tiles < sm * 4 ? (tiles > 0 ? tiles : 1) : sm * 4;
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
-                                                 b.epoch, b.pkeysA, b.pvalsA, b.pairCapacity,
+                                                 b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
                                                  b.depthBits, b.counters);
         nl += 1;
     }
@@ -908,7 +911,8 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
             uint32_t *ko = toOut ? d_keys_out : tmpK;
             uint32_t *vo = toOut ? d_vals_out : tmpV;
             k_radix_pass<<<grid, kSortThreads, 0, s>>>(ki, vi, ko, vo, nullptr, n, n, 8 * p,
-                                                       hist + p * kRadix, status, epoch * 8u + (uint32_t)p,
+                                                       hist + p * kRadix, status, nullptr,
+                                                       epoch * 8u + (uint32_t)p,
                                                        tickets + p, err);
             ki = ko;
             vi = vo;

@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(kSortThreads)
     k_radix_pass(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                  uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, const int *n_dev,
                  int n_static, int cap, int shift, const uint32_t *__restrict__ hist,
-                 unsigned long long *status, uint32_t epoch, int *ticket, int *err)
+                 unsigned long long *status, const uint32_t *epochWord, uint32_t epochLo, int *ticket,
+                 int *err)
 {
     constexpr int WARPS = kSortThreads / 32;
     __shared__ uint32_t s_start[kRadix];
@@ -67,6 +68,9 @@ __global__ void __launch_bounds__(kSortThreads)
 
     const int n = sort_count(n_dev, n_static, cap);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // look-back tag of this pass: 8 x (launch number, a device word that k_init
+    // advances, so graph replays get fresh tags) + pass slot
+    const uint32_t epoch = (epochWord ? *epochWord * 8u : 0u) + epochLo;
 
     // Exclusive scan of this pass's digit histogram (digit = tid).
     {

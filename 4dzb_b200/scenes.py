@@ -144,3 +144,24 @@ def preset(name: str, **over) -> Scene:
     kw = dict(PRESETS[name])
     kw.update(over)
     return make_scene(name=name, **kw)
+
+
+def batch_frame(k: int, s_range=(256 * 256, 1920 * 1080), t_range=(10_000, 500_000), ns=(8, 16),
+                light_side=(0.5, 4.0), seed_base: int = 1000) -> Scene:
+    """Frame k of the batched workload: an independent scene (seed seed_base + k)
+    whose sample count is log-uniform in s_range (aspect uniform in [1, 16/9]),
+    triangle count log-uniform in t_range, light grid N drawn from ns and light
+    side uniform in light_side; occluders as in the HD frame (sigma 0.1,
+    heights in [0.5, 3]).  bins = 0: left to the autotuner."""
+    seed = seed_base + k
+    u = uniform(seed, 31, 5)
+    S = float(np.exp(np.log(s_range[0]) + u[0] * (np.log(s_range[1]) - np.log(s_range[0]))))
+    aspect = 1.0 + u[1] * (16.0 / 9.0 - 1.0)
+    W = max(1, int(round(np.sqrt(S * aspect))))
+    H = max(1, int(round(S / W)))
+    T = int(round(np.exp(np.log(t_range[0]) + u[2] * (np.log(t_range[1]) - np.log(t_range[0])))))
+    n = int(ns[min(int(u[3] * len(ns)), len(ns) - 1)])
+    side = light_side[0] + u[4] * (light_side[1] - light_side[0])
+    s = make_scene(W, H, T, n=n, bins=0, seed=seed, sigma=0.1, zlo=0.5, zhi=3.0, radius=side / 2.0,
+                   name=f"batch{k}")
+    return s

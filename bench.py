@@ -219,6 +219,108 @@ def reference_arm(args, scene) -> dict:
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> dict:
+    """64 independent frames (resolution log-uniform in [256^2, 1920x1080],
+    triangles log-uniform in [10k, 500k], N in {8, 16}, light side uniform in
+    [0.5, 4]; frame k from seed 1000 + k) through one launch per stage, replayed
+    from a CUDA graph, bins autotuned per size class.  Compared with the plain
+    per-frame loop (one synchronous launch per frame, same kernels, same bins)
+    on the same GPU and inputs; both are device-timed with CUDA events on the
+    launch stream; the inputs (~1.3 GB of samples) are larger than L2."""
+    scenes = importlib.import_module("4dzb_b200.scenes")
+    t0 = time.time()
+    frames = [scenes.batch_frame(k) for k in range(nframes)]
+    gen_s = time.time() - t0
+    dev = []
+    for s in frames:
+        pos, nrm, vtx, idx = fdzb.upload_scene(s)
+        w = fdzb.mask_words(s.light.n)
+        dev.append(dict(pos=pos, nrm=nrm, vtx=vtx, idx=idx,
+                        shadow=torch.empty(s.S, dtype=torch.float32, device="cuda"),
+                        masks=torch.empty(s.S * w, dtype=torch.int32, device="cuda"),
+                        pshadow=torch.empty(s.S, dtype=torch.float32, device="cuda"),
+                        pmasks=torch.empty(s.S * w, dtype=torch.int32, device="cuda")))
+
+    def desc(i, bins, plain=False):
+        s, t = frames[i], dev[i]
+        return fdzb.frame_desc(t["pos"], t["nrm"], s.W, s.H, t["vtx"], s.V, t["idx"], s.T, s.light,
+                               t["pshadow"] if plain else t["shadow"], t["pmasks"] if plain else t["masks"],
+                               bins=bins, cull=False, esp=s.esp)
+
+    bat = fdzb.Batch()
+    bat.set_stream(stream.cuda_stream)
+    d_tune = [desc(i, 0) for i in range(nframes)]
+    scratch = torch.empty(4 << 20, dtype=torch.float32, device="cuda")
+    t0 = time.time()
+    bat.autotune(d_tune, scratch)
+    tune_s = time.time() - t0
+    bat.launch(d_tune)                       # bins from the tuner; captures the graph
+    bins = [bat.frame_bins(i) for i in range(nframes)]
+    d_batch = [desc(i, bins[i]) for i in range(nframes)]
+    for _ in range(2):
+        bat.launch(d_batch)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    batch_ms = []
+    for _ in range(steps):
+        a, b = ev(), ev()
+        a.record(stream)
+        bat.launch_async(d_batch)
+        b.record(stream)
+        bat.sync()
+        stream.synchronize()
+        batch_ms.append(a.elapsed_time(b))
+    bst = bat.stats()
+
+    # plain loop: one frame per synchronous launch (the FDLaunch pattern)
+    plain = fdzb.Batch()
+    plain.set_stream(stream.cuda_stream)
+    plain.set_graph(False)                   # every frame has a new shape: nothing to replay
+    d_plain = [[desc(i, bins[i], plain=True)] for i in range(nframes)]
+    for d in d_plain:                        # warm-up: grows the arena to the largest frame
+        plain.launch(d)
+    plain_ms = []
+    pair_tests = 0
+    for _ in range(max(2, steps // 2)):
+        a, b = ev(), ev()
+        a.record(stream)
+        pair_tests = 0
+        for d in d_plain:
+            plain.launch(d)
+            pair_tests += plain.frame_stats(0)["pair_tests"]
+        b.record(stream)
+        stream.synchronize()
+        plain_ms.append(a.elapsed_time(b))
+    same = all(torch.equal(t["masks"], t["pmasks"]) and torch.equal(t["shadow"], t["pshadow"]) for t in dev)
+    ms_b = statistics.mean(batch_ms)
+    ms_p = statistics.mean(plain_ms)
+    sxt = sum(s.S * s.T for s in frames)
+    hist = {}
+    for g in bins:
+        hist[str(g)] = hist.get(str(g), 0) + 1
+    out = {
+        "workload": f"{nframes} frames: samples log-uniform [256^2, 1920x1080], triangles log-uniform "
+                    "[10k, 500k], N in {8, 16}, light side uniform [0.5, 4], seeds 1000+k",
+        "frames": nframes, "samples": sum(s.S for s in frames), "triangles": sum(s.T for s in frames),
+        "frames_per_s": nframes * 1e3 / ms_b, "ms_per_batch": ms_b,
+        "plain_frames_per_s": nframes * 1e3 / ms_p, "plain_ms_per_loop": ms_p,
+        "speedup_vs_plain": ms_p / ms_b,
+        "pair_tests_per_s": bst["totals"]["pair_tests"] * 1e3 / ms_b,
+        "effective_gpairs_per_s": sxt * 1e3 / ms_b / 1e9,
+        "plain_pair_tests": pair_tests, "batch_pair_tests": bst["totals"]["pair_tests"],
+        "masks_identical": bool(same), "graph": bool(bst["from_graph"]),
+        "graph_replays": bst["graph_replays"], "kernel_launches_per_batch": bst["totals"]["kernel_launches"],
+        "tuned_bins": hist, "tuned_classes": bst["tuned_classes"], "autotune_s": tune_s,
+        "autotune_launches": bst["tune_launches"], "generate_s": gen_s, "steps": steps,
+        "timing": "CUDA events on the launch stream; inputs > L2",
+    }
+    bat.close()
+    plain.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,6 +330,8 @@ def main():
     ap.add_argument("--config", default="hd", choices=["small", "hd", "large"])
     ap.add_argument("--tri-order", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-only", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -249,8 +353,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    scene = scenes.preset(args.config)
     stream = torch.cuda.Stream()
+    if args.batched_only:
+        print(json.dumps(batched_workload(fdzb, torch, stream)), flush=True)
+        return
+    scene = scenes.preset(args.config)
     ctx, t = fdzb.context_for_scene(scene, masks=True, tri_order=args.tri_order)
     ctx.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -334,6 +441,10 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
+    batched = None
+    if ws == 1 and not args.no_batched:
+        ctx.close()
+        batched = batched_workload(fdzb, torch, stream)
 
     peaks = measured_peaks()
     clocks = clk.summary()
@@ -367,6 +478,8 @@ def main():
     }
     if cpu:
         out["cpu_baseline"] = cpu
+    if batched:
+        out["batched"] = batched
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()

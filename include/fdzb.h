@@ -216,6 +216,83 @@ int fdzb_light_setup(const fdzb_area_light_desc *light, float mat[16], float rec
 /* Library version string. */
 const char *fdzb_version(void);
 
+/* CUDA graphs (no counterpart in the reference, which issues each kernel, sort
+ * and read-back of FDLaunch separately, FS/api.cpp:405-575).  On by default: a
+ * launch is captured once per launch shape (frame count, sizes, bin totals,
+ * pair capacity, stream) and replayed while the shape is unchanged.  Graphs
+ * are not used with profiling or debug capture on, or on the legacy default
+ * stream. */
+int fdzb_ctx_set_graph(fdzb_ctx *ctx, int enable);
+
+/* ---- batches: many independent frames per launch ------------------------- */
+
+/* No counterpart in the reference, which renders one frame per FD::FDLaunch
+ * (FS/api.cpp:405-575).  A batch runs a list of independent frames -- each with
+ * its own view samples, triangle soup, light and bin grid -- through one launch
+ * per pipeline stage: the frames' samples, triangles and bins are laid end to
+ * end in HBM and every stage processes all of them at once.  Each frame's
+ * results are identical to a separate fdzb_ctx_launch of the same inputs. */
+typedef struct fdzb_frame_desc {
+    const float *d_pos;            /* float4[W*H] row-major, NaN x = background */
+    const float *d_nrm;            /* float4[W*H] */
+    int32_t W, H;
+    const float *d_vtx;            /* vertices: xyz at the start of every stride */
+    size_t n_vtx;
+    size_t vtx_stride_bytes;
+    const int32_t *d_idx;          /* int3 per triangle */
+    size_t n_tri;
+    fdzb_area_light_desc light;    /* N x N grid, N in [1, 32] */
+    int32_t bins;                  /* bins per side: power of two in [1, 512]; 0 = autotuned */
+    int32_t cull;                  /* back-face culling of triangles (FDsetBackfaceCull) */
+    float esp;                     /* FDsetScenesEsp */
+    float *d_shadow;               /* float[W*H] at y*W+x */
+    uint32_t *d_masks;             /* nullable: uint32[W*H*ceil(N*N/32)], bit i*N+j */
+} fdzb_frame_desc;
+
+typedef struct fdzb_batch fdzb_batch;
+
+typedef struct fdzb_batch_stats {
+    fdzb_frame_stats totals;       /* launch-wide: sums over frames (state = 2) */
+    int32_t frames;
+    int32_t from_graph;            /* last launch replayed or captured a graph */
+    int64_t graph_captures;
+    int64_t graph_replays;
+    int32_t tuned_classes;         /* size classes with an autotuned bin grid */
+    int32_t pad0;
+    int64_t tune_launches;
+    float ms;                      /* GPU time of the last launch */
+    float pad1;
+} fdzb_batch_stats;
+
+int fdzb_batch_create(fdzb_batch **out, int device);
+int fdzb_batch_destroy(fdzb_batch *batch);
+/* stream: a cudaStream_t; NULL = the batch's own stream. */
+int fdzb_batch_set_stream(fdzb_batch *batch, void *stream);
+int fdzb_batch_set_graph(fdzb_batch *batch, int enable);
+int fdzb_batch_set_profiling(fdzb_batch *batch, int enable);
+int fdzb_batch_set_tri_order(fdzb_batch *batch, int order);
+/* Enqueue frames[0..n) (the descriptors are copied; buffers must stay valid until
+ * fdzb_batch_sync returns). */
+int fdzb_batch_launch_async(fdzb_batch *batch, const fdzb_frame_desc *frames, int n);
+/* Waits, re-runs the launch if the pair buffer overflowed, *ms_out (nullable)
+ * gets the GPU time of the launch. */
+int fdzb_batch_sync(fdzb_batch *batch, float *ms_out);
+int fdzb_batch_launch(fdzb_batch *batch, const fdzb_frame_desc *frames, int n, float *ms_out);
+/* Per-frame stats of the last launch (launch-wide counters read -1 when the
+ * launch held more than one frame; they are in fdzb_batch_stats.totals). */
+int fdzb_batch_get_frame_stats(fdzb_batch *batch, int frame, fdzb_frame_stats *out);
+int fdzb_batch_get_stats(fdzb_batch *batch, fdzb_batch_stats *out);
+/* Bins per side used for frame i of the last launch (>0), or an error code. */
+int fdzb_batch_frame_bins(fdzb_batch *batch, int frame);
+/* Autotuner: for every size class (ceil(log2 samples), ceil(log2 triangles), N)
+ * of the frames with bins == 0 not tuned yet, times three bin grids around
+ * ~128 samples per bin (each as a launch of up to 8 copies of the class's first
+ * frame, so that the GPU is as full as inside a batch) and keeps the fastest
+ * for later launches of this batch.  d_scratch: device float[scratch_floats],
+ * at least one frame's W*H (receives the copies' shadows). */
+int fdzb_batch_autotune(fdzb_batch *batch, const fdzb_frame_desc *frames, int n, float *d_scratch,
+                        size_t scratch_floats);
+
 /* ---- allocation-free sort ------------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -94,3 +94,24 @@ def test_context_creation_without_gpu_is_an_error_not_a_crash(fdzb):
         pytest.skip("a GPU is present")
     with pytest.raises(fdzb.FdzbError):
         fdzb.Context()
+
+
+def test_batch_api_rejects_null_handles(fdzb):
+    lib = fdzb.load()
+    assert lib.fdzb_batch_launch(None, None, 0, None) == -3
+    assert lib.fdzb_batch_sync(None, None) == -3
+    assert lib.fdzb_batch_get_stats(None, None) == -3
+    assert lib.fdzb_batch_frame_bins(None, 0) == -3
+    assert lib.fdzb_batch_autotune(None, None, 0, None, 0) == -3
+    assert lib.fdzb_batch_destroy(None) == 0
+    assert lib.fdzb_ctx_set_graph(None, 1) == -3
+
+
+def test_batch_struct_layouts(fdzb):
+    """ctypes mirrors match the C layouts (the library static_asserts the same sizes)."""
+    import ctypes
+    assert ctypes.sizeof(fdzb.AreaLightDesc) == 52
+    assert ctypes.sizeof(fdzb.FrameStats) == 184
+    assert ctypes.sizeof(fdzb.FrameDesc) == 144
+    assert ctypes.sizeof(fdzb.BatchStats) == 232
+    assert fdzb.FrameDesc.light.offset == 64 and fdzb.FrameDesc.d_shadow.offset == 128
