@@ -55,6 +55,9 @@ EXPORTED = [
     "fdzb_batch_set_graph", "fdzb_batch_set_profiling", "fdzb_batch_set_tri_order",
     "fdzb_batch_launch_async", "fdzb_batch_sync", "fdzb_batch_launch", "fdzb_batch_get_frame_stats",
     "fdzb_batch_get_stats", "fdzb_batch_frame_bins", "fdzb_batch_autotune",
+    "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
+    "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
+    "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
 ]
 
 STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
@@ -131,6 +134,42 @@ class BatchStats(ctypes.Structure):
         return out
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32), ("max_batch_frames", ctypes.c_int32),
+                ("use_graphs", ctypes.c_int32), ("max_batch_samples", ctypes.c_int64),
+                ("memory_budget_bytes", ctypes.c_uint64)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("scene_id", ctypes.c_int32), ("W", ctypes.c_int32), ("H", ctypes.c_int32),
+                ("bins", ctypes.c_int32), ("d_pos", ctypes.c_void_p), ("d_nrm", ctypes.c_void_p),
+                ("light", AreaLightDesc), ("pad0", ctypes.c_int32), ("d_shadow", ctypes.c_void_p),
+                ("d_masks", ctypes.c_void_p)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("batch_frames", ctypes.c_int32), ("latency_ms", ctypes.c_double),
+                ("queue_ms", ctypes.c_double), ("stats", FrameStats)]
+
+    def as_dict(self) -> dict:
+        out = {n: getattr(self, n) for n, _ in self._fields_ if n != "stats"}
+        out["stats"] = self.stats.as_dict()
+        return out
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("rejected", ctypes.c_int64),
+                ("failed", ctypes.c_int64), ("batches", ctypes.c_int64), ("batched_frames", ctypes.c_int64),
+                ("overlapped_batches", ctypes.c_int64), ("queued", ctypes.c_int64), ("busy_slots", ctypes.c_int32),
+                ("max_inflight_batches", ctypes.c_int32), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("frames_per_s", ctypes.c_double),
+                ("held_bytes", ctypes.c_int64), ("peak_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64),
+                ("tuned_classes", ctypes.c_int32), ("slots", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -184,6 +223,16 @@ def load() -> ctypes.CDLL:
         "fdzb_batch_get_frame_stats": ([vp, i32, P(FrameStats)], i32),
         "fdzb_batch_get_stats": ([vp, P(BatchStats)], i32), "fdzb_batch_frame_bins": ([vp, i32], i32),
         "fdzb_batch_autotune": ([vp, P(FrameDesc), i32, vp, sz], i32),
+        "fdzb_serve_default_config": ([P(ServeConfig)], None),
+        "fdzb_serve_create": ([P(vp), P(ServeConfig)], i32), "fdzb_serve_destroy": ([vp], i32),
+        "fdzb_serve_add_scene": ([vp, vp, sz, sz, vp, sz, i32, f32, P(ctypes.c_int32)], i32),
+        "fdzb_serve_submit": ([vp, P(Request), P(ctypes.c_uint64)], i32),
+        "fdzb_serve_poll": ([vp, ctypes.c_uint64, P(RequestResult)], i32),
+        "fdzb_serve_wait": ([vp, ctypes.c_uint64, i32, P(RequestResult)], i32),
+        "fdzb_serve_drain": ([vp, i32], i32),
+        "fdzb_serve_autotune": ([vp, P(Request), i32, vp, sz], i32),
+        "fdzb_serve_get_stats": ([vp, P(ServeStats)], i32), "fdzb_serve_reset_stats": ([vp], i32),
+        "fdzb_serve_last_worker_error": ([vp], ctypes.c_char_p),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -539,3 +588,92 @@ class Batch:
         if rc <= 0:
             _check(rc if rc < 0 else -1)
         return rc
+
+
+# ---- serving ---------------------------------------------------------------
+
+
+def request(scene_id: int, pos, nrm, W: int, H: int, light, shadow, masks=None, bins: int = 0) -> Request:
+    """An fdzb_request from device tensors (or int pointers)."""
+    r = Request()
+    r.scene_id, r.W, r.H, r.bins = scene_id, W, H, bins
+    r.d_pos, r.d_nrm = _ptr(pos), _ptr(nrm)
+    r.light = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+    r.d_shadow, r.d_masks = _ptr(shadow), _ptr(masks)
+    return r
+
+
+class Server:
+    """Request loop with continuous batching (the fdzb_serve_* API)."""
+
+    def __init__(self, slots: int = 2, max_batch_frames: int = 16, max_batch_samples: int = 16 << 20,
+                 memory_budget_bytes: int = 150 * 10**9, use_graphs: bool = False, device: int = -1):
+        self._lib = load()
+        cfg = ServeConfig()
+        self._lib.fdzb_serve_default_config(ctypes.byref(cfg))
+        cfg.device, cfg.slots, cfg.max_batch_frames = device, slots, max_batch_frames
+        cfg.max_batch_samples, cfg.memory_budget_bytes = max_batch_samples, memory_budget_bytes
+        cfg.use_graphs = int(bool(use_graphs))
+        h = ctypes.c_void_p()
+        _check(self._lib.fdzb_serve_create(ctypes.byref(h), ctypes.byref(cfg)))
+        self._h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fdzb_serve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, vtx, n_vtx: int, idx, n_tri: int, cull: bool = False, esp: float = 1e-3,
+                  stride_bytes: int = 16) -> int:
+        self._keep += [vtx, idx]
+        sid = ctypes.c_int32()
+        _check(self._lib.fdzb_serve_add_scene(self._h, _ptr(vtx), n_vtx, stride_bytes, _ptr(idx), n_tri,
+                                              int(bool(cull)), esp, ctypes.byref(sid)))
+        return int(sid.value)
+
+    def submit(self, req: Request) -> int:
+        t = ctypes.c_uint64()
+        _check(self._lib.fdzb_serve_submit(self._h, ctypes.byref(req), ctypes.byref(t)))
+        return int(t.value)
+
+    def poll(self, ticket: int):
+        out = RequestResult()
+        rc = self._lib.fdzb_serve_poll(self._h, ticket, ctypes.byref(out))
+        if rc < 0:
+            _check(rc)
+        return out.as_dict() if rc == 1 else None
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        out = RequestResult()
+        rc = self._lib.fdzb_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(out))
+        if rc < 0:
+            _check(rc)
+        return out.as_dict() if rc == 1 else None
+
+    def drain(self, timeout_ms: int = -1) -> bool:
+        rc = self._lib.fdzb_serve_drain(self._h, timeout_ms)
+        if rc < 0:
+            _check(rc)
+        return rc == 1
+
+    def autotune(self, reqs, scratch) -> None:
+        arr = (Request * len(reqs))(*reqs)
+        _check(self._lib.fdzb_serve_autotune(self._h, arr, len(reqs), _ptr(scratch), scratch.numel()))
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(self._lib.fdzb_serve_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self) -> None:
+        _check(self._lib.fdzb_serve_reset_stats(self._h))
+
+    def worker_error(self) -> str:
+        return self._lib.fdzb_serve_last_worker_error(self._h).decode()

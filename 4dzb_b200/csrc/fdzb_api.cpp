@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/fdzb.h"
+#include "fdzb_engine.h"
 #include "fdzb_internal.h"
 
 namespace {
@@ -68,65 +69,11 @@ struct Model {
     std::string name;
 };
 
-// Host copy of one frame's inputs.
-struct FrameSpec {
-    const float4 *pos = nullptr, *nrm = nullptr;
-    int W = 0, H = 0;
-    const float *vtx = nullptr;
-    size_t nv = 0, strideBytes = 16;
-    const int32_t *idx = nullptr;
-    size_t nt = 0;
-    fdzb::LightParams light{};
-    int bins = 16;
-    int cull = 1;
-    float esp = 1e-6f;
-    float *shadow = nullptr;
-    uint32_t *masks = nullptr;
-};
+}  // namespace
 
-// Host-side parameters that a captured graph bakes in; a launch whose key
-// differs re-captures.
-struct GraphKey {
-    int nf = -1, S = 0, T = 0, NB = 0, P = 0, sp = 0, pp = 0, db = 0, maxS = 0, maxT = 0, maxV = 0;
-    const void *arena = nullptr, *hFrames = nullptr;
-    cudaStream_t stream = nullptr;
-    auto tie() const { return std::tie(nf, S, T, NB, P, sp, pp, db, maxS, maxT, maxV, arena, hFrames, stream); }
-    bool operator==(const GraphKey &o) const { return tie() == o.tie(); }
-};
+namespace fdzb {
 
-struct Engine {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t ownStream = nullptr;
-    void *arena = nullptr;
-    size_t arenaBytes = 0;
-    fdzb::DeviceBuffers buf{};
-    long long pairCapacity = 0;
-    int debug = 0;  // keep pre-sort copies for export
-    int triOrder = FDZB_TRI_ORDER_DEPTH;
-    bool profile = false;  // record events at the stage boundaries
-    bool useGraph = true;
-    // pinned host staging, grown to the largest frame list
-    fdzb::FrameDesc *hFrames = nullptr;
-    fdzb::FrameState *hStates = nullptr;
-    int *hBases = nullptr;
-    int hCap = 0;
-    fdzb::Counters *hCounters = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t stageEv[fdzb::STAGE_COUNT + 1] = {};
-    // the frame list of the pending / last launch
-    std::vector<FrameSpec> frames;
-    int maxS = 0, maxT = 0, maxV = 0;
-    int launches = 0;
-    bool pending = false;
-    int replans = 0;
-    float lastMs = 0.f;
-    // graph of the last launch shape
-    cudaGraphExec_t graph = nullptr;
-    GraphKey graphKey{};
-    bool lastFromGraph = false;
-    long long graphCaptures = 0, graphReplays = 0;
-};
+namespace {
 
 // Lays out every buffer of a launch of nf frames inside the arena; returns bytes.
 size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long T, long long NB, long long P,
@@ -184,12 +131,16 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long
     return align_up(off, 256);
 }
 
+}  // namespace
+
 void drop_graph(Engine &e)
 {
     if (e.graph) cudaGraphExecDestroy(e.graph);
     e.graph = nullptr;
     e.graphKey = GraphKey{};
 }
+
+namespace {
 
 int ensure_arena(Engine &e, int nf, long long S, long long T, long long NB, long long P)
 {
@@ -239,6 +190,18 @@ int ensure_host(Engine &e, int nf)
     return FDZB_OK;
 }
 
+}  // namespace
+
+void engine_free_arena(Engine &e)
+{
+    if (e.stream) cudaStreamSynchronize(e.stream);
+    e.pending = false;
+    drop_graph(e);
+    if (e.arena) cudaFree(e.arena);
+    e.arena = nullptr;
+    e.arenaBytes = 0;
+}
+
 int engine_init(Engine &e, int device)
 {
     if (device < 0) {
@@ -272,6 +235,8 @@ void engine_release(Engine &e)
     if (e.ownStream) cudaStreamDestroy(e.ownStream);
     e = Engine{};
 }
+
+namespace {
 
 // Checks one frame's inputs (the conditions FD:: assumes of its callers).
 int check_frame(const FrameSpec &f, int i)
@@ -308,6 +273,8 @@ cudaError_t enqueue_body(Engine &e, int nf)
     return cudaMemcpyAsync(e.hStates, b.states, sizeof(fdzb::FrameState) * nf, cudaMemcpyDeviceToHost, s);
 }
 
+}  // namespace
+
 int engine_enqueue(Engine &e)
 {
     const int nf = (int)e.frames.size();
@@ -329,7 +296,7 @@ int engine_enqueue(Engine &e)
     if (T > 0x3fffffffll) return fail(FDZB_ERR_INVALID_ARG, "too many triangles in one launch");
     if (NB > kMaxTotalBins) return fail(FDZB_ERR_INVALID_ARG, "too many light-plane bins in one launch");
     if (nf > 65535) return fail(FDZB_ERR_INVALID_ARG, "too many frames in one launch (max 65535)");
-    if (e.pairCapacity <= 0) e.pairCapacity = std::min(std::max<long long>(1 << 20, T * 64), kMaxPairCapacity);
+    if (e.pairCapacity <= 0) e.pairCapacity = default_pair_capacity(T);
     if (int rc = ensure_host(e, nf)) return rc;
     if (int rc = ensure_arena(e, nf, S, T, NB, e.pairCapacity)) return rc;
     e.maxS = maxS;
@@ -544,7 +511,10 @@ void launch_stats(const Engine &e, fdzb_frame_stats &o)
     }
 }
 
-}  // namespace
+}  // namespace fdzb
+
+using namespace fdzb;
+
 
 // ---- FD-shaped context: one scene, one view, one light -----------------------
 
@@ -568,33 +538,10 @@ struct fdzb_ctx {
 
 // ---- batch: a list of independent frames per launch --------------------------
 
-namespace {
-
-// Autotuner table: bins per side for a size class (log2 samples, log2
-// triangles, light grid N).
-using TuneKey = std::tuple<int, int, int>;
-
-TuneKey tune_key(long long S, long long T, int N)
-{
-    return TuneKey(ceil_log2(std::max(S, 1ll)), ceil_log2(std::max(T, 1ll)), N);
-}
-
-// Starting point of the autotuner: about 128 samples per bin on the light plane
-// (the HD frame's 1920x1080 samples over 128 x 128 bins), clamped to [8, 256].
-int heuristic_bins(long long S)
-{
-    const double side = std::sqrt((double)std::max(S, 1ll) / 128.0);
-    int b = 8;
-    while (b < 256 && b * 2 <= side * 1.41421356) b *= 2;
-    return b;
-}
-
-}  // namespace
-
 struct fdzb_batch {
     Engine eng;
     int triOrder = FDZB_TRI_ORDER_DEPTH;
-    std::map<TuneKey, int> tuned;
+    TuneTable tuned;
     std::vector<int> chosenBins;
     long long tuneLaunches = 0;
 };
@@ -647,7 +594,23 @@ int ctx_sync(fdzb_ctx *c)
     return FDZB_OK;
 }
 
-int desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
+int batch_bins_for(fdzb_batch *b, const FrameSpec &f) { return tuned_bins(b->tuned, f); }
+
+}  // namespace
+
+int fdzb::set_error(int code, const std::string &msg) { return fail(code, msg); }
+
+// Starting point of the autotuner: about 128 samples per bin on the light plane
+// (the HD frame's 1920x1080 samples over 128 x 128 bins), clamped to [8, 256].
+int fdzb::heuristic_bins(long long S)
+{
+    const double side = std::sqrt((double)std::max(S, 1ll) / 128.0);
+    int b = 8;
+    while (b < 256 && b * 2 <= side * 1.41421356) b *= 2;
+    return b;
+}
+
+int fdzb::desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
 {
     const fdzb_area_light_desc &L = d.light;
     if (L.lightResWidth != L.lightResHeight || L.lightResWidth < 1 || L.lightResWidth > fdzb::kMaxLightN)
@@ -671,16 +634,92 @@ int desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
     return FDZB_OK;
 }
 
-int batch_bins_for(fdzb_batch *b, const FrameSpec &f)
+size_t fdzb::launch_bytes(const std::vector<FrameSpec> &frames, long long pairCapacity, bool debug)
 {
-    const long long S = (long long)f.W * f.H;
-    auto it = b->tuned.find(tune_key(S, (long long)f.nt, f.light.N));
-    return it != b->tuned.end() ? it->second : heuristic_bins(S);
+    long long S = 0, T = 0, NB = 0;
+    for (const FrameSpec &f : frames) {
+        S += (long long)f.W * f.H;
+        T += (long long)f.nt;
+        NB += (long long)f.bins * f.bins;
+    }
+    DeviceBuffers probe{};
+    return layout(probe, nullptr, (int)frames.size(), S, T, NB, pairCapacity, debug);
 }
 
-}  // namespace
+long long fdzb::default_pair_capacity(long long T)
+{
+    return std::min(std::max<long long>(1 << 20, T * 64), kMaxPairCapacity);
+}
 
-int fdzb::set_error(int code, const std::string &msg) { return fail(code, msg); }
+fdzb::TuneKey fdzb::tune_key(long long S, long long T, int N)
+{
+    return TuneKey(ceil_log2(std::max(S, 1ll)), ceil_log2(std::max(T, 1ll)), N);
+}
+
+int fdzb::tuned_bins(const TuneTable &table, const FrameSpec &f)
+{
+    const long long S = (long long)f.W * f.H;
+    auto it = table.find(tune_key(S, (long long)f.nt, f.light.N));
+    return it != table.end() ? it->second : heuristic_bins(S);
+}
+
+// For every size class of `frames` not in `table`: times the grids h/2, h, 2h
+// around the heuristic h, each as a launch of up to 8 copies of the class's
+// first frame (shadows into `scratch`, no masks) so that the GPU is as full as
+// inside a batch, twice; the faster of the two counts.
+int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec> &frames, float *scratch,
+                        size_t scratchFloats, long long *launches)
+{
+    if (!scratch) return fail(FDZB_ERR_INVALID_ARG, "scratch buffer is NULL");
+    std::map<TuneKey, size_t> firstOf;
+    for (size_t i = 0; i < frames.size(); ++i) {
+        const FrameSpec &f = frames[i];
+        const TuneKey k = tune_key((long long)f.W * f.H, (long long)f.nt, f.light.N);
+        if (!table.count(k) && !firstOf.count(k)) firstOf[k] = i;
+    }
+    const bool savedGraph = e.useGraph;
+    e.useGraph = false;  // one-off shapes: no point capturing them
+    int rc = FDZB_OK;
+    for (const auto &kv : firstOf) {
+        const FrameSpec &f = frames[kv.second];
+        const long long S = (long long)f.W * f.H;
+        if ((size_t)S > scratchFloats) {
+            rc = fail(FDZB_ERR_INVALID_ARG, "autotune scratch smaller than a frame");
+            break;
+        }
+        const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, (long long)(scratchFloats / S)}));
+        const int h = heuristic_bins(S);
+        int best = h;
+        float bestMs = 1e30f;
+        for (int cand : {h / 2, h, h * 2}) {
+            if (cand < 4 || cand > kMaxBins) continue;
+            std::vector<FrameSpec> specs((size_t)reps, f);
+            for (int r = 0; r < reps; ++r) {
+                specs[r].bins = cand;
+                specs[r].shadow = scratch + (size_t)r * S;
+                specs[r].masks = nullptr;
+            }
+            float t = 1e30f;
+            for (int trial = 0; trial < 2 && rc == FDZB_OK; ++trial) {
+                e.frames = specs;
+                rc = engine_enqueue(e);
+                if (rc == FDZB_OK) rc = engine_sync(e);
+                if (launches) ++*launches;
+                if (rc == FDZB_OK) t = std::min(t, e.lastMs);
+            }
+            if (rc) break;
+            if (t < bestMs) {
+                bestMs = t;
+                best = cand;
+            }
+        }
+        if (rc) break;
+        table[kv.first] = best;
+    }
+    e.useGraph = savedGraph;
+    return rc;
+}
+
 
 namespace {
 fdzb_ctx *g_ctx = nullptr;
@@ -1142,58 +1181,15 @@ int fdzb_batch_autotune(fdzb_batch *b, const fdzb_frame_desc *frames, int n, flo
 {
     if (int rc = batch_check(b)) return rc;
     if (!frames || n <= 0) return fail(FDZB_ERR_INVALID_ARG, "empty frame list");
-    if (!d_scratch) return fail(FDZB_ERR_INVALID_ARG, "scratch buffer is NULL");
     if (int rc = engine_sync(b->eng)) return rc;
-    std::map<TuneKey, int> firstOf;
+    std::vector<FrameSpec> specs;
     for (int i = 0; i < n; ++i) {
         if (frames[i].bins != 0) continue;
         FrameSpec f;
         if (int rc = desc_to_spec(frames[i], f, i)) return rc;
-        const TuneKey k = tune_key((long long)f.W * f.H, (long long)f.nt, f.light.N);
-        if (!b->tuned.count(k) && !firstOf.count(k)) firstOf[k] = i;
+        specs.push_back(f);
     }
-    const bool savedGraph = b->eng.useGraph;
-    b->eng.useGraph = false;  // one-off shapes: no point capturing them
-    int rc = FDZB_OK;
-    for (const auto &kv : firstOf) {
-        FrameSpec f;
-        desc_to_spec(frames[kv.second], f, kv.second);
-        const long long S = (long long)f.W * f.H;
-        if ((size_t)S > scratch_floats) {
-            rc = fail(FDZB_ERR_INVALID_ARG, "autotune scratch smaller than a frame");
-            break;
-        }
-        const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, (long long)(scratch_floats / S)}));
-        const int h = heuristic_bins(S);
-        int best = h;
-        float bestMs = 1e30f;
-        for (int cand : {h / 2, h, h * 2}) {
-            if (cand < 4 || cand > fdzb::kMaxBins) continue;
-            std::vector<FrameSpec> specs((size_t)reps, f);
-            for (int r = 0; r < reps; ++r) {
-                specs[r].bins = cand;
-                specs[r].shadow = d_scratch + (size_t)r * S;
-                specs[r].masks = nullptr;
-            }
-            float t = 1e30f;
-            for (int trial = 0; trial < 2 && rc == FDZB_OK; ++trial) {
-                b->eng.frames = specs;
-                rc = engine_enqueue(b->eng);
-                if (rc == FDZB_OK) rc = engine_sync(b->eng);
-                ++b->tuneLaunches;
-                if (rc == FDZB_OK) t = std::min(t, b->eng.lastMs);
-            }
-            if (rc) break;
-            if (t < bestMs) {
-                bestMs = t;
-                best = cand;
-            }
-        }
-        if (rc) break;
-        b->tuned[kv.first] = best;
-    }
-    b->eng.useGraph = savedGraph;
-    return rc;
+    return autotune_bins(b->eng, b->tuned, specs, d_scratch, scratch_floats, &b->tuneLaunches);
 }
 
 // ---- reference-shaped global context -----------------------------------------

@@ -1,0 +1,111 @@
+// fdzb_engine.h -- the launch engine shared by contexts, batches and the server.
+//
+// An Engine owns one device arena (every scratch buffer of a launch), pinned
+// staging blocks, a stream and the CUDA graph of its last launch shape.  It runs
+// a list of frames (FrameSpec) through the pipeline in one launch per stage.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fdzb.h"
+#include "fdzb_internal.h"
+
+namespace fdzb {
+
+// Host copy of one frame's inputs.
+struct FrameSpec {
+    const float4 *pos = nullptr, *nrm = nullptr;
+    int W = 0, H = 0;
+    const float *vtx = nullptr;
+    size_t nv = 0, strideBytes = 16;
+    const int32_t *idx = nullptr;
+    size_t nt = 0;
+    LightParams light{};
+    int bins = 16;
+    int cull = 1;
+    float esp = 1e-6f;
+    float *shadow = nullptr;
+    uint32_t *masks = nullptr;
+};
+
+// Host-side parameters that a captured graph bakes in; a launch whose key
+// differs re-captures.
+struct GraphKey {
+    int nf = -1, S = 0, T = 0, NB = 0, P = 0, sp = 0, pp = 0, db = 0, maxS = 0, maxT = 0, maxV = 0;
+    const void *arena = nullptr, *hFrames = nullptr;
+    cudaStream_t stream = nullptr;
+    auto tie() const { return std::tie(nf, S, T, NB, P, sp, pp, db, maxS, maxT, maxV, arena, hFrames, stream); }
+    bool operator==(const GraphKey &o) const { return tie() == o.tie(); }
+};
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t ownStream = nullptr;
+    void *arena = nullptr;
+    size_t arenaBytes = 0;
+    DeviceBuffers buf{};
+    long long pairCapacity = 0;
+    int debug = 0;  // keep pre-sort copies for export
+    int triOrder = FDZB_TRI_ORDER_DEPTH;
+    bool profile = false;  // record events at the stage boundaries
+    bool useGraph = true;
+    // pinned host staging, grown to the largest frame list
+    FrameDesc *hFrames = nullptr;
+    FrameState *hStates = nullptr;
+    int *hBases = nullptr;
+    int hCap = 0;
+    Counters *hCounters = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t stageEv[STAGE_COUNT + 1] = {};
+    // the frame list of the pending / last launch
+    std::vector<FrameSpec> frames;
+    int maxS = 0, maxT = 0, maxV = 0;
+    int launches = 0;
+    bool pending = false;
+    int replans = 0;
+    float lastMs = 0.f;
+    // graph of the last launch shape
+    cudaGraphExec_t graph = nullptr;
+    GraphKey graphKey{};
+    bool lastFromGraph = false;
+    long long graphCaptures = 0, graphReplays = 0;
+};
+
+int engine_init(Engine &e, int device);
+void engine_release(Engine &e);
+// Enqueues e.frames (checked) without waiting.
+int engine_enqueue(Engine &e);
+// Waits for the pending launch; re-runs it if the pair buffer overflowed.
+int engine_sync(Engine &e);
+// Statistics of frame i of the last completed launch / of the whole launch.
+void frame_stats(const Engine &e, int i, fdzb_frame_stats &o);
+void launch_stats(const Engine &e, fdzb_frame_stats &o);
+// Device arena bytes a launch of `frames` needs with the given pair capacity.
+size_t launch_bytes(const std::vector<FrameSpec> &frames, long long pairCapacity, bool debug);
+// Pair capacity an engine starts from for T triangles (grown on overflow).
+long long default_pair_capacity(long long T);
+// Frame descriptor of the public API to a FrameSpec (light setup on the host).
+int desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i);
+// Bin grid before any tuning: about 128 samples per bin.
+int heuristic_bins(long long S);
+void drop_graph(Engine &e);
+// Waits for the engine's stream and frees its arena (the next launch allocates anew).
+void engine_free_arena(Engine &e);
+
+// Autotuner table: bins per side for a size class (ceil(log2 samples),
+// ceil(log2 triangles), light grid N).
+using TuneKey = std::tuple<int, int, int>;
+using TuneTable = std::map<TuneKey, int>;
+TuneKey tune_key(long long S, long long T, int N);
+// The tuned grid of f's class, else the heuristic.
+int tuned_bins(const TuneTable &table, const FrameSpec &f);
+// Tunes every class of `frames` missing from `table` (runs launches on e).
+int autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec> &frames, float *scratch,
+                  size_t scratchFloats, long long *launches);
+
+}  // namespace fdzb

@@ -293,6 +293,85 @@ int fdzb_batch_frame_bins(fdzb_batch *batch, int frame);
 int fdzb_batch_autotune(fdzb_batch *batch, const fdzb_frame_desc *frames, int n, float *d_scratch,
                         size_t scratch_floats);
 
+/* ---- serving: a request loop with continuous batching -------------------- */
+
+/* No counterpart in the reference (one frame per FD::FDLaunch from a
+ * single-threaded GL application, FS/api.cpp:405-575).  Scenes are registered
+ * once and stay resident on the device (caller-owned buffers); requests --
+ * scene id, view-sample buffers, light rectangle, grid size -- are submitted
+ * from any thread and return a ticket.  A worker thread owns `slots` engines
+ * (stream + arena each): whenever a slot is free it launches the requests at the
+ * head of the queue as one batch, as many as fit max_batch_frames,
+ * max_batch_samples and the memory budget (slot arenas -- sample and pair lists
+ * -- plus the shadows and masks of the requests in flight).  Batches on
+ * different slots overlap on the GPU.  Each request's results are identical to
+ * a plain launch of the same inputs.  A request that does not fit the budget
+ * even on an idle server completes with FDZB_ERR_NO_MEMORY. */
+typedef struct fdzb_server fdzb_server;
+
+typedef struct fdzb_serve_config {
+    int32_t device;                /* < 0: current device */
+    int32_t slots;                 /* concurrent batches (engines), 1..16; default 2 */
+    int32_t max_batch_frames;      /* default 16 */
+    int32_t use_graphs;            /* capture batches in CUDA graphs (default 0: shapes rarely repeat) */
+    int64_t max_batch_samples;     /* default 16 Mi samples */
+    uint64_t memory_budget_bytes;  /* default 150 GB */
+} fdzb_serve_config;
+
+typedef struct fdzb_request {
+    int32_t scene_id;
+    int32_t W, H;
+    int32_t bins;                  /* bins per side, power of two; 0 = autotuned / heuristic */
+    const float *d_pos;            /* float4[W*H] */
+    const float *d_nrm;            /* float4[W*H] */
+    fdzb_area_light_desc light;
+    int32_t pad0;
+    float *d_shadow;               /* float[W*H] */
+    uint32_t *d_masks;             /* nullable */
+} fdzb_request;
+
+typedef struct fdzb_request_result {
+    int32_t status;                /* FDZB_OK or an error code */
+    int32_t batch_frames;          /* requests in the launch that carried this one */
+    double latency_ms;             /* submission to completion */
+    double queue_ms;               /* submission to launch */
+    fdzb_frame_stats stats;
+} fdzb_request_result;
+
+typedef struct fdzb_serve_stats {
+    int64_t submitted, completed, rejected, failed;
+    int64_t batches, batched_frames, overlapped_batches;   /* launches; frames in them; launched while another was in flight */
+    int64_t queued;
+    int32_t busy_slots, max_inflight_batches;
+    double p50_ms, p99_ms, mean_ms, max_ms;                /* latency of completed requests */
+    double frames_per_s;                                   /* completed / (last completion - first submission) */
+    int64_t held_bytes, peak_bytes, budget_bytes;
+    int32_t tuned_classes, slots;
+} fdzb_serve_stats;
+
+/* Fills cfg with the defaults. */
+void fdzb_serve_default_config(fdzb_serve_config *cfg);
+int fdzb_serve_create(fdzb_server **out, const fdzb_serve_config *cfg /* nullable: defaults */);
+/* Stops the worker after the launches in flight; queued requests are dropped. */
+int fdzb_serve_destroy(fdzb_server *server);
+int fdzb_serve_add_scene(fdzb_server *server, const float *d_vtx, size_t n_vtx, size_t vtx_stride_bytes,
+                         const int32_t *d_idx, size_t n_tri, int cull, float esp, int32_t *scene_id);
+int fdzb_serve_submit(fdzb_server *server, const fdzb_request *request, uint64_t *ticket);
+/* 1 = done (*out filled, ticket released), 0 = not yet, < 0 = error. */
+int fdzb_serve_poll(fdzb_server *server, uint64_t ticket, fdzb_request_result *out);
+/* Blocks up to timeout_ms (< 0: forever); same returns as fdzb_serve_poll. */
+int fdzb_serve_wait(fdzb_server *server, uint64_t ticket, int timeout_ms, fdzb_request_result *out);
+/* Waits until the queue is empty and no batch is in flight: 1, or 0 on timeout. */
+int fdzb_serve_drain(fdzb_server *server, int timeout_ms);
+/* Autotunes bin grids for the size classes of `requests` (see fdzb_batch_autotune);
+ * call with no requests in flight. */
+int fdzb_serve_autotune(fdzb_server *server, const fdzb_request *requests, int n, float *d_scratch,
+                        size_t scratch_floats);
+int fdzb_serve_get_stats(fdzb_server *server, fdzb_serve_stats *out);
+int fdzb_serve_reset_stats(fdzb_server *server);
+/* Message of the last failure inside the worker ("" if none). */
+const char *fdzb_serve_last_worker_error(fdzb_server *server);
+
 /* ---- allocation-free sort ------------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot allocate device
