@@ -137,7 +137,7 @@ class BatchStats(ctypes.Structure):
 class ServeConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32), ("max_batch_frames", ctypes.c_int32),
                 ("use_graphs", ctypes.c_int32), ("max_batch_samples", ctypes.c_int64),
-                ("memory_budget_bytes", ctypes.c_uint64)]
+                ("memory_budget_bytes", ctypes.c_uint64), ("max_batch_triangles", ctypes.c_int64)]
 
 
 class Request(ctypes.Structure):
@@ -607,13 +607,15 @@ class Server:
     """Request loop with continuous batching (the fdzb_serve_* API)."""
 
     def __init__(self, slots: int = 2, max_batch_frames: int = 16, max_batch_samples: int = 16 << 20,
-                 memory_budget_bytes: int = 150 * 10**9, use_graphs: bool = False, device: int = -1):
+                 memory_budget_bytes: int = 150 * 10**9, use_graphs: bool = False, device: int = -1,
+                 max_batch_triangles: int = 4 << 20):
         self._lib = load()
         cfg = ServeConfig()
         self._lib.fdzb_serve_default_config(ctypes.byref(cfg))
         cfg.device, cfg.slots, cfg.max_batch_frames = device, slots, max_batch_frames
         cfg.max_batch_samples, cfg.memory_budget_bytes = max_batch_samples, memory_budget_bytes
         cfg.use_graphs = int(bool(use_graphs))
+        cfg.max_batch_triangles = max_batch_triangles
         h = ctypes.c_void_p()
         _check(self._lib.fdzb_serve_create(ctypes.byref(h), ctypes.byref(cfg)))
         self._h = h

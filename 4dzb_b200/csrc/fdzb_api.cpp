@@ -687,7 +687,10 @@ int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec
             rc = fail(FDZB_ERR_INVALID_ARG, "autotune scratch smaller than a frame");
             break;
         }
-        const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, (long long)(scratchFloats / S)}));
+        // copies: up to 8, ~2M samples and ~1M triangles in all, within the scratch
+        const long long T = std::max<long long>((long long)f.nt, 1);
+        const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, 1'000'000 / T,
+                                                                 (long long)(scratchFloats / S)}));
         const int h = heuristic_bins(S);
         int best = h;
         float bestMs = 1e30f;
@@ -706,6 +709,10 @@ int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec
                 if (rc == FDZB_OK) rc = engine_sync(e);
                 if (launches) ++*launches;
                 if (rc == FDZB_OK) t = std::min(t, e.lastMs);
+            }
+            if (rc == FDZB_ERR_CAPACITY) {   // too many pairs at this grid: not a candidate
+                rc = FDZB_OK;
+                continue;
             }
             if (rc) break;
             if (t < bestMs) {

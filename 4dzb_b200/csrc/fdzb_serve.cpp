@@ -33,7 +33,7 @@
 #include "fdzb_internal.h"
 
 // ABI layouts mirrored by the ctypes binding
-static_assert(sizeof(fdzb_serve_config) == 32, "fdzb_serve_config layout");
+static_assert(sizeof(fdzb_serve_config) == 40, "fdzb_serve_config layout");
 static_assert(sizeof(fdzb_request) == 104, "fdzb_request layout");
 static_assert(sizeof(fdzb_request_result) == 208, "fdzb_request_result layout");
 static_assert(sizeof(fdzb_serve_stats) == 144, "fdzb_serve_stats layout");
@@ -101,7 +101,8 @@ struct fdzb_server {
     // statistics
     std::vector<double> lat;          // ms, completed requests since reset
     long long submitted = 0, completed = 0, rejected = 0, failed = 0, batches = 0, batchedFrames = 0;
-    long long overlappedBatches = 0, arenaTrims = 0;
+    long long overlappedBatches = 0, arenaTrims = 0, splits = 0;
+    int frameLimit = 1 << 30;         // lowered after a batch overflowed the pair buffer
     int maxInflight = 0;
     size_t peakBytes = 0;
     double tFirstSubmit = -1, tLastDone = -1;
@@ -141,7 +142,10 @@ std::vector<uint64_t> take_batch(fdzb_server *s, Slot &sl, std::vector<FrameSpec
         const uint64_t t = s->queue.front();
         Request &r = s->reqs[t];
         const long long S = (long long)r.spec.W * r.spec.H;
-        if (!take.empty() && samples + S > s->cfg.max_batch_samples) break;
+        if (!take.empty() && (samples + S > s->cfg.max_batch_samples ||
+                              tris + (long long)r.spec.nt > s->cfg.max_batch_triangles ||
+                              (int)take.size() >= s->frameLimit))
+            break;
         specs.push_back(r.spec);
         const long long pairCap = std::max(sl.eng.pairCapacity, fdzb::default_pair_capacity(tris + (long long)r.spec.nt));
         const size_t arena = std::max(sl.eng.arenaBytes, align_mb(fdzb::launch_bytes(specs, pairCap, false) * 9 / 8));
@@ -188,6 +192,23 @@ void worker_main(fdzb_server *s)
             std::string err = rc ? fdzb_last_error() : std::string();
             const double tDone = sl.eng.replans ? now_s() : sl.tDone;
             lk.lock();
+            if (rc == FDZB_ERR_CAPACITY && sl.tickets.size() > 1) {
+                // the batch's pair list outgrew the largest buffer: requeue its
+                // requests at the head and launch them in smaller batches
+                for (size_t i = sl.tickets.size(); i-- > 0;) {
+                    auto it = s->reqs.find(sl.tickets[i]);
+                    if (it == s->reqs.end()) continue;
+                    it->second.state = REQ_QUEUED;
+                    s->queue.push_front(sl.tickets[i]);
+                }
+                s->frameLimit = std::max(1, (int)sl.tickets.size() / 2);
+                ++s->splits;
+                sl.tickets.clear();
+                sl.busy = false;
+                sl.done.store(false);
+                progressed = true;
+                continue;
+            }
             for (size_t i = 0; i < sl.tickets.size(); ++i) {
                 auto it = s->reqs.find(sl.tickets[i]);
                 if (it == s->reqs.end()) continue;
@@ -336,6 +357,7 @@ void fdzb_serve_default_config(fdzb_serve_config *cfg)
     cfg->slots = 2;
     cfg->max_batch_frames = 16;
     cfg->max_batch_samples = 16ll << 20;
+    cfg->max_batch_triangles = 4ll << 20;
     cfg->memory_budget_bytes = 150ull * 1000 * 1000 * 1000;
     cfg->use_graphs = 0;
 }
@@ -349,6 +371,7 @@ int fdzb_serve_create(fdzb_server **out, const fdzb_serve_config *cfg)
     if (c.slots < 1 || c.slots > 16) return fdzb::set_error(FDZB_ERR_INVALID_ARG, "slots must be in [1, 16]");
     if (c.max_batch_frames < 1) return fdzb::set_error(FDZB_ERR_INVALID_ARG, "max_batch_frames must be >= 1");
     if (c.max_batch_samples < 1) return fdzb::set_error(FDZB_ERR_INVALID_ARG, "max_batch_samples must be >= 1");
+    if (c.max_batch_triangles < 1) return fdzb::set_error(FDZB_ERR_INVALID_ARG, "max_batch_triangles must be >= 1");
     if (c.device < 0) {
         cudaError_t e = cudaGetDevice(&c.device);
         if (e != cudaSuccess) return fdzb::set_error(FDZB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

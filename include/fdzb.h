@@ -302,7 +302,7 @@ int fdzb_batch_autotune(fdzb_batch *batch, const fdzb_frame_desc *frames, int n,
  * from any thread and return a ticket.  A worker thread owns `slots` engines
  * (stream + arena each): whenever a slot is free it launches the requests at the
  * head of the queue as one batch, as many as fit max_batch_frames,
- * max_batch_samples and the memory budget (slot arenas -- sample and pair lists
+ * max_batch_samples, max_batch_triangles and the memory budget (slot arenas -- sample and pair lists
  * -- plus the shadows and masks of the requests in flight).  Batches on
  * different slots overlap on the GPU.  Each request's results are identical to
  * a plain launch of the same inputs.  A request that does not fit the budget
@@ -316,6 +316,7 @@ typedef struct fdzb_serve_config {
     int32_t use_graphs;            /* capture batches in CUDA graphs (default 0: shapes rarely repeat) */
     int64_t max_batch_samples;     /* default 16 Mi samples */
     uint64_t memory_budget_bytes;  /* default 150 GB */
+    int64_t max_batch_triangles;   /* default 4 Mi triangles (bounds the batch's pair list) */
 } fdzb_serve_config;
 
 typedef struct fdzb_request {
