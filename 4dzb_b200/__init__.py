@@ -36,6 +36,7 @@ ARRAYS = {
     "bin_range": (6, np.float32), "tri_count": (7, np.int32), "pair_bin": (8, np.int32),
     "pair_tri": (9, np.int32), "sorted_pair_bin": (10, np.int32), "sorted_pair_tri": (11, np.int32),
     "bin_tri_start": (12, np.int32), "bin_tri_end": (13, np.int32), "tri_aabb": (14, np.float32),
+    "work_counters": (15, np.uint64),
 }
 
 # Every symbol declared in include/fdzb.h.
@@ -55,6 +56,7 @@ EXPORTED = [
     "fdzb_batch_set_graph", "fdzb_batch_set_profiling", "fdzb_batch_set_tri_order",
     "fdzb_batch_launch_async", "fdzb_batch_sync", "fdzb_batch_launch", "fdzb_batch_get_frame_stats",
     "fdzb_batch_get_stats", "fdzb_batch_frame_bins", "fdzb_batch_autotune",
+    "fdzb_ctx_set_occlusion_schedule", "fdzb_batch_set_occlusion_schedule", "fdzb_ctx_set_pair_capacity_limit",
     "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
@@ -64,6 +66,9 @@ STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
 
 TRI_ORDER_REFERENCE = 0
 TRI_ORDER_DEPTH = 1
+
+OCC_LANE_PER_SAMPLE = 0
+OCC_LANE_PER_PAIR = 1
 
 
 class FdzbError(RuntimeError):
@@ -101,7 +106,7 @@ class FrameStats(ctypes.Structure):
                 ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 6),
                 ("model_aabb", ctypes.c_float * 6), ("replans", ctypes.c_int32),
                 ("quirk_key_range", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
-                ("pad0", ctypes.c_int32), ("rows_evaluated", ctypes.c_int64),
+                ("triangle_passes", ctypes.c_int32), ("rows_evaluated", ctypes.c_int64),
                 ("partial_masks", ctypes.c_int64), ("stage_ms", ctypes.c_float * 5),
                 ("pad1", ctypes.c_float)]
 
@@ -214,6 +219,8 @@ def load() -> ctypes.CDLL:
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
         "fdzb_ctx_set_graph": ([vp, i32], i32),
+        "fdzb_ctx_set_occlusion_schedule": ([vp, i32], i32),
+        "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32), "fdzb_batch_set_occlusion_schedule": ([vp, i32], i32),
         "fdzb_batch_create": ([P(vp), i32], i32), "fdzb_batch_destroy": ([vp], i32),
         "fdzb_batch_set_stream": ([vp, vp], i32), "fdzb_batch_set_graph": ([vp, i32], i32),
         "fdzb_batch_set_profiling": ([vp, i32], i32), "fdzb_batch_set_tri_order": ([vp, i32], i32),
@@ -325,6 +332,14 @@ class Context:
     def set_graph(self, enable: bool) -> None:
         """Capture launches in a CUDA graph and replay it while the shape holds (default on)."""
         _check(self._lib.fdzb_ctx_set_graph(self._h, int(bool(enable))))
+
+    def set_occlusion_schedule(self, schedule: int) -> None:
+        """OCC_LANE_PER_SAMPLE (default) or OCC_LANE_PER_PAIR; results are identical."""
+        _check(self._lib.fdzb_ctx_set_occlusion_schedule(self._h, int(schedule)))
+
+    def set_pair_capacity_limit(self, pairs: int) -> None:
+        """Largest pair buffer; frames with more pairs run in triangle passes."""
+        _check(self._lib.fdzb_ctx_set_pair_capacity_limit(self._h, int(pairs)))
 
     def add_model(self, vtx, n_vtx: int, stride_bytes: int, idx, n_tri: int, name: str = "") -> None:
         self._keep += [vtx, idx]
@@ -549,6 +564,9 @@ class Batch:
 
     def set_tri_order(self, order: int) -> None:
         _check(self._lib.fdzb_batch_set_tri_order(self._h, int(order)))
+
+    def set_occlusion_schedule(self, schedule: int) -> None:
+        _check(self._lib.fdzb_batch_set_occlusion_schedule(self._h, int(schedule)))
 
     def set_stream(self, stream) -> None:
         _check(self._lib.fdzb_batch_set_stream(self._h, ctypes.c_void_p(stream)))

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -228,6 +229,7 @@ void engine_release(Engine &e)
     if (e.hStates) cudaFreeHost(e.hStates);
     if (e.hBases) cudaFreeHost(e.hBases);
     if (e.hCounters) cudaFreeHost(e.hCounters);
+    if (e.passMasks) cudaFree(e.passMasks);
     if (e.ev0) cudaEventDestroy(e.ev0);
     if (e.ev1) cudaEventDestroy(e.ev1);
     for (auto &ev : e.stageEv)
@@ -296,7 +298,7 @@ int engine_enqueue(Engine &e)
     if (T > 0x3fffffffll) return fail(FDZB_ERR_INVALID_ARG, "too many triangles in one launch");
     if (NB > kMaxTotalBins) return fail(FDZB_ERR_INVALID_ARG, "too many light-plane bins in one launch");
     if (nf > 65535) return fail(FDZB_ERR_INVALID_ARG, "too many frames in one launch (max 65535)");
-    if (e.pairCapacity <= 0) e.pairCapacity = default_pair_capacity(T);
+    if (e.pairCapacity <= 0) e.pairCapacity = std::min(default_pair_capacity(T), e.maxPairCapacity);
     if (int rc = ensure_host(e, nf)) return rc;
     if (int rc = ensure_arena(e, nf, S, T, NB, e.pairCapacity)) return rc;
     e.maxS = maxS;
@@ -304,6 +306,7 @@ int engine_enqueue(Engine &e)
     e.maxV = maxV;
     fdzb::DeviceBuffers &b = e.buf;
     b.samplePasses = fdzb::sort_passes_for(NB + 1);
+    b.occVariant = e.occVariant;
     // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
     // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
     // order appends a depth bucket below the bin so each bin lists its lowest
@@ -345,6 +348,7 @@ int engine_enqueue(Engine &e)
         f.sampleBase = sb;
         f.triBase = tb;
         f.binBase = bb;
+        f.accumulate = s.accumulate;
         f.light = s.light;
         e.hBases[i] = sb;
         e.hBases[nf + i] = tb;
@@ -408,6 +412,106 @@ int engine_enqueue(Engine &e)
     return FDZB_OK;
 }
 
+namespace {
+
+// A frame whose triangle/bin pairs do not fit the largest pair buffer runs in
+// passes over ranges of its triangles, each OR-ing its occlusion bits into the
+// frame's masks.  The mask is the OR over triangles, so the passes add up to
+// the single-launch result; a launch whose pair list overflowed contributed a
+// subset of its bits, so a range that still overflows is split in two and run
+// again without undoing anything.  The far plane, light plane and bins depend
+// on the samples and on all vertices, not on the triangle range, and are the
+// same in every pass.
+int run_triangle_passes(Engine &e)
+{
+    const FrameSpec full = e.frames[0];
+    const size_t S = (size_t)full.W * full.H;
+    const size_t words = (size_t)(full.light.N * full.light.N + 31) / 32;
+    uint32_t *masks = full.masks;
+    int acc = 1;   // the overflowed launch already wrote a subset of the bits into full.masks
+    if (!masks) {
+        const size_t bytes = S * words * 4;
+        if (e.passMasksBytes < bytes) {
+            if (e.passMasks) cudaFree(e.passMasks);
+            e.passMasks = nullptr;
+            e.passMasksBytes = 0;
+            if (cudaMalloc(&e.passMasks, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(FDZB_ERR_NO_MEMORY, "mask buffer for triangle passes");
+            }
+            e.passMasksBytes = bytes;
+        }
+        masks = e.passMasks;
+        acc = 0;
+    }
+    const bool savedGraph = e.useGraph;
+    e.useGraph = false;
+    e.pairCapacity = e.maxPairCapacity;
+    const long long T = (long long)full.nt;
+    const long long est = std::max<long long>((long long)e.hCounters->pairCount, e.maxPairCapacity);
+    long long K = std::max<long long>(2, (est + e.maxPairCapacity * 3 / 4 - 1) / (e.maxPairCapacity * 3 / 4));
+    K = std::min(K, std::max(T, 1ll));
+    std::vector<std::pair<long long, long long>> todo;   // stack of [t0, t1), first range on top
+    for (long long i = K; i-- > 0;) todo.push_back({T * i / K, T * (i + 1) / K});
+    e.passes = 0;
+    e.passPairs = e.passTests = e.passRows = e.passPartial = 0;
+    e.passValidTris = 0;
+    float msSum = 0.f;
+    int rc = FDZB_OK;
+    while (!todo.empty() && rc == FDZB_OK) {
+        const auto r = todo.back();
+        todo.pop_back();
+        if (r.second <= r.first) continue;
+        FrameSpec f = full;
+        f.idx = full.idx + 3 * r.first;
+        f.nt = (size_t)(r.second - r.first);
+        f.masks = masks;
+        f.accumulate = acc;
+        e.frames.assign(1, f);
+        rc = engine_enqueue(e);
+        if (rc) break;
+        cudaError_t w = cudaStreamSynchronize(e.stream);
+        e.pending = false;
+        if (w != cudaSuccess) {
+            rc = fail(FDZB_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(w));
+            break;
+        }
+        acc = 1;
+        const fdzb::Counters &k = *e.hCounters;
+        if (k.errorFlags) {
+            rc = fail(k.errorFlags & fdzb::ERR_BAD_INPUT ? FDZB_ERR_INVALID_ARG : FDZB_ERR_DEVICE_TIMEOUT,
+                      "device error during a triangle pass");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.ev0, e.ev1);
+        msSum += ms;
+        ++e.passes;
+        if (k.pairOverflow) {
+            if (r.second - r.first <= 1) {
+                rc = fail(FDZB_ERR_CAPACITY, "one triangle overflows the pair buffer");
+                break;
+            }
+            const long long mid = (r.first + r.second) / 2;
+            todo.push_back({mid, r.second});
+            todo.push_back({r.first, mid});
+            continue;
+        }
+        e.passPairs += (unsigned long long)k.pairCount;
+        e.passTests += k.pairTests;
+        e.passRows += k.rowsEvaluated;
+        e.passPartial += k.partialMasks;
+        e.passValidTris += e.hStates[0].state == 2 ? e.hStates[0].nValidTris : 0;
+    }
+    e.frames.assign(1, full);
+    e.useGraph = savedGraph;
+    e.lastMs = msSum;
+    e.replans = e.passes;
+    return rc;
+}
+
+}  // namespace
+
 int engine_sync(Engine &e)
 {
     if (!e.pending) return FDZB_OK;
@@ -426,10 +530,12 @@ int engine_sync(Engine &e)
         if (k.errorFlags & fdzb::ERR_INTERNAL)
             return fail(FDZB_ERR_CUDA, "internal consistency check failed on the device");
         if (!k.pairOverflow) break;
-        if (e.replans >= 3 || k.pairCount >= kMaxPairCapacity)
+        if ((long long)k.pairCount > e.maxPairCapacity || e.pairCapacity >= e.maxPairCapacity || e.replans >= 3) {
+            if (e.frames.size() == 1) return run_triangle_passes(e);
             return fail(FDZB_ERR_CAPACITY, "triangle/bin pair buffer overflow (" + std::to_string(k.pairCount) +
-                                               " pairs)");
-        e.pairCapacity = std::min<long long>((long long)k.pairCount + k.pairCount / 4 + 1024, kMaxPairCapacity);
+                                               " pairs) in a launch of several frames");
+        }
+        e.pairCapacity = std::min<long long>((long long)k.pairCount + k.pairCount / 4 + 1024, e.maxPairCapacity);
         ++e.replans;
         const int replans = e.replans;
         if (int rc = engine_enqueue(e)) return rc;
@@ -438,6 +544,7 @@ int engine_sync(Engine &e)
     float ms = 0.f;
     FDZB_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
     e.lastMs = ms;
+    e.passes = 1;
     return FDZB_OK;
 }
 
@@ -470,8 +577,17 @@ void frame_stats(const Engine &e, int i, fdzb_frame_stats &o)
     o.replans = e.replans;
     o.quirk_key_range = s.quirkKeyRange;
     o.kernel_launches = e.launches;
+    o.triangle_passes = e.passes;
     o.rows_evaluated = single ? (int64_t)k.rowsEvaluated : -1;
     o.partial_masks = single ? (int64_t)k.partialMasks : -1;
+    if (single && e.passes > 1) {
+        o.num_pairs = (int32_t)std::min<unsigned long long>(e.passPairs, 0x7fffffffull);
+        o.pair_tests = (int64_t)e.passTests;
+        o.rows_evaluated = (int64_t)e.passRows;
+        o.partial_masks = (int64_t)e.passPartial;
+        o.valid_triangles = o.state == 2 ? (int32_t)e.passValidTris : 0;
+        o.kernel_launches = e.launches * e.passes;
+    }
     for (int j = 0; j < fdzb::STAGE_COUNT; ++j) {
         float t = 0.f;
         if (e.profile) cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
@@ -808,6 +924,26 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second)
     return FDZB_OK;
 }
 
+int fdzb_ctx_set_occlusion_schedule(fdzb_ctx *c, int schedule)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (schedule != FDZB_OCC_LANE_PER_SAMPLE && schedule != FDZB_OCC_LANE_PER_PAIR)
+        return fail(FDZB_ERR_INVALID_ARG, "unknown occlusion schedule");
+    c->eng.occVariant = schedule;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_pair_capacity_limit(fdzb_ctx *c, int64_t pairs)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (int rc = ctx_sync(c)) return rc;
+    if (pairs < 1024 || pairs > kMaxPairCapacity)
+        return fail(FDZB_ERR_INVALID_ARG, "pair capacity limit must be in [1024, 2^29]");
+    c->eng.maxPairCapacity = pairs;
+    c->eng.pairCapacity = std::min<long long>(c->eng.pairCapacity, pairs);
+    return FDZB_OK;
+}
+
 int fdzb_ctx_set_tri_order(fdzb_ctx *c, int order)
 {
     if (int rc = ctx_check(c)) return rc;
@@ -1027,6 +1163,13 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
         std::memcpy(dst, tmp.data(), bytes);
         return FDZB_OK;
     }
+    case FDZB_ARR_WORK_COUNTERS: {
+        const fdzb::Counters &k = *c->eng.hCounters;
+        const uint64_t v[6] = {k.pairTests, k.rowsEvaluated, k.partialMasks, k.pairsExamined, k.chunks, k.rounds};
+        if (bytes > sizeof(v)) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
+        std::memcpy(dst, v, bytes);
+        return FDZB_OK;
+    }
     default: return fail(FDZB_ERR_INVALID_ARG, "unknown array id");
     }
     if (bytes > avail) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
@@ -1102,6 +1245,15 @@ int fdzb_batch_set_profiling(fdzb_batch *b, int enable)
 {
     if (int rc = batch_check(b)) return rc;
     b->eng.profile = enable != 0;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_occlusion_schedule(fdzb_batch *b, int schedule)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (schedule != FDZB_OCC_LANE_PER_SAMPLE && schedule != FDZB_OCC_LANE_PER_PAIR)
+        return fail(FDZB_ERR_INVALID_ARG, "unknown occlusion schedule");
+    b->eng.occVariant = schedule;
     return FDZB_OK;
 }
 

@@ -30,6 +30,7 @@ struct FrameSpec {
     float esp = 1e-6f;
     float *shadow = nullptr;
     uint32_t *masks = nullptr;
+    int accumulate = 0;   // OR into `masks` (a later triangle pass of the same frame)
 };
 
 // Host-side parameters that a captured graph bakes in; a launch whose key
@@ -54,6 +55,14 @@ struct Engine {
     int triOrder = FDZB_TRI_ORDER_DEPTH;
     bool profile = false;  // record events at the stage boundaries
     bool useGraph = true;
+    int occVariant = 0;    // occlusion kernel (DeviceBuffers::occVariant)
+    long long maxPairCapacity = 1ll << 29;   // largest pair buffer; beyond it a frame runs in triangle passes
+    // triangle passes of the last single-frame launch (1 = none) and their sums
+    int passes = 1;
+    unsigned long long passPairs = 0, passTests = 0, passRows = 0, passPartial = 0;
+    long long passValidTris = 0;
+    uint32_t *passMasks = nullptr;            // mask buffer for passes when the caller keeps none
+    size_t passMasksBytes = 0;
     // pinned host staging, grown to the largest frame list
     FrameDesc *hFrames = nullptr;
     FrameState *hStates = nullptr;

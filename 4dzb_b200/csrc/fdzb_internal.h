@@ -41,7 +41,7 @@ struct FrameDesc {
     float esp;
     int maskWords;
     int sampleBase, triBase, binBase;
-    int pad;
+    int accumulate;         // 1: OR into the masks already in `masks` (later triangle passes)
     LightParams light;
 };
 
@@ -81,6 +81,9 @@ struct Counters {
     int sortTileCounter[8]; // one ticket per radix pass (4 sample + 4 pair)
     unsigned long long rowsEvaluated;   // light rows evaluated by pair tests
     unsigned long long partialMasks;    // row masks that needed the ceil(-D/B) threshold
+    unsigned long long pairsExamined;   // sample/triangle pairs reaching the AABB pre-cull
+    unsigned long long chunks;          // staged triangle chunks (warp-level)
+    unsigned long long rounds;          // compute rounds of 32 pair slots (k_occlusion_pairs)
 };
 
 // Stage boundaries recorded when per-stage timing is on.
@@ -119,6 +122,7 @@ struct DeviceBuffers {
     // sorted data lands in the A buffers after an even number of passes, B after odd
     int samplePasses, pairPasses;
     int depthBits;                              // secondary (depth-bucket) bits of the pair key
+    int occVariant;                             // 0: k_occlusion (lane per sample), 1: k_occlusion_pairs
     uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
                                                 // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays

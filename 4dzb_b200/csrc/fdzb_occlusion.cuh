@@ -192,6 +192,35 @@ __device__ __forceinline__ void write_result(const FrameDesc &fr, int local, int
     }
 }
 
+// Rows of a sample from its packed mask (bit r*N + j is row r, column j), for a
+// launch that accumulates into masks of an earlier triangle pass.  Returns the
+// set of full rows.
+__device__ __forceinline__ uint32_t load_rows(const FrameDesc &fr, int local, int N, uint32_t full,
+                                              uint32_t (*rows)[32], int lane)
+{
+    const uint32_t *mi = fr.masks + (size_t)local * fr.maskWords;
+    uint32_t fullRows = 0u;
+    for (int r = 0; r < N; ++r) {
+        const int bit = r * N, w = bit >> 5, o = bit & 31;
+        uint32_t v = mi[w] >> o;
+        if (o + N > 32) v |= mi[w + 1] << (32 - o);
+        v &= full;
+        rows[r][lane] = v;
+        if (v == full) fullRows |= 1u << r;
+    }
+    return fullRows;
+}
+
+// First contact of a sample with the pipeline's occlusion stage: rows cleared,
+// or loaded from the masks of an earlier triangle pass.
+__device__ __forceinline__ uint32_t init_rows(const FrameDesc &fr, int local, int N, uint32_t full,
+                                              uint32_t (*rows)[32], int lane)
+{
+    if (fr.accumulate) return load_rows(fr, local, N, full, rows, lane);
+    for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+    return 0u;
+}
+
 __device__ __forceinline__ void write_zero(const FrameDesc &fr, int local)
 {
     fr.shadow[local] = 0.0f;
@@ -273,10 +302,14 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
         const int nT = bte[bin] - tS;
 
         if (nT <= 0) {
-            for (int k = sLo + lane; k < sHi; k += 32) {
-                const int local = (int)sortedVals[k] - fr.sampleBase;
-                if ((unsigned)local < (unsigned)S) write_zero(fr, local);
-                else atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+            // no triangle in this bin: shadow 0 -- or, in a later triangle pass,
+            // the result of the earlier passes, left as it is
+            if (!fr.accumulate) {
+                for (int k = sLo + lane; k < sHi; k += 32) {
+                    const int local = (int)sortedVals[k] - fr.sampleBase;
+                    if ((unsigned)local < (unsigned)S) write_zero(fr, local);
+                    else atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                }
             }
             continue;
         }
@@ -304,7 +337,8 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                     active = true;
                     remaining = nT;
                     load_sample(smp, fr, st, local);
-                    for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+                    fullRows = init_rows(fr, local, N, FULL, rows, lane);
+                    if (fullRows == FULL) remaining = 0;
                 }
             }
             next += 32;
@@ -360,9 +394,9 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                     } else {
                         active = true;
                         remaining = nT;
-                        fullRows = 0u;
                         load_sample(smp, fr, st, local);
-                        for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+                        fullRows = init_rows(fr, local, N, FULL, rows, lane);
+                        if (fullRows == FULL) remaining = 0;
                     }
                 }
                 next += __popc(freeLanes);
@@ -380,6 +414,321 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
         atomicAdd(&ctr->pairTests, t);
         atomicAdd(&ctr->rowsEvaluated, tr);
         atomicAdd(&ctr->partialMasks, tp);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// k_occlusion_pairs: the same pair tests, scheduled so that every lane of a
+// warp works on a pair that passed the AABB pre-cull.
+//
+// A warp owns a work item (up to 32 samples of one bin, one per lane, as in
+// k_occlusion) and walks the bin's triangle list in chunks of kOccChunk staged
+// triangles.  Per chunk:
+//  1. cull: every lane tests its sample against each staged triangle's AABB and
+//     minimum depth (the reference's pre-cull, K/Step5_2_shadowCalPerSample.inl
+//     :120-128); a ballot per triangle gives the samples that pass it, and lane
+//     t keeps the mask of triangle t;
+//  2. compute: the passing pairs, numbered triangle-major through a warp scan
+//     of the masks' popcounts, are dealt 32 at a time, one per lane; a lane
+//     finds its pair's triangle by binary search over the scan, its sample as
+//     the k-th set bit of that triangle's mask, fetches the sample's point from
+//     the owning lane by shuffle and computes the pair's edge coefficients and
+//     row filter;
+//  3. rows: the (pair, light row) units of those 32 pairs are dealt 32 at a
+//     time the same way; each lane evaluates the three row masks of its unit
+//     (coefficients fetched from the pair's lane by shuffle) and ORs them into
+//     the sample's row in shared memory by an atomic.
+// A sample whose light rows are all full stops taking part (the reference's
+// early-out); the pairs it still had in the chunk being dealt are skipped at
+// their start.  The final mask is the OR over the bin's triangles either way.
+// ---------------------------------------------------------------------------
+
+#ifndef FDZB_OCC2_MINBLOCKS
+#define FDZB_OCC2_MINBLOCKS 6
+#endif
+
+// Bit position of the k-th (0-based) set bit of m; k < popc(m).
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int k)
+{
+    int pos = 0;
+    int c = __popc(m & 0xffffu);
+    if (k >= c) { k -= c; pos += 16; m >>= 16; }
+    c = __popc(m & 0xffu);
+    if (k >= c) { k -= c; pos += 8; m >>= 8; }
+    c = __popc(m & 0xfu);
+    if (k >= c) { k -= c; pos += 4; m >>= 4; }
+    c = __popc(m & 0x3u);
+    if (k >= c) { k -= c; pos += 2; m >>= 2; }
+    c = (int)(m & 1u);
+    if (k >= c) pos += 1;
+    return pos;
+}
+
+// row_mask without branches: the threshold is computed whatever the case and
+// selected away when the row is full or empty (same result as row_mask).
+__device__ __forceinline__ uint32_t row_mask_sel(float D, float slopeNm1, float slope, uint32_t full,
+                                                 uint32_t &npart)
+{
+    const bool f1 = D >= 0.0f;
+    const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
+    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
+    const int k = __float2int_rz(ceilf(q));
+    uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
+    m -= 1u;
+    m = f1 ? m : ~m;
+    npart += (f1 != f2) ? 1u : 0u;
+    m = (f1 == f2) ? (f1 ? full : 0u) : m;
+    return m & full;
+}
+
+// Edge coefficients of one pair (K/Step5_2_shadowCalPerSample.inl:129-191): the
+// light rows still open after the row filter, or 0 (self-skip, or nothing).
+struct PairEdges {
+    float A[3], B[3], C[3], Bn[3];
+};
+
+__device__ __forceinline__ uint32_t pair_setup(const StagedTri &T, f3 Q, f3 L0Q, f3 xd, f3 yd, float esp,
+                                               float nm1, uint32_t FULL, uint32_t fullRows, PairEdges &e,
+                                               uint32_t &npart)
+{
+    const float4 p1 = T.p[1], p2 = T.p[2], p3 = T.p[3], p4 = T.p[4], p5 = T.p[5], p6 = T.p[6];
+    const f3 v0 = mk3(p1.y, p1.z, p1.w), v1 = mk3(p2.x, p2.y, p2.z), v2 = mk3(p2.w, p3.x, p3.y);
+    const f3 n = mk3(p3.z, p3.w, p4.x);
+    const f3 e01 = mk3(p4.y, p4.z, p4.w), e12 = mk3(p5.x, p5.y, p5.z), e20 = mk3(p5.w, p6.x, p6.y);
+    const float dir = dot3(sub3(Q, v0), n);
+    if (fabsf(dir) < esp && point_in_tri(v0, v1, v2, Q)) return 0u;
+    const bool neg = dir < 0.0f;
+    const f3 t0 = neg ? mk3(-xd.x, -xd.y, -xd.z) : xd;
+    const f3 t1 = neg ? mk3(-yd.x, -yd.y, -yd.z) : yd;
+    const f3 lq = neg ? mk3(-L0Q.x, -L0Q.y, -L0Q.z) : L0Q;
+    const f3 n0 = cross3(sub3(v1, Q), e01);
+    const f3 n1 = cross3(sub3(v2, Q), e12);
+    const f3 n2 = cross3(sub3(v0, Q), e20);
+    e.A[0] = dot3(n0, t0); e.B[0] = dot3(n0, t1); e.C[0] = dot3(n0, lq);
+    e.A[1] = dot3(n1, t0); e.B[1] = dot3(n1, t1); e.C[1] = dot3(n1, lq);
+    e.A[2] = dot3(n2, t0); e.B[2] = dot3(n2, t1); e.C[2] = dot3(n2, lq);
+    uint32_t vr = FULL & ~fullRows;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float An = __fmul_rn(e.A[k], nm1);
+        e.Bn[k] = __fmul_rn(e.B[k], nm1);
+        vr &= row_mask_sel(__fadd_rn(e.B[k] > 0.0f ? e.Bn[k] : 0.0f, e.C[k]), An, e.A[k], FULL, npart);
+    }
+    return vr;
+}
+
+__global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
+    k_occlusion_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
+                      const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
+                      const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
+                      const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
+                      const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
+                      const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
+{
+    __shared__ StagedTri s_tri[kOccWarps][kOccChunk];
+    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
+    __shared__ uint32_t s_full[kOccWarps][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t(*rows)[32] = s_rows[warp];
+    volatile uint32_t *sfull = s_full[warp];
+    StagedTri *tris = s_tri[warp];
+    unsigned long long tested = 0, nexam = 0, nchunks = 0, nrounds = 0;
+    uint32_t nrows = 0, npart = 0;
+    int nitems = *(volatile const int *)&ctr->itemCount;
+    if (nitems > itemCapacity) nitems = itemCapacity;
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(&ctr->itemCursor, 1);
+        it = __shfl_sync(kFullWarp, it, 0);
+        if (it >= nitems) break;
+        const int4 item = items[it];
+        const int bin = item.x, fi = item.z;
+        if ((unsigned)bin >= (unsigned)totalBins || (unsigned)fi >= (unsigned)nframes) {
+            if (lane == 0) atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+            continue;
+        }
+        const FrameDesc &fr = frames[fi];
+        const FrameState &st = states[fi];
+        const int S = fr.W * fr.H;
+        const int sLo = bss[bin] + item.y;
+        const int sHi = min(sLo + kItemSamples, bse[bin]);
+        const int tS = bts[bin];
+        const int nT = bte[bin] - tS;
+
+        if (nT <= 0) {
+            // no triangle in this bin: shadow 0 -- or, in a later triangle pass,
+            // the result of the earlier passes, left as it is
+            if (!fr.accumulate) {
+                for (int k = sLo + lane; k < sHi; k += 32) {
+                    const int local = (int)sortedVals[k] - fr.sampleBase;
+                    if ((unsigned)local < (unsigned)S) write_zero(fr, local);
+                    else atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                }
+            }
+            continue;
+        }
+
+        const int N = fr.light.N;
+        const uint32_t FULL = fr.light.full;
+        const float nm1 = (float)(N - 1);
+        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd);
+        const float esp = fr.esp;
+
+        LaneSample smp;
+        smp.Q = mk3(0.f, 0.f, 0.f);
+        smp.L0Q = smp.Q;
+        smp.spx = smp.spy = smp.spz = smp.spw = smp.spZ = 0.f;
+        int local = 0;
+        bool has = false;
+        {
+            const int k = sLo + lane;
+            if (k < sHi) {
+                local = (int)sortedVals[k] - fr.sampleBase;
+                if ((unsigned)local >= (unsigned)S) {
+                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                } else {
+                    has = true;
+                    load_sample(smp, fr, st, local);
+                }
+            }
+        }
+        uint32_t fr0 = FULL;
+        if (has) fr0 = init_rows(fr, local, N, FULL, rows, lane);
+        else
+            for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
+        sfull[lane] = fr0;
+        bool active = has && fr0 != FULL;
+        for (int base = 0; base < nT && __any_sync(kFullWarp, active); base += kOccChunk) {
+            const int m = min(kOccChunk, nT - base);
+            __syncwarp();
+            if (lane < m) {
+                int tri = (int)pairTri[tS + base + lane];
+                if ((unsigned)tri >= (unsigned)totalTris) {
+                    atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
+                    tri = 0;
+                }
+                stage_triangle(tris[lane], rec, tri);
+            }
+            __syncwarp();
+            // 1. cull: lane t keeps the samples passing triangle t
+            uint32_t mine = 0u;
+            for (int t = 0; t < m; ++t) {
+                const float4 p0 = tris[t].p[0];
+                const float minz = tris[t].p[1].x;
+                const bool pass = active && p0.x <= smp.spx && p0.y <= smp.spy && smp.spz <= p0.z &&
+                                  smp.spw <= p0.w && minz <= smp.spZ;
+                const uint32_t b = __ballot_sync(kFullWarp, pass);
+                if (lane == t) mine = b;
+            }
+            // 2. compute: pairs numbered triangle-major
+            nexam += (unsigned long long)m * (unsigned)__popc(__ballot_sync(kFullWarp, active));
+            ++nchunks;
+            const int cnt = __popc(mine);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFullWarp, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(kFullWarp, incl, 31);
+            const int excl = incl - cnt;
+            for (int p0 = 0; p0 < total; p0 += 32) {
+                ++nrounds;
+                // (a) one pair per lane: edge coefficients and open rows
+                const int p = p0 + lane;
+                int t = 0;
+#pragma unroll
+                for (int w = 16; w >= 1; w >>= 1) {
+                    const int e = __shfl_sync(kFullWarp, excl, t + w);
+                    if (e <= p) t += w;
+                }
+                const uint32_t mt = __shfl_sync(kFullWarp, mine, t);
+                const int kth = p - __shfl_sync(kFullWarp, excl, t);
+                const bool valid = p < total;
+                const int sl = valid ? nth_set_bit(mt, kth) : lane;
+                const f3 Q = mk3(__shfl_sync(kFullWarp, smp.Q.x, sl), __shfl_sync(kFullWarp, smp.Q.y, sl),
+                                 __shfl_sync(kFullWarp, smp.Q.z, sl));
+                const f3 L0Q = mk3(__shfl_sync(kFullWarp, smp.L0Q.x, sl), __shfl_sync(kFullWarp, smp.L0Q.y, sl),
+                                   __shfl_sync(kFullWarp, smp.L0Q.z, sl));
+                PairEdges pe;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) pe.A[k] = pe.B[k] = pe.C[k] = pe.Bn[k] = 0.0f;
+                uint32_t vr = 0u;
+                if (valid) {
+                    const uint32_t fullRows = sfull[sl];
+                    if (fullRows != FULL) {
+                        ++tested;
+                        vr = pair_setup(tris[t], Q, L0Q, xd, yd, esp, nm1, FULL, fullRows, pe, npart);
+                    }
+                }
+                // (b) the (pair, row) units of this round, one per lane
+                const int uc = __popc(vr);
+                int uin = uc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(kFullWarp, uin, o);
+                    if (lane >= o) uin += y;
+                }
+                const int utotal = __shfl_sync(kFullWarp, uin, 31);
+                const int uex = uin - uc;
+                for (int u0 = 0; u0 < utotal; u0 += 32) {
+                    const int u = u0 + lane;
+                    int j = 0;
+#pragma unroll
+                    for (int w = 16; w >= 1; w >>= 1) {
+                        const int e = __shfl_sync(kFullWarp, uex, j + w);
+                        if (e <= u) j += w;
+                    }
+                    const uint32_t vj = __shfl_sync(kFullWarp, vr, j);
+                    const int kk = u - __shfl_sync(kFullWarp, uex, j);
+                    const int slj = __shfl_sync(kFullWarp, sl, j);
+                    float A[3], B[3], C[3], Bn[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        A[k] = __shfl_sync(kFullWarp, pe.A[k], j);
+                        B[k] = __shfl_sync(kFullWarp, pe.B[k], j);
+                        C[k] = __shfl_sync(kFullWarp, pe.C[k], j);
+                        Bn[k] = __shfl_sync(kFullWarp, pe.Bn[k], j);
+                    }
+                    if (u < utotal) {
+                        const int r = nth_set_bit(vj, kk);
+                        ++nrows;
+                        const float fr = (float)r;
+                        uint32_t M = FULL;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            M &= row_mask_sel(__fadd_rn(__fmul_rn(A[k], fr), C[k]), Bn[k], B[k], FULL, npart);
+                        if (M) {
+                            const uint32_t old = atomicOr(&rows[r][slj], M);
+                            if (old != FULL && (old | M) == FULL) atomicOr((uint32_t *)&sfull[slj], 1u << r);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            active = active && sfull[lane] != FULL;
+        }
+        __syncwarp();
+        if (has) write_result(fr, local, N, rows, lane);
+    }
+    unsigned long long t = tested, tr = nrows, tp = npart;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_xor_sync(kFullWarp, t, o);
+        tr += __shfl_xor_sync(kFullWarp, tr, o);
+        tp += __shfl_xor_sync(kFullWarp, tp, o);
+    }
+    if (lane == 0 && t) {
+        atomicAdd(&ctr->pairTests, t);
+        atomicAdd(&ctr->rowsEvaluated, tr);
+        atomicAdd(&ctr->partialMasks, tp);
+    }
+    if (lane == 0 && nchunks) {
+        atomicAdd(&ctr->pairsExamined, nexam);
+        atomicAdd(&ctr->chunks, nchunks);
+        atomicAdd(&ctr->rounds, nrounds);
     }
 }
 

@@ -753,9 +753,14 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
         b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
         b.items, b.itemCapacity, b.counters);
-    k_occlusion<<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
-        b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
-        b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    if (b.occVariant == 1)
+        k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(
+            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
+            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    else
+        k_occlusion<<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
+            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
+            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
     nl += 2;
     if (ev) cudaEventRecord(ev[STAGE_COUNT], s);
     if (launches) *launches = nl;

@@ -126,7 +126,8 @@ typedef struct fdzb_frame_stats {
     int32_t replans;           /* pair-buffer regrowths in this launch */
     int32_t quirk_key_range;   /* samples whose bin fell outside the grid (treated as unbinned) */
     int32_t kernel_launches;   /* kernels enqueued by the frame */
-    int32_t pad0;
+    int32_t triangle_passes;   /* 1, or the passes over triangle ranges of a frame whose pairs
+                                  exceeded the pair-capacity limit */
     int64_t rows_evaluated;    /* light-grid rows evaluated by pair tests */
     int64_t partial_masks;     /* row masks that needed the ceil(-D/B) threshold */
     float stage_ms[5];         /* with profiling on: setup, sample sort, triangle pairs,
@@ -178,6 +179,10 @@ enum fdzb_array_id {
     FDZB_ARR_BIN_TRI_START,         /* int32[num_bins] */
     FDZB_ARR_BIN_TRI_END,           /* int32[num_bins] */
     FDZB_ARR_TRI_AABB,              /* float[8*T] (min xyz,1, max xyz,1) */
+    FDZB_ARR_WORK_COUNTERS,         /* uint64[6] occlusion work: pair tests, light rows, partial row
+                                       masks, pairs reaching the AABB pre-cull, triangle chunks,
+                                       compute rounds (the last three: counted by the pair-compacting
+                                       occlusion kernel only) */
     FDZB_ARR_COUNT
 };
 int fdzb_ctx_export(fdzb_ctx *ctx, int what, void *dst, size_t bytes);
@@ -196,6 +201,26 @@ int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
 #define FDZB_TRI_ORDER_REFERENCE 0
 #define FDZB_TRI_ORDER_DEPTH     1
 int fdzb_ctx_set_tri_order(fdzb_ctx *ctx, int order);
+
+/* Warp schedule of the occlusion stage (no counterpart in the reference, which
+ * runs one thread per sample, K/Step5_2_shadowCalPerSample.inl:37-231).  Results
+ * are identical; only the speed differs.
+ *   FDZB_OCC_LANE_PER_SAMPLE (default): a lane per sample of a bin, the warp
+ *     streaming the bin's triangles through shared memory;
+ *   FDZB_OCC_LANE_PER_PAIR: the pairs that pass the AABB pre-cull, and then
+ *     their (pair, light row) units, are dealt one per lane. */
+#define FDZB_OCC_LANE_PER_SAMPLE 0
+#define FDZB_OCC_LANE_PER_PAIR   1
+int fdzb_ctx_set_occlusion_schedule(fdzb_ctx *ctx, int schedule);
+
+/* Largest triangle/bin pair buffer (pairs; default and maximum 2^29, 8 GB of
+ * pair arrays).  No counterpart in the reference, whose fixed 70M-pair buffer
+ * overflows unchecked (FS/constants.h:15).  A frame whose pairs exceed it runs
+ * in passes over ranges of its triangles whose occlusion bits are OR-ed
+ * together (results identical; fdzb_frame_stats.triangle_passes counts them).
+ * When the frame has no mask output, the library keeps a mask buffer of its own
+ * for the passes. */
+int fdzb_ctx_set_pair_capacity_limit(fdzb_ctx *ctx, int64_t pairs);
 
 /* Per-stage GPU timing (CUDA events between stages, read back in
  * fdzb_frame_stats.stage_ms); off by default.  The reference times only the whole
@@ -271,6 +296,7 @@ int fdzb_batch_set_stream(fdzb_batch *batch, void *stream);
 int fdzb_batch_set_graph(fdzb_batch *batch, int enable);
 int fdzb_batch_set_profiling(fdzb_batch *batch, int enable);
 int fdzb_batch_set_tri_order(fdzb_batch *batch, int order);
+int fdzb_batch_set_occlusion_schedule(fdzb_batch *batch, int schedule);
 /* Enqueue frames[0..n) (the descriptors are copied; buffers must stay valid until
  * fdzb_batch_sync returns). */
 int fdzb_batch_launch_async(fdzb_batch *batch, const fdzb_frame_desc *frames, int n);

@@ -11,12 +11,14 @@ import numpy as np
 import oracle
 
 
-def run_gpu(scene, masks: bool = True, tri_order: int = 0):
+def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0):
     """One frame through the library's public Context API; returns
     (outputs dict, stats dict, exported intermediates dict).  tri_order 0 is the
-    reference's per-bin triangle order, 1 the depth order."""
+    reference's per-bin triangle order, 1 the depth order; schedule selects the
+    occlusion kernel's warp schedule."""
     fdzb = importlib.import_module("4dzb_b200")
     ctx, t = fdzb.context_for_scene(scene, masks=masks, debug=True, tri_order=tri_order)
+    ctx.set_occlusion_schedule(schedule)
     ms = ctx.launch()
     st = ctx.stats()
     S, T, NB = scene.S, scene.T, scene.bins * scene.bins

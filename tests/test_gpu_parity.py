@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 ORDERS = [0, 1]
 
 
-def _check(scene, tri_order=0, occ_stride=1):
+def _check(scene, tri_order=0, occ_stride=1, schedule=0):
     orc = oracle.frame(scene, occ_stride=occ_stride)
-    errs = parity.compare(scene, gpu=parity.run_gpu(scene, tri_order=tri_order), orc=orc)
+    errs = parity.compare(scene, gpu=parity.run_gpu(scene, tri_order=tri_order, schedule=schedule), orc=orc)
     assert not errs, "\n".join(errs)
 
 
@@ -66,3 +66,41 @@ def test_hd_preset_sampled(cuda_ok, scenes):
     """1920x1080 x 200k triangles x 16x16 light, 128^2 bins: every stage exact;
     masks checked on every 97th binned sample."""
     _check(scenes.preset("hd"), 1, occ_stride=97)
+
+
+@pytest.mark.parametrize("n,bins", [(1, 4), (4, 8), (8, 16), (16, 32), (32, 16)])
+@pytest.mark.parametrize("order", ORDERS)
+def test_lane_per_pair_schedule(cuda_ok, scenes, n, bins, order):
+    """The lane-per-pair occlusion schedule: same masks and shadows, bit for bit."""
+    _check(scenes.make_scene(200, 150, 3000, n=n, bins=bins, seed=80 + n, sigma=0.12), order, schedule=1)
+
+
+def test_lane_per_pair_schedule_medium(cuda_ok, scenes):
+    _check(scenes.make_scene(640, 480, 20000, n=16, bins=64, seed=21, sigma=0.1), 1, schedule=1)
+
+
+@pytest.mark.parametrize("masks", [True, False])
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_triangle_passes_match_oracle(cuda_ok, fdzb, scenes, masks, schedule):
+    """A pair-capacity limit far below the frame's pairs: the frame runs in
+    passes over triangle ranges (overflowing ranges split again) and still
+    matches the oracle bit for bit."""
+    s = scenes.make_scene(320, 240, 6000, n=8, bins=32, seed=91, sigma=0.12)
+    orc = oracle.frame(s)
+    ctx, t = fdzb.context_for_scene(s, masks=masks)
+    ctx.set_occlusion_schedule(schedule)
+    ctx.set_pair_capacity_limit(20000)
+    ctx.launch()
+    st = ctx.stats()
+    assert st["triangle_passes"] > 2, st["triangle_passes"]
+    assert st["num_pairs"] == orc.scalars["num_pairs"]
+    assert st["valid_triangles"] == orc.scalars["valid_tris"]
+    sh = t["shadow"].cpu().numpy()
+    assert np.array_equal(sh.view(np.uint32), orc.arrays["shadow"].astype(np.float32).view(np.uint32))
+    if masks:
+        mk = t["masks"].cpu().numpy().view(np.uint32)
+        assert np.array_equal(mk, orc.arrays["masks"].reshape(-1).astype(np.uint32)[: mk.size])
+    # a second launch reuses the limit and gives the same result
+    ctx.launch()
+    assert np.array_equal(t["shadow"].cpu().numpy(), sh)
+    ctx.close()
