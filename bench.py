@@ -128,7 +128,7 @@ def cpu_baseline(scene, seconds_target: float = 15.0) -> dict:
     sample of the frame's samples; extrapolated to frames/s."""
     import numpy as np
     import oracle
-    fr = oracle.frame(scene, occ_stride=1 << 30)          # light plane / records only
+    fr = oracle.frame(scene, setup_only=True)              # light plane only; triangles rebuilt
     rng = np.random.default_rng(12345)
     threads = os.cpu_count() or 1
     n = 256

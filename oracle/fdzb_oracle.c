@@ -493,6 +493,7 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
     o->lp_factor[0] = fx;
     o->lp_factor[1] = fy;
     o->state = 2;
+    if (in->setup_only) goto done;
 
     /* A7: K/Step3_bindSampleToBin.inl:5-59 */
     int32_t *keys = (int32_t *)malloc(sizeof(int32_t) * (size_t)S);

@@ -64,6 +64,8 @@ typedef struct {
     int32_t nthreads;            /* <= 0: OpenMP default */
     int32_t occ_stride;          /* occlusion only for sorted samples k with k % occ_stride == 0
                                     (<= 1: all); others keep mask 0 / shadow 0 */
+    int32_t setup_only;          /* 1: stop after the light plane (A1-A5); enough for the
+                                    exhaustive baselines, which rebuild their triangle list */
 } orc_frame_in;
 
 typedef struct {

@@ -40,7 +40,7 @@ class FrameIn(ctypes.Structure):
                 ("vtx", f32p), ("vtx_stride_floats", ctypes.c_int32), ("V", ctypes.c_int32),
                 ("idx", i32p), ("T", ctypes.c_int32), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
                 ("esp", ctypes.c_float), ("light", ctypes.POINTER(Light)), ("nthreads", ctypes.c_int32),
-                ("occ_stride", ctypes.c_int32)]
+                ("occ_stride", ctypes.c_int32), ("setup_only", ctypes.c_int32)]
 
 
 class FrameOut(ctypes.Structure):
@@ -152,13 +152,30 @@ def _frame_in(scene, light: Light, nthreads: int, keep: list, occ_stride: int = 
     return fi
 
 
-def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride: int = 1) -> OrcFrame:
+def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride: int = 1,
+          setup_only: bool = False) -> OrcFrame:
     """Run the FP32 restatement (O2) on a scenes.Scene.  occ_stride > 1 runs the
-    occlusion stage only for every occ_stride-th sorted valid sample."""
+    occlusion stage only for every occ_stride-th sorted valid sample;
+    setup_only stops after the light plane (what the exhaustive baselines need)."""
     lib = load()
     keep: list = []
     light = light_setup(scene.light)
     fi = _frame_in(scene, light, nthreads, keep, occ_stride)
+    if setup_only:
+        # scalars only: every output array pointer stays NULL
+        fi.setup_only = 1
+        fo = FrameOut()
+        rc = lib.orc_frame(ctypes.byref(fi), ctypes.byref(fo))
+        if rc != 0:
+            raise RuntimeError(f"orc_frame failed: {rc}")
+        sc = {}
+        for name, _ in FrameOut._fields_:
+            v = getattr(fo, name)
+            if isinstance(v, (int, float)):
+                sc[name] = v
+            elif hasattr(v, "_length_") and not hasattr(v, "contents"):
+                sc[name] = list(v)
+        return OrcFrame(scalars=sc, arrays={}, _in=fi, _out=fo, _keep=keep)
     S, T, NB = scene.W * scene.H, scene.T, scene.bins * scene.bins
     words = mask_words(scene.light.n)
     # first a counting run to size the pair buffers
