@@ -422,13 +422,19 @@ namespace {
 // again without undoing anything.  The far plane, light plane and bins depend
 // on the samples and on all vertices, not on the triangle range, and are the
 // same in every pass.
-int run_triangle_passes(Engine &e)
+decltype(Engine::passKey) pass_key(const Engine &e, const FrameSpec &f)
+{
+    return {f.pos, f.nrm, f.W, f.H, f.vtx, f.idx, f.nt, f.bins, f.light.N, e.maxPairCapacity};
+}
+
+int run_triangle_passes(Engine &e, bool planned)
 {
     const FrameSpec full = e.frames[0];
     const size_t S = (size_t)full.W * full.H;
     const size_t words = (size_t)(full.light.N * full.light.N + 31) / 32;
     uint32_t *masks = full.masks;
-    int acc = 1;   // the overflowed launch already wrote a subset of the bits into full.masks
+    // after an overflowed launch, full.masks already holds a subset of the bits
+    int acc = planned ? 0 : 1;
     if (!masks) {
         const size_t bytes = S * words * 4;
         if (e.passMasksBytes < bytes) {
@@ -448,14 +454,21 @@ int run_triangle_passes(Engine &e)
     e.useGraph = false;
     e.pairCapacity = e.maxPairCapacity;
     const long long T = (long long)full.nt;
-    const long long est = std::max<long long>((long long)e.hCounters->pairCount, e.maxPairCapacity);
-    long long K = std::max<long long>(2, (est + e.maxPairCapacity * 3 / 4 - 1) / (e.maxPairCapacity * 3 / 4));
-    K = std::min(K, std::max(T, 1ll));
     std::vector<std::pair<long long, long long>> todo;   // stack of [t0, t1), first range on top
-    for (long long i = K; i-- > 0;) todo.push_back({T * i / K, T * (i + 1) / K});
+    if (planned) {
+        for (size_t i = e.passPlan.size(); i-- > 0;) todo.push_back(e.passPlan[i]);
+    } else {
+        const long long est = std::max<long long>((long long)e.hCounters->pairCount, e.maxPairCapacity);
+        long long K = std::max<long long>(2, (est + e.maxPairCapacity * 3 / 4 - 1) / (e.maxPairCapacity * 3 / 4));
+        K = std::min(K, std::max(T, 1ll));
+        for (long long i = K; i-- > 0;) todo.push_back({T * i / K, T * (i + 1) / K});
+    }
+    std::vector<std::pair<long long, long long>> done;
+    int splits = planned ? 0 : 1;   // the overflowed first launch counts as one re-plan
     e.passes = 0;
     e.passPairs = e.passTests = e.passRows = e.passPartial = 0;
     e.passValidTris = 0;
+    for (float &t : e.passStageMs) t = 0.f;
     float msSum = 0.f;
     int rc = FDZB_OK;
     while (!todo.empty() && rc == FDZB_OK) {
@@ -487,6 +500,12 @@ int run_triangle_passes(Engine &e)
         cudaEventElapsedTime(&ms, e.ev0, e.ev1);
         msSum += ms;
         ++e.passes;
+        if (e.profile)
+            for (int j = 0; j < fdzb::STAGE_COUNT; ++j) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
+                e.passStageMs[j] += t;
+            }
         if (k.pairOverflow) {
             if (r.second - r.first <= 1) {
                 rc = fail(FDZB_ERR_CAPACITY, "one triangle overflows the pair buffer");
@@ -495,8 +514,10 @@ int run_triangle_passes(Engine &e)
             const long long mid = (r.first + r.second) / 2;
             todo.push_back({mid, r.second});
             todo.push_back({r.first, mid});
+            ++splits;
             continue;
         }
+        done.push_back(r);
         e.passPairs += (unsigned long long)k.pairCount;
         e.passTests += k.pairTests;
         e.passRows += k.rowsEvaluated;
@@ -506,7 +527,13 @@ int run_triangle_passes(Engine &e)
     e.frames.assign(1, full);
     e.useGraph = savedGraph;
     e.lastMs = msSum;
-    e.replans = e.passes;
+    e.replans = splits;
+    if (rc == FDZB_OK) {
+        e.passPlan = done;
+        e.passKey = pass_key(e, full);
+    } else {
+        e.passPlan.clear();
+    }
     return rc;
 }
 
@@ -531,7 +558,7 @@ int engine_sync(Engine &e)
             return fail(FDZB_ERR_CUDA, "internal consistency check failed on the device");
         if (!k.pairOverflow) break;
         if ((long long)k.pairCount > e.maxPairCapacity || e.pairCapacity >= e.maxPairCapacity || e.replans >= 3) {
-            if (e.frames.size() == 1) return run_triangle_passes(e);
+            if (e.frames.size() == 1) return run_triangle_passes(e, false);
             return fail(FDZB_ERR_CAPACITY, "triangle/bin pair buffer overflow (" + std::to_string(k.pairCount) +
                                                " pairs) in a launch of several frames");
         }
@@ -546,6 +573,17 @@ int engine_sync(Engine &e)
     e.lastMs = ms;
     e.passes = 1;
     return FDZB_OK;
+}
+
+int engine_launch(Engine &e)
+{
+    if (e.frames.size() == 1 && !e.passPlan.empty() && e.passKey == pass_key(e, e.frames[0])) {
+        const int rc = run_triangle_passes(e, true);
+        e.pending = false;
+        return rc;
+    }
+    e.passes = 1;
+    return engine_enqueue(e);
 }
 
 // Statistics of frame i of the last completed launch.
@@ -590,7 +628,10 @@ void frame_stats(const Engine &e, int i, fdzb_frame_stats &o)
     }
     for (int j = 0; j < fdzb::STAGE_COUNT; ++j) {
         float t = 0.f;
-        if (e.profile) cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
+        if (e.profile) {
+            if (single && e.passes > 1) t = e.passStageMs[j];
+            else cudaEventElapsedTime(&t, e.stageEv[j], e.stageEv[j + 1]);
+        }
         o.stage_ms[j] = t;
     }
 }
@@ -1061,7 +1102,9 @@ int fdzb_ctx_launch_async(fdzb_ctx *c)
     FrameSpec f;
     if (int rc = ctx_frame(c, f)) return rc;
     c->eng.frames.assign(1, f);
-    return engine_enqueue(c->eng);
+    const int rc = engine_launch(c->eng);
+    if (rc == FDZB_OK && !c->eng.pending) frame_stats(c->eng, 0, c->stats);
+    return rc;
 }
 
 int fdzb_ctx_sync(fdzb_ctx *c)
@@ -1279,7 +1322,7 @@ int fdzb_batch_launch_async(fdzb_batch *b, const fdzb_frame_desc *frames, int n)
         b->chosenBins[i] = specs[i].bins;
     }
     b->eng.frames.swap(specs);
-    return engine_enqueue(b->eng);
+    return engine_launch(b->eng);
 }
 
 int fdzb_batch_sync(fdzb_batch *b, float *ms)

@@ -60,9 +60,15 @@ struct Engine {
     // triangle passes of the last single-frame launch (1 = none) and their sums
     int passes = 1;
     unsigned long long passPairs = 0, passTests = 0, passRows = 0, passPartial = 0;
+    float passStageMs[STAGE_COUNT] = {};
     long long passValidTris = 0;
     uint32_t *passMasks = nullptr;            // mask buffer for passes when the caller keeps none
     size_t passMasksBytes = 0;
+    // triangle ranges of the last frame that needed passes, reused while the
+    // same frame (buffers, sizes, bins, light grid, capacity) is launched again
+    std::vector<std::pair<long long, long long>> passPlan;
+    std::tuple<const void *, const void *, int, int, const void *, const void *, size_t, int, int, long long>
+        passKey{};
     // pinned host staging, grown to the largest frame list
     FrameDesc *hFrames = nullptr;
     FrameState *hStates = nullptr;
@@ -89,6 +95,9 @@ int engine_init(Engine &e, int device);
 void engine_release(Engine &e);
 // Enqueues e.frames (checked) without waiting.
 int engine_enqueue(Engine &e);
+// Launch entry of contexts and batches: a single frame known to need triangle
+// passes runs them at once (synchronously); anything else is engine_enqueue.
+int engine_launch(Engine &e);
 // Waits for the pending launch; re-runs it if the pair buffer overflowed.
 int engine_sync(Engine &e);
 // Statistics of frame i of the last completed launch / of the whole launch.
