@@ -46,6 +46,23 @@ OPS_PER_PARTIAL = 7
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
+def max_over_ranks(x: float, dist, device: str = "cuda") -> float:
+    """The largest value of x over all ranks (the timing rule for N > 1): every
+    rank calls it at the same point; with no process group it returns x."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, n_ranks: int, ms_max: float) -> float:
+    """Units per second of the whole job: every rank processed units_per_rank
+    in at most ms_max milliseconds (replicas, weak scaling)."""
+    return n_ranks * units_per_rank * 1e3 / ms_max
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -111,9 +128,10 @@ def measured_peaks() -> dict:
         return {}
 
 
-def profile_traffic(kernel: str) -> float | None:
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_hd.md")
+def profile_traffic(kernel: str, workload: str) -> float | None:
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary, if there is one."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -583,13 +601,9 @@ def main():
     with ClockSampler(local) as clk:
         frame_ms, stats = timed(False)
     torch.cuda.synchronize()
-    total_ms = sum(frame_ms)
-    if dist:
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(sum(frame_ms), dist)
     ms_step = total_ms / args.steps
-    value = args.gpus * 1e3 / ms_step
+    value = whole_job_rate(args.steps, args.gpus, total_ms)
     st = stats[-1]
     assert all(s["replans"] == 0 for s in stats), "pair buffer regrown inside the timed region"
 
@@ -623,12 +637,8 @@ def main():
         ctx.sync()
         stream.synchronize()
         e2e_ms.append(a.elapsed_time(b))
-    e2e_total = sum(e2e_ms)
-    if dist:
-        tt = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
-    e2e_value = args.gpus * 1e3 * args.steps / e2e_total
+    e2e_total = max_over_ranks(sum(e2e_ms), dist)
+    e2e_value = whole_job_rate(args.steps, args.gpus, e2e_total)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -657,7 +667,7 @@ def main():
         "stage_ms": dict(zip(fdzb.STAGES, stage)),
         "roofline": {"kernel": "k_occlusion", "bound": "alu", "achieved": achieved / 1e9,
                      "peak": alu_peak / 1e9, "unit": "Gop/s", "frac": achieved / alu_peak,
-                     "traffic": profile_traffic("k_occlusion"),
+                     "traffic": profile_traffic("k_occlusion", args.config),
                      "ops_per_launch": ops, "launch_ms": occ_ms,
                      "note": "algorithmic FP32/INT32 ops of the reference per-pair code / measured FP32 "
                              "issue rate (lane ops/s) of this GPU"},
