@@ -65,7 +65,8 @@ EXPORTED = [
 STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
 
 TRI_ORDER_REFERENCE = 0
-TRI_ORDER_DEPTH = 1
+TRI_ORDER_COVERAGE = 1
+TRI_ORDER_DEPTH = TRI_ORDER_COVERAGE
 
 OCC_LANE_PER_SAMPLE = 0
 OCC_LANE_PER_PAIR = 1
@@ -326,7 +327,7 @@ class Context:
         _check(self._lib.fdzb_ctx_set_profiling(self._h, int(bool(enable))))
 
     def set_tri_order(self, order: int) -> None:
-        """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_DEPTH."""
+        """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_COVERAGE."""
         _check(self._lib.fdzb_ctx_set_tri_order(self._h, int(order)))
 
     def set_graph(self, enable: bool) -> None:

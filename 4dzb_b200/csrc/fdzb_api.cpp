@@ -314,7 +314,7 @@ int engine_enqueue(Engine &e)
     // key bits left over in the last radix pass, at least 4.
     {
         const int binBits = ceil_log2(NB);
-        if (e.triOrder == FDZB_TRI_ORDER_DEPTH) {
+        if (e.triOrder == FDZB_TRI_ORDER_COVERAGE) {
             const int passes = (binBits + 4 + 7) / 8;
             b.depthBits = std::min(10, passes * 8 - binBits);
         } else {
@@ -697,7 +697,7 @@ struct fdzb_ctx {
 
 struct fdzb_batch {
     Engine eng;
-    int triOrder = FDZB_TRI_ORDER_DEPTH;
+    int triOrder = FDZB_TRI_ORDER_COVERAGE;
     TuneTable tuned;
     std::vector<int> chosenBins;
     long long tuneLaunches = 0;
@@ -988,7 +988,7 @@ int fdzb_ctx_set_pair_capacity_limit(fdzb_ctx *c, int64_t pairs)
 int fdzb_ctx_set_tri_order(fdzb_ctx *c, int order)
 {
     if (int rc = ctx_check(c)) return rc;
-    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_DEPTH)
+    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_COVERAGE)
         return fail(FDZB_ERR_INVALID_ARG, "unknown triangle order");
     c->eng.triOrder = order;
     return FDZB_OK;
@@ -1303,7 +1303,7 @@ int fdzb_batch_set_occlusion_schedule(fdzb_batch *b, int schedule)
 int fdzb_batch_set_tri_order(fdzb_batch *b, int order)
 {
     if (int rc = batch_check(b)) return rc;
-    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_DEPTH)
+    if (order != FDZB_TRI_ORDER_REFERENCE && order != FDZB_TRI_ORDER_COVERAGE)
         return fail(FDZB_ERR_INVALID_ARG, "unknown triangle order");
     b->eng.triOrder = order;
     return FDZB_OK;

@@ -52,7 +52,7 @@ struct Engine {
     DeviceBuffers buf{};
     long long pairCapacity = 0;
     int debug = 0;  // keep pre-sort copies for export
-    int triOrder = FDZB_TRI_ORDER_DEPTH;
+    int triOrder = FDZB_TRI_ORDER_COVERAGE;
     bool profile = false;  // record events at the stage boundaries
     bool useGraph = true;
     int occVariant = 0;    // occlusion kernel (DeviceBuffers::occVariant)

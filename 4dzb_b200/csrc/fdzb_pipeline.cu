@@ -562,16 +562,27 @@ __global__ void __launch_bounds__(kTriThreads)
         if (cnt > 0) {
             unsigned long long pos = s_excl + mine_excl;
             const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
-            // Secondary key (depth order): bucket of the triangle's largest light
-            // depth, ascending bucket = lowest triangles first.  Bucket 0 in
-            // reference order, which keeps the reference's (bin, triangle) order.
+            // Secondary key (coverage order): the triangle's angular size seen
+            // from below, world area / (f - minz)^2 with f - minz the light-depth
+            // distance from the far plane (about the receivers' depth) to the
+            // triangle's vertex nearest the light, as a log-scale bucket; the
+            // largest come first.  A sample's mask is the OR over its bin's
+            // triangles, so the order changes only how soon its light rows fill
+            // (the early-out), never the result.  Bucket 0 in reference order,
+            // which keeps the reference's (bin, triangle) order.
             uint32_t bucket = 0u;
             if (depthBits > 0) {
                 const float f = states[fi].f;
-                const float maxz = __ldg(&rec[4 * (size_t)g + 1].w);
-                const float q = __fmul_rn(__fsub_rn(f, maxz), __fdiv_rn((float)(1 << depthBits), f));
-                const int bq = (int)fminf(fmaxf(q, 0.0f), (float)((1 << depthBits) - 1));
-                bucket = (uint32_t)bq;
+                const float4 r0 = __ldg(&rec[4 * (size_t)g]), r1 = __ldg(&rec[4 * (size_t)g + 1]),
+                             r2 = __ldg(&rec[4 * (size_t)g + 2]);
+                const float ax = r1.x - r0.x, ay = r1.y - r0.y, az = r1.z - r0.z;
+                const float bx = r2.x - r0.x, by = r2.y - r0.y, bz = r2.z - r0.z;
+                const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+                const float area2 = fmaxf(sqrtf(cx * cx + cy * cy + cz * cz), 1e-30f);
+                const float d = fmaxf(f - r0.w, 1e-6f);   // r0.w: the triangle's least light depth
+                const float nb = (float)(1 << depthBits);
+                const float q = -log2f(area2 / (d * d)) * (nb / 40.0f) + 0.5f * nb;
+                bucket = (uint32_t)(int)fminf(fmaxf(q, 0.0f), nb - 1.0f);
             }
             for (int j = c.cby; j < c.cey; ++j)
                 for (int i = c.cbx; i < c.cex; ++i) {

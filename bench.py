@@ -660,7 +660,7 @@ def main():
         "config": {"workload": f"{args.config}: {scene.W}x{scene.H} samples x {scene.T} triangles x "
                                f"{scene.light.n}x{scene.light.n} light, {scene.bins}^2 bins",
                    "W": scene.W, "H": scene.H, "triangles": scene.T, "light_grid": scene.light.n,
-                   "bins": scene.bins, "tri_order": "depth" if args.tri_order else "reference",
+                   "bins": scene.bins, "tri_order": "coverage" if args.tri_order else "reference",
                    "l2": "flushed (256 MB write) before every timed frame", "parallelism": f"replicas{args.gpus}"},
         "pair_tests_per_s": st["pair_tests"] * 1e3 / ms_step * args.gpus,
         "effective_gpairs_per_s": scene.S * scene.T * 1e3 / ms_step * args.gpus / 1e9,

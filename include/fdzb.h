@@ -197,9 +197,11 @@ int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
  * both orders -- a sample's mask is the OR over its bin's triangles -- only the
  * number of pair tests before a sample's light is fully blocked changes.
  *   FDZB_TRI_ORDER_REFERENCE: the reference's order (parity of the sorted lists);
- *   FDZB_TRI_ORDER_DEPTH (default): lowest triangles first. */
+ *   FDZB_TRI_ORDER_COVERAGE (default): largest angular size first (triangle area
+ *     over the squared light-depth distance from the far plane to its top vertex). */
 #define FDZB_TRI_ORDER_REFERENCE 0
-#define FDZB_TRI_ORDER_DEPTH     1
+#define FDZB_TRI_ORDER_COVERAGE  1
+#define FDZB_TRI_ORDER_DEPTH     FDZB_TRI_ORDER_COVERAGE   /* earlier name of the same value */
 int fdzb_ctx_set_tri_order(fdzb_ctx *ctx, int order);
 
 /* Warp schedule of the occlusion stage (no counterpart in the reference, which

@@ -14,7 +14,7 @@ import oracle
 def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0):
     """One frame through the library's public Context API; returns
     (outputs dict, stats dict, exported intermediates dict).  tri_order 0 is the
-    reference's per-bin triangle order, 1 the depth order; schedule selects the
+    reference's per-bin triangle order, 1 the coverage order; schedule selects the
     occlusion kernel's warp schedule."""
     fdzb = importlib.import_module("4dzb_b200")
     ctx, t = fdzb.context_for_scene(scene, masks=masks, debug=True, tri_order=tri_order)
@@ -110,7 +110,7 @@ def compare(scene, gpu=None, orc=None, check_intermediates: bool = True) -> list
                 if out.get("tri_order", 0) == 0:
                     _eq("sorted_pair_tri", ex["sorted_pair_tri"], o["sorted_pair_tri"], errs)
                 else:
-                    # depth order: same bins, same triangle set per bin, lowest first
+                    # coverage order: same bins, same triangle set per bin, other order
                     kb, vt = _per_bin_sorted(ex["sorted_pair_bin"], ex["sorted_pair_tri"])
                     _eq("sorted_pair_tri (per-bin set)", vt, o["sorted_pair_tri"], errs)
             _eq("bin_tri_start", ex["bin_tri_start"], o["bin_tri_start"], errs)

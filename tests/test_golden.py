@@ -3,7 +3,7 @@
 
 * the oracle reproduces every stored stage bit for bit (CPU);
 * the CUDA pipeline reproduces every stored stage bit for bit (GPU), in the
-  reference's triangle order and, for masks and shadows, in depth order;
+  reference's triangle order and, for masks and shadows, in coverage order;
 * where the reference sources are present, the harness rebuilt here
   reproduces the fixtures (pins the fixtures to the sources).
 """

@@ -4,7 +4,7 @@ Bar: bin keys, sorted sample order, per-bin segments and statistics, triangle
 footprints, per-triangle bin counts, triangle/bin pairs (before and after the
 sort), per-bin triangle segments, N^2-bit masks and shadow values all equal the
 FP32 restatement bit for bit (both sides compute with unfused IEEE binary32
-operations in the reference's order).  In depth order the per-bin triangle
+operations in the reference's order).  In coverage order the per-bin triangle
 lists are a permutation of the reference's (checked as sets); masks and shadows
 must still match bit for bit.
 """

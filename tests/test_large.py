@@ -70,7 +70,7 @@ def test_large_full_frame_properties(cuda_ok, fdzb, large):
     t["masks"].zero_()
     ctx.launch()
     assert torch.equal(t["masks"], mk)
-    ctx.set_tri_order(fdzb.TRI_ORDER_DEPTH)
+    ctx.set_tri_order(fdzb.TRI_ORDER_COVERAGE)
     ctx.set_occlusion_schedule(fdzb.OCC_LANE_PER_PAIR)
     t["masks"].zero_()
     ctx.launch()
