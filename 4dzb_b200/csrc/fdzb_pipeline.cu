@@ -467,6 +467,75 @@ __device__ __forceinline__ bool bin_accepts(const uint32_t *binStat, int gbin, c
     return maxz >= c.bz && c.bx < Rx && c.by < Ry && Rz < c.ex && Rw < c.ey;
 }
 
+// Coverage-order bucket of a triangle (secondary pair key): the triangle's
+// angular size seen from below, world area / (f - minz)^2 with f - minz the
+// light-depth distance from the far plane (about the receivers' depth) to the
+// triangle's vertex nearest the light, as a log-scale bucket; the largest
+// come first.  A sample's mask is the OR over its bin's triangles, so the order
+// changes only how soon its light rows fill (the early-out), never the result.
+__device__ __forceinline__ uint32_t coverage_bucket(const float4 *__restrict__ rec, int g, float f, int depthBits)
+{
+    if (depthBits <= 0) return 0u;   // reference order: the reference's (bin, triangle) order
+    const float4 r0 = __ldg(&rec[4 * (size_t)g]), r1 = __ldg(&rec[4 * (size_t)g + 1]),
+                 r2 = __ldg(&rec[4 * (size_t)g + 2]);
+    const float ax = r1.x - r0.x, ay = r1.y - r0.y, az = r1.z - r0.z;
+    const float bx = r2.x - r0.x, by = r2.y - r0.y, bz = r2.z - r0.z;
+    const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    const float area2 = fmaxf(sqrtf(cx * cx + cy * cy + cz * cz), 1e-30f);
+    const float d = fmaxf(f - r0.w, 1e-6f);   // r0.w: the triangle's least light depth
+    const float nb = (float)(1 << depthBits);
+    const float q = -log2f(area2 / (d * d)) * (nb / 40.0f) + 0.5f * nb;
+    return (uint32_t)(int)fminf(fmaxf(q, 0.0f), nb - 1.0f);
+}
+
+// Candidate bins of a triangle, swept by a warp 32 at a time in row-major
+// order; returns the number accepted and, with write != nullptr, writes the
+// accepted (bin, triangle) pairs from position `pos` on, in order.
+__device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, const TriBins &c, int bb, int l2,
+                                          int lane, uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals,
+                                          unsigned long long pos, int capacity, int depthBits, uint32_t bucket,
+                                          int g, bool write)
+{
+    const int w = c.cex - c.cbx, h = c.cey - c.cby;
+    if (w <= 0 || h <= 0) return 0;
+    const int n = w * h;
+    int total = 0;
+    // lane's slot li = base + lane; (j, i) kept incrementally
+    int j = c.cby + lane / w, i = c.cbx + lane % w;
+    const int stepJ = 32 / w, stepI = 32 % w;
+    for (int base = 0; base < n; base += 32) {
+        const int li = base + lane;
+        bool ok = false;
+        int gb = 0;
+        if (li < n) {
+            gb = bb + ((j << l2) | i);
+            ok = bin_accepts(binStat, gb, c);
+        }
+        const unsigned m = __ballot_sync(kFullWarp, ok);
+        if (write && ok) {
+            const unsigned long long p = pos + (unsigned long long)total + (unsigned)__popc(m & lanemask_lt());
+            if (p < (unsigned long long)capacity) {
+                pkeys[p] = ((uint32_t)gb << depthBits) | bucket;
+                pvals[p] = (uint32_t)g;
+            }
+        }
+        total += __popc(m);
+        j += stepJ;
+        i += stepI;
+        if (i >= c.cex) {
+            i -= w;
+            ++j;
+        }
+    }
+    return total;
+}
+
+// k_tri_pairs: persistent tiles of kTriThreads triangles; a warp takes the
+// tile's triangles in turn (warp w: triangles w, w + 8, ...) and sweeps each
+// one's candidate bins with its 32 lanes.  Count pass, block scan of the
+// per-triangle counts, decoupled look-back over tiles for the tile's global
+// offset, then the write pass in the same order: pairs come out in triangle
+// order, bins row-major -- the reference's layout.
 __global__ void __launch_bounds__(kTriThreads)
     k_tri_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int *__restrict__ triBases, int nframes, int totalTris,
@@ -477,6 +546,7 @@ __global__ void __launch_bounds__(kTriThreads)
 {
     constexpr int WARPS = kTriThreads / 32;
     __shared__ int s_tile;
+    __shared__ int s_cnt[kTriThreads];
     __shared__ unsigned long long s_wsum[WARPS];
     __shared__ unsigned long long s_excl;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -488,27 +558,29 @@ __global__ void __launch_bounds__(kTriThreads)
         __syncthreads();
         const int tile = s_tile;
         if (tile >= ntiles) break;
-        const int g = tile * kTriThreads + tid;
-        TriBins c;
-        c.any = false;
-        int fi = 0, cnt = 0;
-        if (g < totalTris) {
-            fi = frame_of(triBases, nframes, g);
-            const FrameState &st = states[fi];
-            if (st.state == 2 && st.nValidTris > 0) {
-                const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
-                             q3 = __ldg(rec + 4 * (size_t)g + 3);
-                c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
-                if (c.any) {
-                    const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
-                    for (int j = c.cby; j < c.cey; ++j)
-                        for (int i = c.cbx; i < c.cex; ++i)
-                            cnt += bin_accepts(binStat, bb + ((j << l2) | i), c) ? 1 : 0;
+        const int t0 = tile * kTriThreads;
+        // count pass: warp per triangle
+        for (int k = warp; k < kTriThreads; k += WARPS) {
+            const int g = t0 + k;
+            int cnt = 0;
+            if (g < totalTris) {
+                const int fi = frame_of(triBases, nframes, g);
+                const FrameState &st = states[fi];
+                if (st.state == 2 && st.nValidTris > 0) {
+                    const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
+                                 q3 = __ldg(rec + 4 * (size_t)g + 3);
+                    const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
+                    if (c.any)
+                        cnt = sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals, 0,
+                                         capacity, depthBits, 0u, g, false);
                 }
+                if (lane == 0) triCount[g] = cnt;
             }
-            triCount[g] = cnt;
+            if (lane == 0) s_cnt[k] = cnt;
         }
-        // block inclusive scan of cnt
+        __syncthreads();
+        // block inclusive scan of the per-triangle counts (thread tid holds triangle tid)
+        const int cnt = s_cnt[tid];
         unsigned long long x = (unsigned long long)cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -523,6 +595,8 @@ __global__ void __launch_bounds__(kTriThreads)
             total += s_wsum[w];
         }
         const unsigned long long mine_excl = wbase + x - (unsigned long long)cnt;
+        __syncthreads();
+        s_cnt[tid] = (int)min(mine_excl, (unsigned long long)0x7fffffff);   // now: exclusive offset in the tile
         if (tid == 0) {
             unsigned long long excl = 0;
             unsigned long long *my = scanStatus + tile;
@@ -559,42 +633,21 @@ __global__ void __launch_bounds__(kTriThreads)
             }
         }
         __syncthreads();
-        if (cnt > 0) {
-            unsigned long long pos = s_excl + mine_excl;
-            const int bb = frames[fi].binBase, l2 = frames[fi].log2Wb;
-            // Secondary key (coverage order): the triangle's angular size seen
-            // from below, world area / (f - minz)^2 with f - minz the light-depth
-            // distance from the far plane (about the receivers' depth) to the
-            // triangle's vertex nearest the light, as a log-scale bucket; the
-            // largest come first.  A sample's mask is the OR over its bin's
-            // triangles, so the order changes only how soon its light rows fill
-            // (the early-out), never the result.  Bucket 0 in reference order,
-            // which keeps the reference's (bin, triangle) order.
-            uint32_t bucket = 0u;
-            if (depthBits > 0) {
-                const float f = states[fi].f;
-                const float4 r0 = __ldg(&rec[4 * (size_t)g]), r1 = __ldg(&rec[4 * (size_t)g + 1]),
-                             r2 = __ldg(&rec[4 * (size_t)g + 2]);
-                const float ax = r1.x - r0.x, ay = r1.y - r0.y, az = r1.z - r0.z;
-                const float bx = r2.x - r0.x, by = r2.y - r0.y, bz = r2.z - r0.z;
-                const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
-                const float area2 = fmaxf(sqrtf(cx * cx + cy * cy + cz * cz), 1e-30f);
-                const float d = fmaxf(f - r0.w, 1e-6f);   // r0.w: the triangle's least light depth
-                const float nb = (float)(1 << depthBits);
-                const float q = -log2f(area2 / (d * d)) * (nb / 40.0f) + 0.5f * nb;
-                bucket = (uint32_t)(int)fminf(fmaxf(q, 0.0f), nb - 1.0f);
-            }
-            for (int j = c.cby; j < c.cey; ++j)
-                for (int i = c.cbx; i < c.cex; ++i) {
-                    const int gb = bb + ((j << l2) | i);
-                    if (bin_accepts(binStat, gb, c)) {
-                        if (pos < (unsigned long long)capacity) {
-                            pkeys[pos] = ((uint32_t)gb << depthBits) | bucket;
-                            pvals[pos] = (uint32_t)g;
-                        }
-                        ++pos;
-                    }
-                }
+        // write pass, same order
+        const unsigned long long tileBase = s_excl;
+        for (int k = warp; k < kTriThreads; k += WARPS) {
+            const int g = t0 + k;
+            if (g >= totalTris) continue;
+            const int fi = frame_of(triBases, nframes, g);
+            const FrameState &st = states[fi];
+            if (!(st.state == 2 && st.nValidTris > 0)) continue;
+            const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
+                         q3 = __ldg(rec + 4 * (size_t)g + 3);
+            const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
+            if (!c.any) continue;
+            const uint32_t bucket = coverage_bucket(rec, g, st.f, depthBits);
+            sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals,
+                       tileBase + (unsigned long long)s_cnt[k], capacity, depthBits, bucket, g, true);
         }
     }
 }
