@@ -147,7 +147,10 @@ cudaError_t measure_alu_rate(double *laneOpsPerSecond);
 int set_error(int code, const std::string &msg);
 int sort_passes_for(long long keyRangeExclusive);
 cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t stream);
-constexpr int kSortTileHost = 4096;   // keys per radix-sort tile (fdzb_sort.cuh)
+#ifndef FDZB_SORT_ITEMS
+#define FDZB_SORT_ITEMS 8
+#endif
+constexpr int kSortTileHost = 256 * FDZB_SORT_ITEMS;   // keys per radix-sort tile (fdzb_sort.cuh)
 constexpr int kTriTileHost = 256;     // triangles per pair-scan tile
 
 }  // namespace fdzb

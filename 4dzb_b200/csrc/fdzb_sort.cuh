@@ -8,7 +8,9 @@
 //   2. one scatter pass per digit: each CTA takes the next tile ticket, ranks its
 //      keys with warp match/popc against per-warp shared histograms, publishes its
 //      per-digit tile count, and finds its global offsets by a decoupled look-back
-//      over the previous tiles' published counts (bounded waits), then scatters.
+//      over the previous tiles' published counts (bounded waits); the tile is
+//      reordered by digit in shared memory, then written out in digit runs, so
+//      that consecutive threads store to consecutive addresses.
 // The element count may live in device memory (n_dev), so the sort is enqueued
 // without a host round trip.
 #pragma once
@@ -16,9 +18,12 @@
 
 namespace fdzb {
 
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;   // 4096 keys per tile
+#ifndef FDZB_SORT_MINBLOCKS
+#define FDZB_SORT_MINBLOCKS 4
+#endif
+constexpr int kSortThreads = 256;                      // = kRadix: thread d handles digit d
+constexpr int kSortItems = FDZB_SORT_ITEMS;
+constexpr int kSortTile = kSortThreads * kSortItems;   // keys per tile
 constexpr int kRadix = 256;
 // Look-back status word: [63:32] launch epoch, [31:30] flag, [29:0] count.  A
 // word whose epoch is not the current one reads as "not yet published", so the
@@ -52,7 +57,7 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 // One digit pass.  status: [tiles * 256] zeroed before the pass; ticket zeroed.
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
     k_radix_pass(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                  uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, const int *n_dev,
                  int n_static, int cap, int shift, const uint32_t *__restrict__ hist,
@@ -63,7 +68,10 @@ __global__ void __launch_bounds__(kSortThreads)
     __shared__ uint32_t s_start[kRadix];
     __shared__ uint32_t s_whist[WARPS][kRadix];
     __shared__ uint32_t s_base[kRadix];
+    __shared__ uint32_t s_tstart[kRadix];
     __shared__ uint32_t s_scan[WARPS];
+    __shared__ uint32_t s_k[kSortTile];
+    __shared__ uint32_t s_v[kSortTile];
     __shared__ int s_tile;
 
     const int n = sort_count(n_dev, n_static, cap);
@@ -95,6 +103,7 @@ __global__ void __launch_bounds__(kSortThreads)
         __syncthreads();
         const int tile = s_tile;
         if ((long long)tile * kSortTile >= n) break;
+        const int tileN = min(kSortTile, n - tile * kSortTile);
 
         const int base = tile * kSortTile + warp * (kSortItems * 32);
         uint32_t k[kSortItems], v[kSortItems], rk[kSortItems];
@@ -120,13 +129,26 @@ __global__ void __launch_bounds__(kSortThreads)
         }
         __syncthreads();
 
-        // Per digit: prefix over warps and tile total.
+        // Per digit: prefix over warps, tile total, and the digit's start in the tile.
         uint32_t run = 0;
 #pragma unroll
         for (int w = 0; w < WARPS; ++w) {
             uint32_t c = s_whist[w][tid];
             s_whist[w][tid] = run;
             run += c;
+        }
+        {
+            uint32_t x = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(kFullWarp, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_scan[warp] = x;
+            __syncthreads();
+            uint32_t wbase = 0;
+            for (int w = 0; w < warp; ++w) wbase += s_scan[w];
+            s_tstart[tid] = wbase + x - run;
         }
         // Decoupled look-back on digit tid.
         unsigned long long *my = status + (size_t)tile * kRadix + tid;
@@ -154,19 +176,30 @@ __global__ void __launch_bounds__(kSortThreads)
             }
             st_volatile_u64(my, ep | kStatPrefix | (excl + run));
         }
+        // global position of the tile's first element with digit tid
         s_base[tid] = s_start[tid] + excl;
         __syncthreads();
 
+        // reorder the tile by digit in shared memory (stable)
 #pragma unroll
         for (int i = 0; i < kSortItems; ++i) {
             const int idx = base + i * 32 + lane;
             if (idx < n) {
                 const uint32_t d = (k[i] >> shift) & 255u;
-                const uint32_t dst = s_base[d] + s_whist[warp][d] + rk[i];
-                if (dst < (uint32_t)cap) {
-                    kout[dst] = k[i];
-                    vout[dst] = v[i];
-                }
+                const uint32_t lp = s_tstart[d] + s_whist[warp][d] + rk[i];
+                s_k[lp] = k[i];
+                s_v[lp] = v[i];
+            }
+        }
+        __syncthreads();
+        // write out: element j of the reordered tile goes to s_base[d] + (j - s_tstart[d])
+        for (int j = tid; j < tileN; j += kSortThreads) {
+            const uint32_t kk = s_k[j];
+            const uint32_t d = (kk >> shift) & 255u;
+            const uint32_t dst = s_base[d] + ((uint32_t)j - s_tstart[d]);
+            if (dst < (uint32_t)cap) {
+                kout[dst] = kk;
+                vout[dst] = s_v[j];
             }
         }
     }
