@@ -68,15 +68,17 @@ def test_hd_preset_sampled(cuda_ok, scenes):
     _check(scenes.preset("hd"), 1, occ_stride=97)
 
 
+@pytest.mark.parametrize("schedule", [1])
 @pytest.mark.parametrize("n,bins", [(1, 4), (4, 8), (8, 16), (16, 32), (32, 16)])
 @pytest.mark.parametrize("order", ORDERS)
-def test_lane_per_pair_schedule(cuda_ok, scenes, n, bins, order):
+def test_other_occlusion_schedules(cuda_ok, scenes, n, bins, order, schedule):
     """The lane-per-pair occlusion schedule: same masks and shadows, bit for bit."""
-    _check(scenes.make_scene(200, 150, 3000, n=n, bins=bins, seed=80 + n, sigma=0.12), order, schedule=1)
+    _check(scenes.make_scene(200, 150, 3000, n=n, bins=bins, seed=80 + n, sigma=0.12), order, schedule=schedule)
 
 
-def test_lane_per_pair_schedule_medium(cuda_ok, scenes):
-    _check(scenes.make_scene(640, 480, 20000, n=16, bins=64, seed=21, sigma=0.1), 1, schedule=1)
+@pytest.mark.parametrize("schedule", [1])
+def test_other_occlusion_schedules_medium(cuda_ok, scenes, schedule):
+    _check(scenes.make_scene(640, 480, 20000, n=16, bins=64, seed=21, sigma=0.1), 1, schedule=schedule)
 
 
 @pytest.mark.parametrize("masks", [True, False])
