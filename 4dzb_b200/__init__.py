@@ -57,6 +57,7 @@ EXPORTED = [
     "fdzb_batch_launch_async", "fdzb_batch_sync", "fdzb_batch_launch", "fdzb_batch_get_frame_stats",
     "fdzb_batch_get_stats", "fdzb_batch_frame_bins", "fdzb_batch_autotune",
     "fdzb_ctx_set_occlusion_schedule", "fdzb_batch_set_occlusion_schedule", "fdzb_ctx_set_pair_capacity_limit",
+    "fdzb_ctx_set_model_transform", "fdzb_ctx_set_shadow_method", "fdzb_light_sample_positions", "fdzb_shade",
     "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
@@ -67,6 +68,9 @@ STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
 TRI_ORDER_REFERENCE = 0
 TRI_ORDER_COVERAGE = 1
 TRI_ORDER_DEPTH = TRI_ORDER_COVERAGE
+
+SHADOW_EDGE_MASKS = 0
+SHADOW_RAY_CAST = 1
 
 OCC_LANE_PER_SAMPLE = 0
 OCC_LANE_PER_PAIR = 1
@@ -125,7 +129,8 @@ class FrameDesc(ctypes.Structure):
                 ("H", ctypes.c_int32), ("d_vtx", ctypes.c_void_p), ("n_vtx", ctypes.c_size_t),
                 ("vtx_stride_bytes", ctypes.c_size_t), ("d_idx", ctypes.c_void_p), ("n_tri", ctypes.c_size_t),
                 ("light", AreaLightDesc), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
-                ("esp", ctypes.c_float), ("d_shadow", ctypes.c_void_p), ("d_masks", ctypes.c_void_p)]
+                ("esp", ctypes.c_float), ("d_shadow", ctypes.c_void_p), ("d_masks", ctypes.c_void_p),
+                ("model_transform", ctypes.POINTER(ctypes.c_float))]
 
 
 class BatchStats(ctypes.Structure):
@@ -150,7 +155,7 @@ class Request(ctypes.Structure):
     _fields_ = [("scene_id", ctypes.c_int32), ("W", ctypes.c_int32), ("H", ctypes.c_int32),
                 ("bins", ctypes.c_int32), ("d_pos", ctypes.c_void_p), ("d_nrm", ctypes.c_void_p),
                 ("light", AreaLightDesc), ("pad0", ctypes.c_int32), ("d_shadow", ctypes.c_void_p),
-                ("d_masks", ctypes.c_void_p)]
+                ("d_masks", ctypes.c_void_p), ("model_transform", ctypes.POINTER(ctypes.c_float))]
 
 
 class RequestResult(ctypes.Structure):
@@ -174,6 +179,15 @@ class ServeStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class ShadeDesc(ctypes.Structure):
+    """fdzb_shade_desc."""
+    _fields_ = [("W", ctypes.c_int32), ("H", ctypes.c_int32), ("d_g0", ctypes.c_void_p), ("d_g1", ctypes.c_void_p),
+                ("d_g2", ctypes.c_void_p), ("d_g3", ctypes.c_void_p), ("d_shadow", ctypes.c_void_p),
+                ("d_rgba", ctypes.c_void_p), ("camera_pos", ctypes.c_float * 3), ("La", ctypes.c_float * 3),
+                ("Ld", ctypes.c_float * 3), ("Ls", ctypes.c_float * 3), ("n_light_samples", ctypes.c_int32),
+                ("d_light_samples", ctypes.c_void_p)]
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -221,7 +235,11 @@ def load() -> ctypes.CDLL:
         "fdzb_version": ([], ctypes.c_char_p),
         "fdzb_ctx_set_graph": ([vp, i32], i32),
         "fdzb_ctx_set_occlusion_schedule": ([vp, i32], i32),
-        "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32), "fdzb_batch_set_occlusion_schedule": ([vp, i32], i32),
+        "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32),
+        "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
+        "fdzb_ctx_set_shadow_method": ([vp, i32], i32),
+        "fdzb_light_sample_positions": ([P(AreaLightDesc), P(ctypes.c_float)], i32),
+        "fdzb_shade": ([P(ShadeDesc), vp], i32), "fdzb_batch_set_occlusion_schedule": ([vp, i32], i32),
         "fdzb_batch_create": ([P(vp), i32], i32), "fdzb_batch_destroy": ([vp], i32),
         "fdzb_batch_set_stream": ([vp, vp], i32), "fdzb_batch_set_graph": ([vp, i32], i32),
         "fdzb_batch_set_profiling": ([vp, i32], i32), "fdzb_batch_set_tri_order": ([vp, i32], i32),
@@ -375,6 +393,18 @@ class Context:
         arr = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
         _check(self._lib.fdzb_ctx_move_model(self._h, arr))
 
+    def set_shadow_method(self, method: int) -> None:
+        """SHADOW_EDGE_MASKS (default) or SHADOW_RAY_CAST (the reference's REF_CAL checker)."""
+        _check(self._lib.fdzb_ctx_set_shadow_method(self._h, int(method)))
+
+    def set_model_transform(self, m) -> None:
+        """Column-major 4x4 applied to the vertices as they are read (None clears)."""
+        if m is None:
+            _check(self._lib.fdzb_ctx_set_model_transform(self._h, None))
+            return
+        arr = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
+        _check(self._lib.fdzb_ctx_set_model_transform(self._h, arr))
+
     def launch(self) -> float:
         ms = ctypes.c_float()
         _check(self._lib.fdzb_ctx_launch(self._h, ctypes.byref(ms)))
@@ -518,10 +548,20 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
 # ---- batches ---------------------------------------------------------------
 
 
+def _mat16(m):
+    if m is None:
+        return None
+    return (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
+
+
 def frame_desc(pos, nrm, W: int, H: int, vtx, n_vtx: int, idx, n_tri: int, light, shadow, masks=None,
-               bins: int = 0, cull: bool = False, esp: float = 1e-3, stride_bytes: int = 16) -> FrameDesc:
-    """An fdzb_frame_desc from device tensors (or int pointers); bins 0 = autotuned."""
+               bins: int = 0, cull: bool = False, esp: float = 1e-3, stride_bytes: int = 16,
+               model_transform=None) -> FrameDesc:
+    """An fdzb_frame_desc from device tensors (or int pointers); bins 0 = autotuned;
+    model_transform: optional column-major 4x4 applied to the vertices as read."""
     d = FrameDesc()
+    d._m = _mat16(model_transform)   # keeps the array alive with the descriptor
+    d.model_transform = ctypes.cast(d._m, ctypes.POINTER(ctypes.c_float)) if d._m is not None else None
     d.d_pos, d.d_nrm = _ptr(pos), _ptr(nrm)
     d.W, d.H = W, H
     d.d_vtx, d.n_vtx, d.vtx_stride_bytes = _ptr(vtx), n_vtx, stride_bytes
@@ -612,9 +652,12 @@ class Batch:
 # ---- serving ---------------------------------------------------------------
 
 
-def request(scene_id: int, pos, nrm, W: int, H: int, light, shadow, masks=None, bins: int = 0) -> Request:
+def request(scene_id: int, pos, nrm, W: int, H: int, light, shadow, masks=None, bins: int = 0,
+            model_transform=None) -> Request:
     """An fdzb_request from device tensors (or int pointers)."""
     r = Request()
+    r._m = _mat16(model_transform)
+    r.model_transform = ctypes.cast(r._m, ctypes.POINTER(ctypes.c_float)) if r._m is not None else None
     r.scene_id, r.W, r.H, r.bins = scene_id, W, H, bins
     r.d_pos, r.d_nrm = _ptr(pos), _ptr(nrm)
     r.light = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
@@ -698,3 +741,29 @@ class Server:
 
     def worker_error(self) -> str:
         return self._lib.fdzb_serve_last_worker_error(self._h).decode()
+
+
+# ---- shading pass -----------------------------------------------------------
+
+
+def light_sample_positions(light) -> np.ndarray:
+    """Light-sample positions [H*W, 3] in the reference's numbering (i*W + j)."""
+    d = AreaLightDesc.from_light(light) if not isinstance(light, AreaLightDesc) else light
+    out = np.zeros(3 * d.lightResWidth * d.lightResHeight, np.float32)
+    _check(load().fdzb_light_sample_positions(ctypes.byref(d), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+    return out.reshape(-1, 3)
+
+
+def shade(W: int, H: int, g0, g1, g2, g3, shadow, rgba, camera_pos, La, Ld, Ls, light_samples, stream=None) -> None:
+    """fdzb_shade on device tensors; light_samples: device float tensor [n, 3]."""
+    d = ShadeDesc()
+    d.W, d.H = W, H
+    d.d_g0, d.d_g1, d.d_g2, d.d_g3 = _ptr(g0), _ptr(g1), _ptr(g2), _ptr(g3)
+    d.d_shadow, d.d_rgba = _ptr(shadow), _ptr(rgba)
+    d.camera_pos[:] = [float(v) for v in camera_pos]
+    d.La[:] = [float(v) for v in La]
+    d.Ld[:] = [float(v) for v in Ld]
+    d.Ls[:] = [float(v) for v in Ls]
+    d.n_light_samples = int(light_samples.shape[0])
+    d.d_light_samples = _ptr(light_samples)
+    _check(load().fdzb_shade(ctypes.byref(d), ctypes.c_void_p(stream)))

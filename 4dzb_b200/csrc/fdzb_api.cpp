@@ -55,8 +55,9 @@ int ceil_log2(long long v)
 // ABI layouts mirrored by the ctypes binding
 static_assert(sizeof(fdzb_area_light_desc) == 52, "fdzb_area_light_desc layout");
 static_assert(sizeof(fdzb_frame_stats) == 184, "fdzb_frame_stats layout");
-static_assert(sizeof(fdzb_frame_desc) == 144, "fdzb_frame_desc layout");
+static_assert(sizeof(fdzb_frame_desc) == 152, "fdzb_frame_desc layout");
 static_assert(sizeof(fdzb_batch_stats) == 232, "fdzb_batch_stats layout");
+static_assert(sizeof(fdzb_shade_desc) == 120, "fdzb_shade_desc layout");
 
 constexpr long long kMaxPairCapacity = 1ll << 29;
 constexpr long long kMaxTotalSamples = 0x7fffffffll / 2;
@@ -307,6 +308,7 @@ int engine_enqueue(Engine &e)
     fdzb::DeviceBuffers &b = e.buf;
     b.samplePasses = fdzb::sort_passes_for(NB + 1);
     b.occVariant = e.occVariant;
+    b.rayCast = e.rayCast;
     // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
     // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
     // order appends a depth bucket below the bin so each bin lists its lowest
@@ -350,6 +352,8 @@ int engine_enqueue(Engine &e)
         f.binBase = bb;
         f.accumulate = s.accumulate;
         f.light = s.light;
+        f.hasXform = s.hasXform ? 1 : 0;
+        if (s.hasXform) std::memcpy(f.xform, s.xform, sizeof(f.xform));
         e.hBases[i] = sb;
         e.hBases[nf + i] = tb;
         e.hBases[2 * nf + i] = bb;
@@ -374,6 +378,7 @@ int engine_enqueue(Engine &e)
         k.maxV = maxV;
         k.arena = e.arena;
         k.hFrames = e.hFrames;
+        k.ov = e.occVariant + 16 * e.rayCast;
         k.stream = e.stream;
         if (!e.graph || !(k == e.graphKey)) {
             drop_graph(e);
@@ -691,6 +696,8 @@ struct fdzb_ctx {
     fdzb_area_light_desc lightDesc{};
     fdzb::LightParams light{};
     fdzb_frame_stats stats{};
+    bool hasXform = false;
+    float xform[16] = {};
 };
 
 // ---- batch: a list of independent frames per launch --------------------------
@@ -740,6 +747,8 @@ int ctx_frame(fdzb_ctx *c, FrameSpec &f)
     f.esp = c->esp;
     f.shadow = c->shadow;
     f.masks = c->masks;
+    f.hasXform = c->hasXform;
+    if (c->hasXform) std::memcpy(f.xform, c->xform, sizeof(f.xform));
     return FDZB_OK;
 }
 
@@ -788,6 +797,8 @@ int fdzb::desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
     f.esp = d.esp;
     f.shadow = d.d_shadow;
     f.masks = d.d_masks;
+    f.hasXform = d.model_transform != nullptr;
+    if (f.hasXform) std::memcpy(f.xform, d.model_transform, sizeof(f.xform));
     return FDZB_OK;
 }
 
@@ -1082,6 +1093,24 @@ int fdzb_ctx_set_area_light(fdzb_ctx *c, const fdzb_area_light_desc *d)
     return FDZB_OK;
 }
 
+int fdzb_ctx_set_shadow_method(fdzb_ctx *c, int method)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (method != FDZB_SHADOW_EDGE_MASKS && method != FDZB_SHADOW_RAY_CAST)
+        return fail(FDZB_ERR_INVALID_ARG, "unknown shadow method");
+    if (int rc = ctx_sync(c)) return rc;
+    c->eng.rayCast = method == FDZB_SHADOW_RAY_CAST ? 1 : 0;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_model_transform(fdzb_ctx *c, const float m[16])
+{
+    if (int rc = ctx_check(c)) return rc;
+    c->hasXform = m != nullptr;
+    if (m) std::memcpy(c->xform, m, sizeof(c->xform));
+    return FDZB_OK;
+}
+
 int fdzb_ctx_move_model(fdzb_ctx *c, const float m[16])
 {
     if (int rc = ctx_check(c)) return rc;
@@ -1217,6 +1246,25 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
     }
     if (bytes > avail) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
     if (bytes) FDZB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return FDZB_OK;
+}
+
+int fdzb_light_sample_positions(const fdzb_area_light_desc *d, float *out)
+{
+    if (!d || !out) return fail(FDZB_ERR_INVALID_ARG, "NULL argument");
+    if (d->lightResWidth < 1 || d->lightResHeight < 1 || d->lightResWidth > 64 || d->lightResHeight > 64)
+        return fail(FDZB_ERR_INVALID_ARG, "bad light grid");
+    fdzb::LightParams L;
+    fdzb::light_setup(d->rightRadius, d->topRadius, d->position, d->viewDir, d->upDir, d->lightResWidth,
+                      d->lightResHeight, &L);
+    for (int i = 0; i < d->lightResHeight; ++i)
+        for (int j = 0; j < d->lightResWidth; ++j) {
+            float *p = out + 3 * (i * d->lightResWidth + j);
+            for (int k = 0; k < 3; ++k) {
+                const float a = L.ur[k] + L.xd[k] * (float)j;   // (upRight + x_delt*j) + y_delt*i
+                p[k] = a + L.yd[k] * (float)i;
+            }
+        }
     return FDZB_OK;
 }
 

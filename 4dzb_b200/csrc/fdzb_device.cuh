@@ -23,6 +23,14 @@ __device__ __forceinline__ f3 sub3(f3 a, f3 b)
 {
     return f3{__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)};
 }
+__device__ __forceinline__ f3 add3(f3 a, f3 b)
+{
+    return f3{__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)};
+}
+__device__ __forceinline__ f3 mul3(f3 a, float b)
+{
+    return f3{__fmul_rn(a.x, b), __fmul_rn(a.y, b), __fmul_rn(a.z, b)};
+}
 // ((ax*bx) + (ay*by)) + (az*bz)
 __device__ __forceinline__ float dot3(f3 a, f3 b)
 {
@@ -59,6 +67,19 @@ __device__ __forceinline__ f3 light_project(const float *M, f3 t)
                         __fmul_rn(M[13], 1.0f));
     r.y = __fadd_rn(__fmul_rn(__fdiv_rn(y, r.z), 0.5f), 0.5f);
     return r;
+}
+
+// M * (x, y, z, 1) for a column-major 4x4 M, each component summed left to
+// right (K/moveModel.inl:4-12, the reference's in-place model transform).
+__device__ __forceinline__ f3 transform_point(const float *m, f3 p)
+{
+    const float w = 1.0f;
+    return f3{__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], p.x), __fmul_rn(m[4], p.y)), __fmul_rn(m[8], p.z)),
+                        __fmul_rn(m[12], w)),
+              __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[1], p.x), __fmul_rn(m[5], p.y)), __fmul_rn(m[9], p.z)),
+                        __fmul_rn(m[13], w)),
+              __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[2], p.x), __fmul_rn(m[6], p.y)), __fmul_rn(m[10], p.z)),
+                        __fmul_rn(m[14], w))};
 }
 
 // Order-preserving float <-> uint32 map, so that unsigned integer max/min

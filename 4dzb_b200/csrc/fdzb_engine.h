@@ -31,15 +31,21 @@ struct FrameSpec {
     float *shadow = nullptr;
     uint32_t *masks = nullptr;
     int accumulate = 0;   // OR into `masks` (a later triangle pass of the same frame)
+    bool hasXform = false;  // vertices read through xform (column-major 4x4)
+    float xform[16] = {};
 };
 
 // Host-side parameters that a captured graph bakes in; a launch whose key
 // differs re-captures.
 struct GraphKey {
     int nf = -1, S = 0, T = 0, NB = 0, P = 0, sp = 0, pp = 0, db = 0, maxS = 0, maxT = 0, maxV = 0;
+    int ov = 0;   // occlusion kernel choice (schedule, ray cast)
     const void *arena = nullptr, *hFrames = nullptr;
     cudaStream_t stream = nullptr;
-    auto tie() const { return std::tie(nf, S, T, NB, P, sp, pp, db, maxS, maxT, maxV, arena, hFrames, stream); }
+    auto tie() const
+    {
+        return std::tie(nf, S, T, NB, P, sp, pp, db, maxS, maxT, maxV, ov, arena, hFrames, stream);
+    }
     bool operator==(const GraphKey &o) const { return tie() == o.tie(); }
 };
 
@@ -56,6 +62,7 @@ struct Engine {
     bool profile = false;  // record events at the stage boundaries
     bool useGraph = true;
     int occVariant = 0;    // occlusion kernel (DeviceBuffers::occVariant)
+    int rayCast = 0;       // ray-cast cross-check instead of edge masks (DeviceBuffers::rayCast)
     long long maxPairCapacity = 1ll << 29;   // largest pair buffer; beyond it a frame runs in triangle passes
     // triangle passes of the last single-frame launch (1 = none) and their sums
     int passes = 1;

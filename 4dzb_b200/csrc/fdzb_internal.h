@@ -43,6 +43,8 @@ struct FrameDesc {
     int sampleBase, triBase, binBase;
     int accumulate;         // 1: OR into the masks already in `masks` (later triangle passes)
     LightParams light;
+    int hasXform;           // 1: vertices are read through `xform`
+    float xform[16];        // column-major model transform (K/moveModel.inl:4-12), applied on read
 };
 
 // Slots of FrameState::acc (order-preserving uint32 encodings of floats).
@@ -123,6 +125,7 @@ struct DeviceBuffers {
     int samplePasses, pairPasses;
     int depthBits;                              // secondary (depth-bucket) bits of the pair key
     int occVariant;                             // 0: k_occlusion (lane per sample), 1: k_occlusion_pairs
+    int rayCast;                                // 1: ray-cast cross-check (REF_CAL) instead of edge masks
     uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
                                                 // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays

@@ -166,6 +166,62 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
     return 1;
 }
 
+// Ray-cast pair test: the reference's REF_CAL cross-check (refCal_kernel and
+// intersect_triangle_branchless, K/Step5_2_calRef.inl:1-126).  For every light
+// sample not yet occluded, a ray from the sample's position to the light
+// sample's position; occluded when it meets the triangle with 1e-3 < t < dist.
+// The reference numbers light sample (i along the light's height, j along its
+// width) as i*W + j and places it at upRight + x_delt*j + y_delt*i
+// (FS/api.cpp:351-357); here it is stored in this library's mask layout, row
+// r = j (width), column c = i (height), so that the ray-cast and edge-function
+// masks compare bit for bit.  Same pre-cull as the reference's checker: the
+// sample's rectangle inside the triangle's AABB and minz - 1e-3 (in double, as
+// the reference's double literal makes it) not above the sample's depth.
+__device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample &s, f3 ur, f3 xd, f3 yd,
+                                            int N, uint32_t FULL, uint32_t (*rows)[32], int lane,
+                                            uint32_t &fullRows, uint32_t &nrows)
+{
+    const float4 p0a = T.p[0];
+    const float4 p1a = T.p[1];
+    if (!(s.spz <= p0a.z && s.spw <= p0a.w && s.spx >= p0a.x && s.spy >= p0a.y)) return 0;
+    if ((double)p1a.x - 1e-3 > (double)s.spZ) return 0;
+    const float4 p2a = T.p[2], p3a = T.p[3];
+    const f3 v0 = mk3(p1a.y, p1a.z, p1a.w), v1 = mk3(p2a.x, p2a.y, p2a.z), v2 = mk3(p2a.w, p3a.x, p3a.y);
+    const f3 e0 = sub3(v1, v0);
+    const f3 e1 = sub3(v0, v2);
+    const f3 n = cross3(e1, e0);
+    const f3 q0 = sub3(v0, s.Q);
+    const float tmin = 1e-3f;
+    for (int r = 0; r < N; ++r) {
+        const uint32_t have = rows[r][lane];
+        if (have == FULL) continue;
+        ++nrows;
+        const f3 lr = add3(ur, mul3(xd, (float)r));   // upRight + x_delt * j
+        uint32_t add = 0u;
+        for (int c = 0; c < N; ++c) {
+            if (have & (1u << c)) continue;
+            const f3 lp = add3(lr, mul3(yd, (float)c));   // ... + y_delt * i
+            const f3 L = sub3(lp, s.Q);
+            const float dist = __fsqrt_rn(dot3(L, L));
+            const f3 dir = mk3(__fdiv_rn(L.x, dist), __fdiv_rn(L.y, dist), __fdiv_rn(L.z, dist));
+            const float inv = __fdiv_rn(1.0f, dot3(n, dir));
+            const f3 e2 = mul3(q0, inv);
+            const f3 iv = cross3(dir, e2);
+            const float beta = dot3(iv, e1);
+            const float gamma = dot3(iv, e0);
+            const float t = dot3(n, e2);
+            if ((t < dist) & (t > tmin) & (beta >= 0.0f) & (gamma >= 0.0f) & (__fadd_rn(beta, gamma) <= 1.0f))
+                add |= 1u << c;
+        }
+        if (add) {
+            const uint32_t nv = have | add;
+            rows[r][lane] = nv;
+            if (nv == FULL) fullRows |= 1u << r;
+        }
+    }
+    return 1;
+}
+
 __device__ __forceinline__ void write_result(const FrameDesc &fr, int local, int N, uint32_t (*rows)[32],
                                              int lane)
 {
@@ -264,6 +320,8 @@ __global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restri
     }
 }
 
+// RAYCAST = 1: the ray-cast cross-check instead of the edge-function masks.
+template <int RAYCAST>
 __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
     k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
@@ -364,8 +422,12 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
 #endif
                 if (remaining > 0) {
                     --remaining;
-                    tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows, nrows,
-                                        npart);
+                    if (RAYCAST)
+                        tested += raycast_pair(tris[t], smp, ld3(fr.light.ur), xd, yd, N, FULL, rows, lane,
+                                               fullRows, nrows);
+                    else
+                        tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows, nrows,
+                                            npart);
                     if (fullRows == FULL) remaining = 0;
                 }
             }

@@ -30,6 +30,15 @@
 
 namespace fdzb {
 
+// Vertex v of a frame's model: xyz from the caller's buffer, through the frame's
+// model transform when it has one (the reference rewrites the buffer in place
+// instead, K/moveModel.inl:14-28; both give the same floats).
+__device__ __forceinline__ f3 load_vertex(const FrameDesc &fr, int v)
+{
+    const f3 q = ld3(fr.vtx + (size_t)v * fr.vstride);
+    return fr.hasXform ? transform_point(fr.xform, q) : q;
+}
+
 // ---------------------------------------------------------------------------
 // k_init: empty bin statistics (K/Step3_bindSampleToBin.inl:83-84) and cleared
 // segment tables (K/binRaster.inl:39-40, 52-53).
@@ -127,7 +136,7 @@ __global__ void __launch_bounds__(kReduceThreads)
         }
     } else {
         for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < fr.V; v += stride) {
-            const f3 q = ld3(fr.vtx + (size_t)v * fr.vstride);
+            const f3 q = load_vertex(fr, v);
             acc_max(a[0], light_depth(M, q));
             const f3 r = light_project(M, q);
             acc_min(a[1], r.x);
@@ -262,9 +271,9 @@ __global__ void __launch_bounds__(256)
             if (!okIdx) {
                 atomicOr(err, (int)ERR_BAD_INPUT);
             } else {
-                v0 = ld3(fr.vtx + (size_t)i0 * fr.vstride);
-                v1 = ld3(fr.vtx + (size_t)i1 * fr.vstride);
-                v2 = ld3(fr.vtx + (size_t)i2 * fr.vstride);
+                v0 = load_vertex(fr, i0);
+                v1 = load_vertex(fr, i1);
+                v2 = load_vertex(fr, i2);
                 const f3 n = cross3(sub3(v0, v2), sub3(v1, v0));
                 const bool culled =
                     fr.cull && dot3(n, sub3(ur, v0)) <= 0.0f && dot3(n, sub3(ur, v1)) <= 0.0f &&
@@ -671,13 +680,10 @@ __global__ void k_move_model(float *vtx, int vstride, int V, Mat16 M)
     const float *m = M.m;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
         float *p = vtx + (size_t)v * vstride;
-        const float x = p[0], y = p[1], z = p[2], w = 1.0f;
-        const float rx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], x), __fmul_rn(m[4], y)), __fmul_rn(m[8], z)), __fmul_rn(m[12], w));
-        const float ry = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[1], x), __fmul_rn(m[5], y)), __fmul_rn(m[9], z)), __fmul_rn(m[13], w));
-        const float rz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[2], x), __fmul_rn(m[6], y)), __fmul_rn(m[10], z)), __fmul_rn(m[14], w));
-        p[0] = rx;
-        p[1] = ry;
-        p[2] = rz;
+        const f3 r = transform_point(m, mk3(p[0], p[1], p[2]));
+        p[0] = r.x;
+        p[1] = r.y;
+        p[2] = r.z;
     }
 }
 
@@ -817,12 +823,16 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
         b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
         b.items, b.itemCapacity, b.counters);
-    if (b.occVariant == 1)
+    if (b.rayCast)
+        k_occlusion<1><<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
+            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
+            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    else if (b.occVariant == 1)
         k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(
             b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
             b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
     else
-        k_occlusion<<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
+        k_occlusion<0><<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
             b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
             b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
     nl += 2;

@@ -34,7 +34,7 @@
 
 // ABI layouts mirrored by the ctypes binding
 static_assert(sizeof(fdzb_serve_config) == 40, "fdzb_serve_config layout");
-static_assert(sizeof(fdzb_request) == 104, "fdzb_request layout");
+static_assert(sizeof(fdzb_request) == 112, "fdzb_request layout");
 static_assert(sizeof(fdzb_request_result) == 208, "fdzb_request_result layout");
 static_assert(sizeof(fdzb_serve_stats) == 144, "fdzb_serve_stats layout");
 
@@ -459,6 +459,7 @@ int fdzb_serve_submit(fdzb_server *s, const fdzb_request *q, uint64_t *ticket)
     d.bins = q->bins;
     d.d_shadow = q->d_shadow;
     d.d_masks = q->d_masks;
+    d.model_transform = q->model_transform;
     Request r;
     if (int rc = fdzb::desc_to_spec(d, r.spec, 0)) return rc;
     if (q->W <= 0 || q->H <= 0 || (long long)q->W * q->H > (1ll << 30))

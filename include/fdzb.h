@@ -151,6 +151,27 @@ int fdzb_ctx_set_scenes_esp(fdzb_ctx *ctx, float scenes_esp);
 int fdzb_ctx_set_scene_params(fdzb_ctx *ctx, size_t max_triangle_num, size_t max_vertices_num);
 int fdzb_ctx_set_area_light(fdzb_ctx *ctx, const fdzb_area_light_desc *light);
 int fdzb_ctx_move_model(fdzb_ctx *ctx, const float m[16]);
+/* Shadow method (the reference chooses at compile time, REF_CAL in
+ * K/FourD.h:17, FS/api.cpp:545-552).
+ *   FDZB_SHADOW_EDGE_MASKS (default): the 4D-Z-buffer edge-function row masks
+ *     (K/Step5_2_shadowCalPerSample.inl);
+ *   FDZB_SHADOW_RAY_CAST: the reference's ray-cast cross-check (refCal_kernel,
+ *     K/Step5_2_calRef.inl): one ray per light sample through each triangle of
+ *     the sample's bin.  Same bins and lists; masks in this library's layout
+ *     (the reference numbers light samples transposed).  Much slower; meant to
+ *     cross-check the edge-function result, which it matches except for light
+ *     samples on or next to a projected triangle edge. */
+#define FDZB_SHADOW_EDGE_MASKS 0
+#define FDZB_SHADOW_RAY_CAST   1
+int fdzb_ctx_set_shadow_method(fdzb_ctx *ctx, int method);
+
+/* Model transform applied to model 0's vertices as they are read, leaving the
+ * vertex buffer untouched (the reference's moveModel rewrites the VBO in place,
+ * K/moveModel.inl:14-50).  m: column-major 4x4, NULL = none.  A launch with m
+ * gives bit for bit what fdzb_ctx_move_model(ctx, m) followed by a launch
+ * gives on the untransformed buffer; unlike moveModel it does not accumulate,
+ * so an animated scene passes each frame's full transform.  No host sync. */
+int fdzb_ctx_set_model_transform(fdzb_ctx *ctx, const float m[16]);
 /* Synchronous frame (FDLaunch form); *ms_out (nullable) gets the GPU time. */
 int fdzb_ctx_launch(fdzb_ctx *ctx, float *ms_out);
 /* Enqueue the frame on the context stream without waiting.  Pair-buffer overflow
@@ -240,6 +261,36 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second);
 int fdzb_light_setup(const fdzb_area_light_desc *light, float mat[16], float rect_factor[2],
                      float corners[12], float deltas[6]);
 
+/* Light-sample positions (host): out[3*(i*W + j) ..] = upRight + x_delt*j +
+ * y_delt*i for i < lightResHeight, j < lightResWidth, in the reference's own
+ * numbering (FS/api.cpp:351-357, the positions its REF_CAL check and the app's
+ * shading use).  out: 3 * W * H floats. */
+int fdzb_light_sample_positions(const fdzb_area_light_desc *light, float *out);
+
+/* ---- shading pass --------------------------------------------------------- */
+
+/* Deferred Phong shading of the shadowed frame, the app's consumer of the
+ * shadow buffer (4DZB/Resources/shader/phoneShading.shf:25-60): per pixel,
+ * the average over the light samples of La*ka + (Ld*kd*max(L.N, 0) +
+ * Ls*ks*max(R.V, 0)^shininess) * (1 - shadow), alpha 1.  G-buffer packing as the
+ * reference's: g0 = position.xyz | ks.r, g1 = normal.xyz | ks.g, g2 = ka.rgb |
+ * ks.b, g3 = kd.rgb | shininess (float4[W*H] each, 16-byte aligned).  Pixels
+ * whose shadow is NaN are left untouched (the shader discards them).  FP32 with
+ * CUDA's math functions; no bit-exact claim against a GLSL driver.  The app
+ * itself shades with one light sample (Render.cpp:461-470, 550). */
+typedef struct fdzb_shade_desc {
+    int32_t W, H;
+    const float *d_g0, *d_g1, *d_g2, *d_g3;
+    const float *d_shadow;         /* float[W*H] */
+    float *d_rgba;                 /* float4[W*H] */
+    float camera_pos[3];
+    float La[3], Ld[3], Ls[3];
+    int32_t n_light_samples;       /* 1..4096 */
+    const float *d_light_samples;  /* device float[3 * n_light_samples] world positions */
+} fdzb_shade_desc;
+/* Enqueued on `stream` (cudaStream_t, NULL = legacy default); no host sync. */
+int fdzb_shade(const fdzb_shade_desc *desc, void *stream);
+
 /* Library version string. */
 const char *fdzb_version(void);
 
@@ -274,6 +325,7 @@ typedef struct fdzb_frame_desc {
     float esp;                     /* FDsetScenesEsp */
     float *d_shadow;               /* float[W*H] at y*W+x */
     uint32_t *d_masks;             /* nullable: uint32[W*H*ceil(N*N/32)], bit i*N+j */
+    const float *model_transform;  /* nullable host pointer: 16 floats, see fdzb_ctx_set_model_transform */
 } fdzb_frame_desc;
 
 typedef struct fdzb_batch fdzb_batch;
@@ -357,6 +409,8 @@ typedef struct fdzb_request {
     int32_t pad0;
     float *d_shadow;               /* float[W*H] */
     uint32_t *d_masks;             /* nullable */
+    const float *model_transform;  /* nullable host pointer: 16 floats applied to the scene's vertices
+                                      for this request only (copied at submission) */
 } fdzb_request;
 
 typedef struct fdzb_request_result {

@@ -221,6 +221,43 @@ typedef struct {
     float esp;
 } pair_ctx;
 
+/* Ray-cast check of one sample/triangle pair (K/Step5_2_calRef.inl:1-126): for
+ * every light sample not yet set, the ray from Q to the light sample (placed at
+ * upRight + x_delt*j + y_delt*i, FS/api.cpp:351-357) against the triangle with
+ * intersect_triangle_branchless (1e-3 < t < dist, barycentric test).  Light
+ * sample (i along the height, j along the width) is stored at row j, column i,
+ * the edge-function masks' layout.  The caller applies the pre-cull. */
+static inline void raycast_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint32_t *mask, uint32_t *full_rows)
+{
+    const int N = c->N;
+    v3 p0 = ld3(t->v0), p1 = ld3(t->v1), p2 = ld3(t->v2);
+    v3 e0 = sub3(p1, p0), e1 = sub3(p0, p2);
+    v3 n = cross3(e1, e0);
+    v3 q0 = sub3(p0, Q);
+    v3 ur = ld3(c->ur), xd = ld3(c->xd), yd = ld3(c->yd);
+    const float tmin = 1e-3f;
+    for (int r = 0; r < N; ++r) {
+        if (mask[r] == c->full) continue;
+        v3 lr = add3(ur, mul3(xd, (float)r));
+        uint32_t add = 0;
+        for (int col = 0; col < N; ++col) {
+            if (mask[r] & (1u << col)) continue;
+            v3 lp = add3(lr, mul3(yd, (float)col));
+            v3 L = sub3(lp, Q);
+            float dist = sqrtf(dot3(L, L));
+            v3 dir = mk3(L.x / dist, L.y / dist, L.z / dist);
+            float inv = 1.0f / dot3(n, dir);
+            v3 e2 = mul3(q0, inv);
+            v3 iv = cross3(dir, e2);
+            float beta = dot3(iv, e1), gamma = dot3(iv, e0), tt = dot3(n, e2);
+            if ((tt < dist) & (tt > tmin) & (beta >= 0.0f) & (gamma >= 0.0f) & (beta + gamma <= 1.0f))
+                add |= 1u << col;
+        }
+        mask[r] |= add;
+        if (mask[r] == c->full) *full_rows |= 1u << r;
+    }
+}
+
 /* One sample/triangle pair: K/Step5_2_shadowCalPerSample.inl:129-222.  `mask` holds
  * N rows, `full_rows` the rows already equal to FULL.  Returns 1 if the pair was
  * evaluated past the self-intersection skip.  Counters track reference quirks. */
@@ -658,6 +695,16 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
             int high = 0;
             for (int p = tstart[bin]; p < tend[bin] && full_rows != c.full; ++p) {
                 const tri_rec *t = &rec[sptri[p]];
+                if (in->shadow_method == 1) {
+                    /* refCal's pre-cull: rectangle containment, and the depth test
+                     * with a double literal (K/Step5_2_calRef.inl:98-102) */
+                    if (!(spz <= t->bmax[0] && spw <= t->bmax[1] && spx >= t->bmin[0] && spy >= t->bmin[1]))
+                        continue;
+                    if ((double)t->minz - 1e-3 > (double)spZ) continue;
+                    ++tested;
+                    raycast_test(&c, Q, t, rows, &full_rows);
+                    continue;
+                }
                 if (!(t->bmin[0] <= spx && t->bmin[1] <= spy && spz <= t->bmax[0] &&
                       spw <= t->bmax[1] && t->minz <= spZ))
                     continue;

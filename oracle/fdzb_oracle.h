@@ -66,6 +66,8 @@ typedef struct {
                                     (<= 1: all); others keep mask 0 / shadow 0 */
     int32_t setup_only;          /* 1: stop after the light plane (A1-A5); enough for the
                                     exhaustive baselines, which rebuild their triangle list */
+    int32_t shadow_method;       /* 0: edge-function row masks (K/Step5_2_shadowCalPerSample.inl);
+                                    1: the reference's ray-cast check (K/Step5_2_calRef.inl) */
 } orc_frame_in;
 
 typedef struct {

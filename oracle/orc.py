@@ -40,7 +40,8 @@ class FrameIn(ctypes.Structure):
                 ("vtx", f32p), ("vtx_stride_floats", ctypes.c_int32), ("V", ctypes.c_int32),
                 ("idx", i32p), ("T", ctypes.c_int32), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
                 ("esp", ctypes.c_float), ("light", ctypes.POINTER(Light)), ("nthreads", ctypes.c_int32),
-                ("occ_stride", ctypes.c_int32), ("setup_only", ctypes.c_int32)]
+                ("occ_stride", ctypes.c_int32), ("setup_only", ctypes.c_int32),
+                ("shadow_method", ctypes.c_int32)]
 
 
 class FrameOut(ctypes.Structure):
@@ -153,7 +154,7 @@ def _frame_in(scene, light: Light, nthreads: int, keep: list, occ_stride: int = 
 
 
 def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride: int = 1,
-          setup_only: bool = False) -> OrcFrame:
+          setup_only: bool = False, shadow_method: int = 0) -> OrcFrame:
     """Run the FP32 restatement (O2) on a scenes.Scene.  occ_stride > 1 runs the
     occlusion stage only for every occ_stride-th sorted valid sample;
     setup_only stops after the light plane (what the exhaustive baselines need)."""
@@ -161,6 +162,7 @@ def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride
     keep: list = []
     light = light_setup(scene.light)
     fi = _frame_in(scene, light, nthreads, keep, occ_stride)
+    fi.shadow_method = int(shadow_method)   # 1: the reference's ray-cast check
     if setup_only:
         # scalars only: every output array pointer stays NULL
         fi.setup_only = 1

@@ -112,6 +112,6 @@ def test_batch_struct_layouts(fdzb):
     import ctypes
     assert ctypes.sizeof(fdzb.AreaLightDesc) == 52
     assert ctypes.sizeof(fdzb.FrameStats) == 184
-    assert ctypes.sizeof(fdzb.FrameDesc) == 144
+    assert ctypes.sizeof(fdzb.FrameDesc) == 152
     assert ctypes.sizeof(fdzb.BatchStats) == 232
     assert fdzb.FrameDesc.light.offset == 64 and fdzb.FrameDesc.d_shadow.offset == 128
