@@ -188,7 +188,9 @@ def reference_arm(args, scene) -> dict:
     bins.  Warm-up times one full frame; each timed step runs the central crop
     holding 1/16 of the samples (and every triangle), and the full-frame time is
     the calibrated full frame scaled by the crop's drift.  Without oracle/_ref
-    the oracle's FP32 port of the binned pipeline stands in (kind "port")."""
+    the oracle's FP32 port of the binned pipeline stands in (kind "port").
+    The line also carries `reference_gpu`: the same sources built for sm_100a
+    and timed on this box's GPU."""
     threads = os.cpu_count() or 1
     from oracle import ref
     if ref.available():
@@ -227,6 +229,7 @@ def reference_arm(args, scene) -> dict:
                   f"{stride}th binned sample, extrapolated")
     ms = 1e3 * statistics.mean(times)
     v = 1e3 / ms
+    gpu = reference_gpu(args, scene)
     return {"metric": "shadow frames/s", "value": v, "unit": "frames/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -234,7 +237,37 @@ def reference_arm(args, scene) -> dict:
             "config": {"workload": args.config, "W": scene.W, "H": scene.H, "triangles": scene.T,
                        "light_grid": scene.light.n, "bins": scene.bins},
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": kind, "sample": sample},
-            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": gpu}
+
+
+def reference_gpu(args, scene) -> dict:
+    """The reference's own CUDA sources (FS/api.cpp + K/*.inl) built for sm_100a
+    with nvcc's defaults (oracle/_ref/libref4dzb_gpu_fmad.so), run on this
+    process's GPU through FDLaunch on the same scene: W untimed and K timed
+    frames, each timed with CUDA events around FDLaunch after an L2 flush.  Its
+    bins are the compile-time 16 x 16.  The scene passes the CPU preflight first
+    (keys inside the bin grid, pairs inside the reference's pair buffers)."""
+    from oracle import ref_gpu
+    if not ref_gpu.available(fmad=True):
+        return {"unavailable": "oracle/_ref/libref4dzb_gpu_fmad.so not built (needs the reference sources)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except ImportError:
+        return {"unavailable": "torch missing"}
+    try:
+        ref_gpu.preflight(scene, occ_stride=256)
+    except ref_gpu.PreflightError as e:
+        return {"unavailable": f"preflight refused the scene: {e}"}
+    r = ref_gpu.run(scene, fmad=True, warmup=args.warmup, reps=args.steps, checked=True)
+    t = [float(x) for x in r["launch_ms"]]
+    ms = statistics.mean(t)
+    return {"value": 1e3 / ms, "unit": "frames/s", "ms_per_frame": ms, "min_ms": min(t), "max_ms": max(t),
+            "frames": len(t), "bins": ref_gpu.REF_BINS, "num_pairs": int(r["num_pairs"]),
+            "build": "reference sources, nvcc 12.9 -O3 sm_100a, default --fmad=true",
+            "timing": "CUDA events around each FDLaunch; 256 MB L2 flush before each"}
 
 
 def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> dict:

@@ -1,0 +1,141 @@
+"""ctypes wrapper of oracle/_ref/libref4dzb_gpu*.so -- the reference's own
+soft-shadow sources (4DZB/FDZB_Soft_Shadow) compiled for sm_100a by
+oracle/ref_gpu/build_ref_gpu.py.  TEST INFRASTRUCTURE ONLY: it pins the product
+against the reference running on the same GPU, and times the reference's GPU
+frame.  Its bin grid is the reference's compile-time 16 x 16 (FS/constants.h:13).
+
+Every input is checked on the CPU first (preflight): the oracle, run with the
+same 16 x 16 bins and the reference's triangle order, must show that every
+sample key stays inside the bin grid and that the triangle/bin pairs fit the
+reference's fixed pair buffers (FS/constants.h:15, FS/api.cpp:132-138); the
+light must be square with N <= 32 (the only form the per-sample kernel runs,
+K/Step5_2_shadowCalPerSample.inl:249-254).  An input that fails is refused
+before anything reaches the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_EXACT = os.path.join(HERE, "_ref", "libref4dzb_gpu.so")
+LIB_FMAD = os.path.join(HERE, "_ref", "libref4dzb_gpu_fmad.so")
+REF_BINS = 16
+# FD_MAX_BT_PIAR_Num * 1.4 (FS/constants.h:15, FS/api.cpp:132-138)
+PAIR_BUFFER = int(50 * 1024 * 1024 * 1.4)
+
+f32p = ctypes.POINTER(ctypes.c_float)
+i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+class RefGpuIn(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_int32), ("H", ctypes.c_int32), ("pos", f32p), ("nrm", f32p), ("vtx", f32p),
+                ("V", ctypes.c_int32), ("vstride_bytes", ctypes.c_int32), ("idx", i32p), ("T", ctypes.c_int32),
+                ("cull", ctypes.c_int32), ("esp", ctypes.c_float), ("rightRadius", ctypes.c_float),
+                ("topRadius", ctypes.c_float), ("position", ctypes.c_float * 3), ("viewDir", ctypes.c_float * 3),
+                ("upDir", ctypes.c_float * 3), ("lightRes", ctypes.c_int32), ("warmup", ctypes.c_int32),
+                ("reps", ctypes.c_int32)]
+
+
+class RefGpuOut(ctypes.Structure):
+    _fields_ = [("shadow", f32p), ("launch_ms", f32p), ("fdlaunch_ms", f32p), ("num_bins", ctypes.c_int32),
+                ("valid_samples", ctypes.c_int32), ("valid_tris", ctypes.c_int32), ("num_pairs", ctypes.c_int32),
+                ("view_log2up", ctypes.c_int32), ("errors", ctypes.c_int32), ("rows_beyond_n", ctypes.c_int64),
+                ("sub", ctypes.c_float * 2), ("lp_begin", ctypes.c_float * 3), ("lp_end", ctypes.c_float * 3),
+                ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 8),
+                ("model_aabb", ctypes.c_float * 8), ("first_error", ctypes.c_char * 160),
+                ("surf_handle", ctypes.c_int64), ("pos_tex_handle", ctypes.c_int64), ("view_error", ctypes.c_int64)]
+
+
+_libs: dict = {}
+
+
+def lib_path(fmad: bool) -> str:
+    return LIB_FMAD if fmad else LIB_EXACT
+
+
+def available(fmad: bool = False) -> bool:
+    return os.path.exists(lib_path(fmad))
+
+
+def load(fmad: bool = False) -> ctypes.CDLL:
+    if fmad not in _libs:
+        lib = ctypes.CDLL(lib_path(fmad), mode=ctypes.RTLD_LOCAL)
+        lib.ref_gpu_frame.argtypes = [ctypes.POINTER(RefGpuIn), ctypes.POINTER(RefGpuOut)]
+        lib.ref_gpu_frame.restype = ctypes.c_int
+        _libs[fmad] = lib
+    return _libs[fmad]
+
+
+class PreflightError(RuntimeError):
+    pass
+
+
+def preflight(scene, occ_stride: int = 64) -> dict:
+    """Check on the CPU, with the oracle at the reference's 16 x 16 bins, that a
+    scene stays inside the reference's buffers.  occ_stride thins the oracle's
+    occlusion stage (the checked quantities come from the binning stages)."""
+    import dataclasses
+
+    from . import orc
+
+    n = scene.light.n
+    if not (1 < n <= 32):
+        raise PreflightError(f"light grid {n} x {n}: the per-sample kernel runs 2..32 square grids only")
+    s16 = dataclasses.replace(scene, bins=REF_BINS)
+    fr = orc.frame(s16, occ_stride=occ_stride)
+    sc = fr.scalars
+    if sc["quirk_key_range"]:
+        raise PreflightError(f"{sc['quirk_key_range']} sample keys outside the {REF_BINS} x {REF_BINS} grid")
+    if sc["num_pairs"] + REF_BINS * REF_BINS > PAIR_BUFFER:
+        raise PreflightError(f"{sc['num_pairs']} triangle/bin pairs exceed the reference's pair buffer")
+    return sc
+
+
+def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool = False) -> dict:
+    """Frames through the reference on the current GPU (device 0 of this process).
+    The shadow buffer of the last launch is returned at y*W+x; launch_ms holds
+    the CUDA-event time of each timed FDLaunch (L2 flushed before each)."""
+    if not checked:
+        preflight(scene)
+    lib = load(fmad)
+    pos = np.ascontiguousarray(scene.pos, np.float32)
+    nrm = np.ascontiguousarray(scene.nrm, np.float32)
+    vtx = np.ascontiguousarray(scene.vtx, np.float32)
+    idx = np.ascontiguousarray(scene.idx, np.int32)
+    reps = max(int(reps), 1)
+    shadow = np.zeros(scene.S, np.float32)
+    launch_ms = np.zeros(reps, np.float32)
+    own_ms = np.zeros(reps, np.float32)
+    ri = RefGpuIn()
+    ri.W, ri.H = scene.W, scene.H
+    ri.pos, ri.nrm = pos.ctypes.data_as(f32p), nrm.ctypes.data_as(f32p)
+    ri.vtx = vtx.ctypes.data_as(f32p)
+    ri.V, ri.vstride_bytes = vtx.shape[0], vtx.shape[1] * 4
+    ri.idx, ri.T = idx.ctypes.data_as(i32p), scene.T
+    ri.cull, ri.esp = int(bool(scene.cull)), scene.esp
+    L = scene.light
+    ri.rightRadius, ri.topRadius = L.right_radius, L.top_radius
+    ri.position[:] = list(L.position)
+    ri.viewDir[:] = list(L.view_dir)
+    ri.upDir[:] = list(L.up_dir)
+    ri.lightRes = L.n
+    ri.warmup, ri.reps = int(warmup), reps
+    ro = RefGpuOut()
+    ro.shadow = shadow.ctypes.data_as(f32p)
+    ro.launch_ms = launch_ms.ctypes.data_as(f32p)
+    ro.fdlaunch_ms = own_ms.ctypes.data_as(f32p)
+    rc = lib.ref_gpu_frame(ctypes.byref(ri), ctypes.byref(ro))
+    out = {"shadow": shadow, "launch_ms": launch_ms, "fdlaunch_ms": own_ms, "rc": rc,
+           "first_error": ro.first_error.decode(errors="replace")}
+    for name, _ in RefGpuOut._fields_:
+        v = getattr(ro, name)
+        if isinstance(v, (int, float)):
+            out[name] = v
+        elif hasattr(v, "_length_") and not hasattr(v, "contents") and name != "first_error":
+            out[name] = np.array(list(v), np.float32)
+    if rc:
+        raise RuntimeError(f"reference GPU frame failed: {out['errors']} CUDA errors, first: {out['first_error']}")
+    return out

@@ -1,0 +1,161 @@
+#!/usr/bin/env python3
+"""Build recipe of the reference GPU harness: 4DZB's own soft-shadow sources,
+compiled for sm_100a into oracle/_ref/ (test infrastructure).
+
+Two libraries, same sources:
+
+* libref4dzb_gpu.so      -- --fmad=false: every float expression is the IEEE
+  sequence of operations the source spells, so its shadows can be compared
+  bit for bit with the oracle and with libfdzb.so;
+* libref4dzb_gpu_fmad.so -- nvcc's default --fmad=true, as the reference's own
+  project builds it: the timing build.
+
+Reads the reference where it lies (default /root/reference, or $FDZB_REFERENCE)
+and writes only into oracle/_ref/.  Nothing from the reference is copied into
+the repository:
+
+* FS/api.cpp (with nvcc, like the kernels: it shares glm types by value with
+  them), FS/util/cudaBuffer.cpp, FS/util/channel.cpp and
+  FS/util/layeredSurface.cpp (with g++) compile unmodified against the shim headers in
+  oracle/ref_gpu/shim (then oracle/ref_emu/shim: GL scalar types, header-name
+  case), with oracle/ref_gpu/refgpu.h force-included (the CUDA-GL interop calls
+  renamed to the harness registry of gl_runtime.cpp; there is no graphics stack);
+* the kernel files K/*.inl are concatenated, in the order of K/FourD.cu:230-257,
+  between harness_pre.cuh and harness_post.cuh into a temporary .cu under
+  oracle/_ref/ that is deleted after compiling.  The concatenation changes
+  three things only, each checked to apply exactly once:
+    - the nested includes of Step2_3 (already concatenated) are dropped and the
+      backslash include path of moveModel.inl is normalised;
+    - the unguarded per-frame pair dump `showBinTriPair(pairNum);`
+      (K/Step4_RasterizeTriangleToBin.inl:218, a full device-to-host copy and
+      an fprintf per pair into a Windows path) is removed from bindTriToBin;
+    - in the per-sample kernel's row loop
+      (K/Step5_2_shadowCalPerSample.inl:204-222) a row index >= N is counted
+      and skipped instead of indexing past the sample's N rows of shared
+      memory (inverted partial row filters can keep bits >= N set).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE = os.path.dirname(HERE)
+OUT_DIR = os.path.join(ORACLE, "_ref")
+LIB_EXACT = os.path.join(OUT_DIR, "libref4dzb_gpu.so")
+LIB_FMAD = os.path.join(OUT_DIR, "libref4dzb_gpu_fmad.so")
+REF = os.environ.get("FDZB_REFERENCE", "/root/reference")
+FS = os.path.join(REF, "4DZB", "FDZB_Soft_Shadow")
+K = os.path.join(FS, "cuda")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+INL_ORDER = ["FDprojection.inl", "blockAABBReduce.inl", "binRaster.inl", "Step0_triangleSetup.inl",
+             "Step2_1_samplerRectangleAABB.inl", "Step2_2_modelRectangleAABB.inl",
+             "Step2_3_defineFDbuffer.inl", "Step3_bindSampleToBin.inl",
+             "Step4_RasterizeTriangleToBin.inl", "Step5_1_prepareBin.inl", "Step5_2_shadowCal.inl",
+             "Step5_2_calRef.inl", "Step5_2_shadowCalPerSample.inl", "moveModel.inl"]
+HOST_SOURCES = [os.path.join(FS, "api.cpp"), os.path.join(FS, "util", "cudaBuffer.cpp"),
+                os.path.join(FS, "util", "channel.cpp"), os.path.join(FS, "util", "layeredSurface.cpp")]
+
+# (file, exact stripped line, replacement) -- each must match exactly once
+EDITS = [
+    ("Step4_RasterizeTriangleToBin.inl", "showBinTriPair(pairNum);",
+     "/* per-frame pair dump removed by the harness */"),
+    ("Step5_2_shadowCalPerSample.inl", "mask[rowID*32] |= M0 & M1 & M2;",
+     "REFGPU_ROW_GUARD(rowID, lightResHeight) mask[rowID*32] |= M0 & M1 & M2;"),
+]
+
+
+def _read(path: str) -> str:
+    raw = open(path, "rb").read()
+    try:
+        return raw.decode("gbk")
+    except UnicodeDecodeError:
+        return raw.decode("latin-1")
+
+
+def kernel_source() -> str:
+    parts = ['#include "harness_pre.cuh"\n']
+    hits = {i: 0 for i in range(len(EDITS))}
+    for name in INL_ORDER:
+        text = _read(os.path.join(K, name))
+        out = [f'#line 1 "{name}"']
+        for line in text.splitlines():
+            s = line
+            stripped = s.strip()
+            if name == "Step2_3_defineFDbuffer.inl" and stripped.startswith('#include "Step2_'):
+                s = "// (concatenated above)"
+            s = s.replace("#include <glm\\glm.hpp>", "#include <glm/glm.hpp>")
+            for i, (fname, old, new) in enumerate(EDITS):
+                if name == fname and stripped == old:
+                    s = s.replace(old, new)
+                    hits[i] += 1
+            out.append(s)
+        parts.append("\n".join(out) + "\n")
+    for i, n in hits.items():
+        if n != 1:
+            raise RuntimeError(f"harness edit {EDITS[i][:2]} matched {n} times (expected 1)")
+    parts.append('#include "harness_post.cuh"\n')
+    return "".join(parts)
+
+
+def build(verbose: bool = False) -> list[str]:
+    if not os.path.isdir(K):
+        raise FileNotFoundError(f"reference sources not found under {REF}")
+    os.makedirs(OUT_DIR, exist_ok=True)
+    inc = ["-I", os.path.join(HERE, "shim"), "-I", os.path.join(ORACLE, "ref_emu", "shim"), "-I", HERE,
+           "-I", K, "-I", os.path.join(FS, "util"), "-I", FS, "-I", os.path.join(REF, "4DZB")]
+    defs = ["-DGLM_FORCE_PURE"]
+    host_flags = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-w"]
+    env = dict(os.environ)
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+        if verbose or r.returncode:
+            sys.stderr.write(r.stdout + r.stderr[-20000:])
+        if r.returncode:
+            raise RuntimeError(f"reference GPU harness build failed: {' '.join(cmd[:4])} ...")
+
+    force = ["-include", os.path.join(HERE, "refgpu.h")]
+    host_objs = []
+    for src in HOST_SOURCES + [os.path.join(HERE, "gl_runtime.cpp")]:
+        o = os.path.join(OUT_DIR, "gpu_" + os.path.splitext(os.path.basename(src))[0] + ".o")
+        if os.path.basename(src) == "api.cpp":
+            # FS/api.cpp takes AreaLightDes (three glm::vec3) by value from the
+            # kernel translation unit; GLM declares its own copy constructor
+            # under nvcc only, which changes how the struct is passed.  Both
+            # sides are compiled by nvcc so that they agree.
+            run([NVCC, *ARCH, "-std=c++17", "-O3", "-x", "cu", "-Xcompiler", ",".join(host_flags), "-w",
+                 "--expt-relaxed-constexpr", *defs, *inc, *force, "-c", src, "-o", o])
+        else:
+            run(["g++", "-std=c++17", *host_flags, *defs, *inc, "-I", "/usr/local/cuda/include", *force,
+                 "-c", src, "-o", o])
+        host_objs.append(o)
+    cu = os.path.join(OUT_DIR, "ref_gpu_kernels.cu")
+    with open(cu, "w") as f:
+        f.write(kernel_source())
+    libs = []
+    try:
+        for lib, fmad in ((LIB_EXACT, "false"), (LIB_FMAD, "true")):
+            o = os.path.join(OUT_DIR, f"gpu_kernels_fmad_{fmad}.o")
+            run([NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", f"--fmad={fmad}", "-Xcompiler",
+                 ",".join(host_flags), "-w", "--expt-relaxed-constexpr", *defs, *inc, *force, "-c", cu, "-o", o])
+            run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib + ".tmp", o, *host_objs,
+                 "-Xlinker", "-Bsymbolic"])
+            os.replace(lib + ".tmp", lib)
+            os.remove(o)
+            libs.append(lib)
+    finally:
+        if os.path.exists(cu):
+            os.remove(cu)
+        for o in host_objs:
+            if os.path.exists(o):
+                os.remove(o)
+    return libs
+
+
+if __name__ == "__main__":
+    for p in build(verbose="-v" in sys.argv):
+        print(p)

@@ -1,0 +1,63 @@
+// harness_pre.cuh -- first part of the reference GPU harness translation unit
+// (test infrastructure).  Declares what K/FourD.cu defines, in that file's
+// roles, since FourD.cu itself does not compile with CUDA 12 (its legacy
+// texture references, K/FourD.cu:36-37, were removed): the __constant__
+// parameter blocks and the device atomics (K/FourD.cu:26-33), and the two
+// sample textures as texture OBJECTS behind the same names, read through a
+// tex2D overload with the reference's sampling (point filter, unnormalized
+// coordinates; K/FourD.cu:167-181).  The kernel files K/*.inl follow this file
+// in the order of K/FourD.cu:230-257.
+#pragma once
+#include <string>
+#include <thrust/device_ptr.h>
+#include <thrust/reduce.h>
+#include <thrust/sort.h>
+
+#include "FourD.h"
+#include "../constants.h"
+
+// file dumps of the debug paths go to /dev/null (gl_runtime.cpp)
+FILE *refgpu_fopen(const char *name, const char *mode);
+#define fopen refgpu_fopen
+
+// SaveBMP1 / BYTE of 4DZB/Util/SaveBMP.h (Windows-only), used by a debug dump
+typedef unsigned char BYTE;
+inline void SaveBMP1(const char *, BYTE *, int, int) {}
+
+// Pre-Volta warp intrinsics of K/Step5_2_shadowCal.inl (the per-bin kernel,
+// compiled but not launched by FDLaunch): their full-warp _sync forms.
+#define __shfl_xor(v, m, w) __shfl_xor_sync(0xffffffffu, (v), (m), (w))
+#define __any(p) __any_sync(0xffffffffu, (p))
+#define __all(p) __all_sync(0xffffffffu, (p))
+#define __ballot(p) __ballot_sync(0xffffffffu, (p))
+
+// K/FourD.cu:17-20
+__inline__ __host__ __device__ float2 make_float2(float4 a) { return make_float2(a.x, a.y); }
+
+// globals of K/FourD.cu the kernel files use without a declaration in FourD.h
+extern int m_validBinNum;
+extern void *g_fdAtomics_addr;
+
+// device-side globals of K/FourD.cu:26-37
+__constant__ FDStaticParams c_fdStaticParams;
+__constant__ FDLightPlaneParams c_fdLightPlaneParams;
+__constant__ float2 c_fdRectangleSubConstant;
+__device__ FDAtomics g_fdAtomics;
+__constant__ float3 c_REF_CAL_lightPos[32 * 32];
+
+struct RefGpuTex2D {
+    cudaTextureObject_t tex;
+};
+__constant__ RefGpuTex2D samplePositionTex;
+__constant__ RefGpuTex2D sampleNormalTex;
+__device__ __forceinline__ float4 tex2D(const RefGpuTex2D &t, float x, float y) { return tex2D<float4>(t.tex, x, y); }
+
+// Harness counter: rows >= N that the per-sample kernel's row loop would index
+// (reference quirk: inverted partial row filters keep bits >= N; the build
+// skips such rows instead of writing past the sample's N rows of shared memory).
+__device__ unsigned long long refgpu_rows_beyond_n;
+#define REFGPU_ROW_GUARD(row, rows)                       \
+    if ((row) >= (rows)) {                                \
+        atomicAdd(&refgpu_rows_beyond_n, 1ull);           \
+        continue;                                         \
+    }
