@@ -58,6 +58,7 @@ EXPORTED = [
     "fdzb_batch_get_stats", "fdzb_batch_frame_bins", "fdzb_batch_autotune",
     "fdzb_ctx_set_occlusion_schedule", "fdzb_batch_set_occlusion_schedule", "fdzb_ctx_set_pair_capacity_limit",
     "fdzb_ctx_set_model_transform", "fdzb_ctx_set_shadow_method", "fdzb_light_sample_positions", "fdzb_shade",
+    "fdzb_ctx_set_depth_plane", "fdzb_batch_set_depth_plane",
     "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
@@ -98,7 +99,7 @@ class AreaLightDesc(ctypes.Structure):
         d.viewDir[:] = list(light.view_dir)
         d.upDir[:] = list(light.up_dir)
         d.lightResWidth = light.n
-        d.lightResHeight = light.n
+        d.lightResHeight = light.nh if getattr(light, "nh", 0) else light.n
         return d
 
 
@@ -238,6 +239,7 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32),
         "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
         "fdzb_ctx_set_shadow_method": ([vp, i32], i32),
+        "fdzb_ctx_set_depth_plane": ([vp, i32], i32), "fdzb_batch_set_depth_plane": ([vp, i32], i32),
         "fdzb_light_sample_positions": ([P(AreaLightDesc), P(ctypes.c_float)], i32),
         "fdzb_shade": ([P(ShadeDesc), vp], i32), "fdzb_batch_set_occlusion_schedule": ([vp, i32], i32),
         "fdzb_batch_create": ([P(vp), i32], i32), "fdzb_batch_destroy": ([vp], i32),
@@ -305,8 +307,10 @@ def measure_alu_rate() -> float:
     return float(v.value)
 
 
-def mask_words(n: int) -> int:
-    return (n * n + 31) // 32
+def mask_words(n: int, cols: Optional[int] = None) -> int:
+    """uint32 words of one sample's mask for an n x cols light grid (cols
+    defaults to n)."""
+    return (n * (cols if cols else n) + 31) // 32
 
 
 class Context:
@@ -392,6 +396,10 @@ class Context:
     def move_model(self, m) -> None:
         arr = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)])
         _check(self._lib.fdzb_ctx_move_model(self._h, arr))
+
+    def set_depth_plane(self, enable: bool) -> None:
+        """fdzb_ctx_set_depth_plane: also test each triangle's own plane."""
+        _check(self._lib.fdzb_ctx_set_depth_plane(self._h, int(bool(enable))))
 
     def set_shadow_method(self, method: int) -> None:
         """SHADOW_EDGE_MASKS (default) or SHADOW_RAY_CAST (the reference's REF_CAL checker)."""
@@ -528,7 +536,8 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
     import torch
     pos, nrm, vtx, idx = upload_scene(scene, device)
     shadow = torch.empty(scene.S, dtype=torch.float32, device=device)
-    mk = torch.empty(scene.S * mask_words(scene.light.n), dtype=torch.int32, device=device) if masks else None
+    mk = (torch.empty(scene.S * mask_words(scene.light.n, scene.light.cols), dtype=torch.int32, device=device)
+          if masks else None)
     ctx = Context()
     if debug:
         ctx.set_debug(1)
@@ -542,6 +551,8 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
     ctx.set_sample_buffers(pos, nrm)
     ctx.set_output_buffer(shadow, mk)
     ctx.set_area_light(scene.light)
+    if getattr(scene, "depth_plane", False):
+        ctx.set_depth_plane(True)
     return ctx, dict(pos=pos, nrm=nrm, vtx=vtx, idx=idx, shadow=shadow, masks=mk)
 
 
@@ -608,6 +619,9 @@ class Batch:
 
     def set_occlusion_schedule(self, schedule: int) -> None:
         _check(self._lib.fdzb_batch_set_occlusion_schedule(self._h, int(schedule)))
+
+    def set_depth_plane(self, enable: bool) -> None:
+        _check(self._lib.fdzb_batch_set_depth_plane(self._h, int(bool(enable))))
 
     def set_stream(self, stream) -> None:
         _check(self._lib.fdzb_batch_set_stream(self._h, ctypes.c_void_p(stream)))

@@ -256,7 +256,8 @@ int check_frame(const FrameSpec &f, int i)
     if (f.nt > 0x3fffffffull || f.nv > 0x3fffffffull) return fail(FDZB_ERR_INVALID_ARG, at + "model too large");
     if (f.bins < 1 || f.bins > fdzb::kMaxBins || (f.bins & (f.bins - 1)))
         return fail(FDZB_ERR_INVALID_ARG, at + "bin number must be a power of two in [1, 512]");
-    if (f.light.N < 1 || f.light.N > fdzb::kMaxLightN) return fail(FDZB_ERR_UNSUPPORTED, at + "light grid N out of [1, 32]");
+    if (f.light.N < 1 || f.light.N > fdzb::kMaxLightN || f.light.NC < 1 || f.light.NC > fdzb::kMaxLightN)
+        return fail(FDZB_ERR_UNSUPPORTED, at + "light grid width and height must be in [1, 64]");
     return FDZB_OK;
 }
 
@@ -307,8 +308,18 @@ int engine_enqueue(Engine &e)
     e.maxV = maxV;
     fdzb::DeviceBuffers &b = e.buf;
     b.samplePasses = fdzb::sort_passes_for(NB + 1);
-    b.occVariant = e.occVariant;
+    // 64-bit row words when some frame's grid exceeds 32 rows or columns; the
+    // lane-per-pair schedule covers square 32-bit grids without the depth
+    // plane, other launches use lane per sample
+    bool wide = false, square = true;
+    for (const FrameSpec &f : e.frames) {
+        wide = wide || f.light.N > fdzb::kMaxLightN32 || f.light.NC > fdzb::kMaxLightN32;
+        square = square && f.light.N == f.light.NC;
+    }
+    b.wide = wide ? 1 : 0;
+    b.depthPlane = e.depthPlane;
     b.rayCast = e.rayCast;
+    b.occVariant = (e.occVariant == 1 && !wide && square && !e.depthPlane) ? 1 : 0;
     // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
     // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
     // order appends a depth bucket below the bin so each bin lists its lowest
@@ -346,7 +357,7 @@ int engine_enqueue(Engine &e)
         f.numBins = s.bins * s.bins;
         f.cull = s.cull;
         f.esp = s.esp;
-        f.maskWords = (s.light.N * s.light.N + 31) / 32;
+        f.maskWords = (s.light.N * s.light.NC + 31) / 32;
         f.sampleBase = sb;
         f.triBase = tb;
         f.binBase = bb;
@@ -378,7 +389,7 @@ int engine_enqueue(Engine &e)
         k.maxV = maxV;
         k.arena = e.arena;
         k.hFrames = e.hFrames;
-        k.ov = e.occVariant + 16 * e.rayCast;
+        k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane;
         k.stream = e.stream;
         if (!e.graph || !(k == e.graphKey)) {
             drop_graph(e);
@@ -429,14 +440,14 @@ namespace {
 // same in every pass.
 decltype(Engine::passKey) pass_key(const Engine &e, const FrameSpec &f)
 {
-    return {f.pos, f.nrm, f.W, f.H, f.vtx, f.idx, f.nt, f.bins, f.light.N, e.maxPairCapacity};
+    return {f.pos, f.nrm, f.W, f.H, f.vtx, f.idx, f.nt, f.bins, f.light.N * 128 + f.light.NC, e.maxPairCapacity};
 }
 
 int run_triangle_passes(Engine &e, bool planned)
 {
     const FrameSpec full = e.frames[0];
     const size_t S = (size_t)full.W * full.H;
-    const size_t words = (size_t)(full.light.N * full.light.N + 31) / 32;
+    const size_t words = (size_t)(full.light.N * full.light.NC + 31) / 32;
     uint32_t *masks = full.masks;
     // after an overflowed launch, full.masks already holds a subset of the bits
     int acc = planned ? 0 : 1;
@@ -779,8 +790,9 @@ int fdzb::heuristic_bins(long long S)
 int fdzb::desc_to_spec(const fdzb_frame_desc &d, FrameSpec &f, int i)
 {
     const fdzb_area_light_desc &L = d.light;
-    if (L.lightResWidth != L.lightResHeight || L.lightResWidth < 1 || L.lightResWidth > fdzb::kMaxLightN)
-        return fail(FDZB_ERR_UNSUPPORTED, "frame " + std::to_string(i) + ": light grid must be square with N in [1, 32]");
+    if (L.lightResWidth < 1 || L.lightResWidth > fdzb::kMaxLightN || L.lightResHeight < 1 ||
+        L.lightResHeight > fdzb::kMaxLightN)
+        return fail(FDZB_ERR_UNSUPPORTED, "frame " + std::to_string(i) + ": light grid width and height must be in [1, 64]");
     f.pos = (const float4 *)d.d_pos;
     f.nrm = (const float4 *)d.d_nrm;
     f.W = d.W;
@@ -827,7 +839,7 @@ fdzb::TuneKey fdzb::tune_key(long long S, long long T, int N)
 int fdzb::tuned_bins(const TuneTable &table, const FrameSpec &f)
 {
     const long long S = (long long)f.W * f.H;
-    auto it = table.find(tune_key(S, (long long)f.nt, f.light.N));
+    auto it = table.find(tune_key(S, (long long)f.nt, f.light.N * 128 + f.light.NC));
     return it != table.end() ? it->second : heuristic_bins(S);
 }
 
@@ -842,7 +854,7 @@ int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec
     std::map<TuneKey, size_t> firstOf;
     for (size_t i = 0; i < frames.size(); ++i) {
         const FrameSpec &f = frames[i];
-        const TuneKey k = tune_key((long long)f.W * f.H, (long long)f.nt, f.light.N);
+        const TuneKey k = tune_key((long long)f.W * f.H, (long long)f.nt, f.light.N * 128 + f.light.NC);
         if (!table.count(k) && !firstOf.count(k)) firstOf[k] = i;
     }
     const bool savedGraph = e.useGraph;
@@ -1084,8 +1096,9 @@ int fdzb_ctx_set_area_light(fdzb_ctx *c, const fdzb_area_light_desc *d)
 {
     if (int rc = ctx_check(c)) return rc;
     if (!d) return fail(FDZB_ERR_INVALID_ARG, "light is NULL");
-    if (d->lightResWidth != d->lightResHeight || d->lightResWidth < 1 || d->lightResWidth > fdzb::kMaxLightN)
-        return fail(FDZB_ERR_UNSUPPORTED, "light grid must be square with N in [1, 32]");
+    if (d->lightResWidth < 1 || d->lightResWidth > fdzb::kMaxLightN || d->lightResHeight < 1 ||
+        d->lightResHeight > fdzb::kMaxLightN)
+        return fail(FDZB_ERR_UNSUPPORTED, "light grid width and height must be in [1, 64]");
     c->lightDesc = *d;
     fdzb::light_setup(d->rightRadius, d->topRadius, d->position, d->viewDir, d->upDir, d->lightResWidth,
                       d->lightResHeight, &c->light);
@@ -1100,6 +1113,14 @@ int fdzb_ctx_set_shadow_method(fdzb_ctx *c, int method)
         return fail(FDZB_ERR_INVALID_ARG, "unknown shadow method");
     if (int rc = ctx_sync(c)) return rc;
     c->eng.rayCast = method == FDZB_SHADOW_RAY_CAST ? 1 : 0;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_depth_plane(fdzb_ctx *c, int enable)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (int rc = ctx_sync(c)) return rc;
+    c->eng.depthPlane = enable ? 1 : 0;
     return FDZB_OK;
 }
 
@@ -1345,6 +1366,13 @@ int fdzb_batch_set_occlusion_schedule(fdzb_batch *b, int schedule)
     if (schedule != FDZB_OCC_LANE_PER_SAMPLE && schedule != FDZB_OCC_LANE_PER_PAIR)
         return fail(FDZB_ERR_INVALID_ARG, "unknown occlusion schedule");
     b->eng.occVariant = schedule;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_depth_plane(fdzb_batch *b, int enable)
+{
+    if (int rc = batch_check(b)) return rc;
+    b->eng.depthPlane = enable ? 1 : 0;
     return FDZB_OK;
 }
 

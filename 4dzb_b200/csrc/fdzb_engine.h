@@ -63,6 +63,7 @@ struct Engine {
     bool useGraph = true;
     int occVariant = 0;    // occlusion kernel (DeviceBuffers::occVariant)
     int rayCast = 0;       // ray-cast cross-check instead of edge masks (DeviceBuffers::rayCast)
+    int depthPlane = 0;    // edge masks also test each triangle's own plane (FrameDesc::depthPlane)
     long long maxPairCapacity = 1ll << 29;   // largest pair buffer; beyond it a frame runs in triangle passes
     // triangle passes of the last single-frame launch (1 = none) and their sums
     int passes = 1;

@@ -13,7 +13,8 @@
 namespace fdzb {
 
 constexpr float kF32Max = 3.402823466e+38f;   // FD_F32_MAX, FS/util/Util.h:59
-constexpr int kMaxLightN = 32;                 // U32 mask rows (K/Step5_2_shadowCalPerSample.inl:251)
+constexpr int kMaxLightN = 64;                 // light grid rows / columns (64-bit row words)
+constexpr int kMaxLightN32 = 32;               // U32 row words (K/Step5_2_shadowCalPerSample.inl:251)
 constexpr int kMaxBins = 512;                  // bins per side
 
 // Light block derived on the host (FS/api.cpp:303-400), device copy per frame.
@@ -22,8 +23,13 @@ struct LightParams {
     float RF[2];            // RectangleFactor
     float ur[3], ul[3], dl[3], dr[3];  // light corners
     float xd[3], yd[3];     // x_delt, y_delt
-    int N;                  // light grid side (lightResWidth == lightResHeight)
-    uint32_t full;          // N low bits set
+    // A sample's mask has N rows (light samples along x_delt, lightResWidth of
+    // them) of NC bits (along y_delt, lightResHeight); bit r * NC + c.  For the
+    // reference's square grids N == NC.
+    int N;                  // rows (lightResWidth)
+    int NC;                 // columns (lightResHeight)
+    uint32_t full;          // NC low bits set, when NC <= 32
+    unsigned long long fullRows, fullCols;  // N and NC low bits set
 };
 
 // Per-frame inputs, outputs and batch offsets (host-filled).
@@ -126,6 +132,9 @@ struct DeviceBuffers {
     int depthBits;                              // secondary (depth-bucket) bits of the pair key
     int occVariant;                             // 0: k_occlusion (lane per sample), 1: k_occlusion_pairs
     int rayCast;                                // 1: ray-cast cross-check (REF_CAL) instead of edge masks
+    int wide;                                   // 1: some frame's light grid exceeds 32 rows or
+                                                // columns: 64-bit row words
+    int depthPlane;                             // 1: the frames test each triangle's own plane
     uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
                                                 // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays

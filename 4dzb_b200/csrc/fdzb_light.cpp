@@ -44,7 +44,10 @@ void light_setup(const float rightRadius, const float topRadius, const float pos
 {
     std::memset(L, 0, sizeof(*L));
     L->N = resW;
-    L->full = resW >= 32 ? 0xffffffffu : ((1u << resW) - 1u);
+    L->NC = resH;
+    L->full = resH >= 32 ? 0xffffffffu : ((1u << resH) - 1u);
+    L->fullRows = resW >= 64 ? ~0ull : ((1ull << resW) - 1ull);
+    L->fullCols = resH >= 64 ? ~0ull : ((1ull << resH) - 1ull);
 
     const V3 pos = v3(position[0], position[1], position[2]);
     const V3 up = normalize(v3(upDir[0], upDir[1], upDir[2]));

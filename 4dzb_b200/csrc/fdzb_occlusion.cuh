@@ -41,20 +41,45 @@ constexpr int kOccThreads = kOccWarps * 32;
 constexpr int kOccChunk = FDZB_OCC_CHUNK;
 constexpr int kItemSamples = FDZB_OCC_ITEM;
 
-// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(N-1) precomputed (the same
-// product) and the result limited to the N-bit light grid.
-__device__ __forceinline__ uint32_t row_mask(float D, float slopeNm1, float slope, uint32_t full,
-                                             uint32_t &npart)
+// Row words: uint32_t (grids up to 32 x 32, the reference's U32) or
+// unsigned long long (up to 64 x 64, the reference's template at T = U64).
+template <class R> struct RowWord;
+template <> struct RowWord<uint32_t> {
+    static constexpr int kBits = 32;
+    static constexpr int kWarps = 4;
+    static constexpr int kMinBlocks = FDZB_OCC_MINBLOCKS;
+    __device__ static int lowest(uint32_t v) { return __ffs(v) - 1; }
+    __device__ static int popc(uint32_t v) { return __popc(v); }
+    __device__ static uint32_t fullCols(const LightParams &L) { return L.full; }
+    __device__ static uint32_t fullRows(const LightParams &L) { return (uint32_t)L.fullRows; }
+};
+template <> struct RowWord<unsigned long long> {
+    static constexpr int kBits = 64;
+    static constexpr int kWarps = 2;
+    static constexpr int kMinBlocks = 5;
+    __device__ static int lowest(unsigned long long v) { return __ffsll((long long)v) - 1; }
+    __device__ static int popc(unsigned long long v) { return __popcll(v); }
+    __device__ static unsigned long long fullCols(const LightParams &L) { return L.fullCols; }
+    __device__ static unsigned long long fullRows(const LightParams &L) { return L.fullRows; }
+};
+typedef unsigned long long u64;
+
+// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(count-1) precomputed (the
+// same product) and the result limited to the grid's bits.  The shift has the
+// PTX shl semantics of the reference's device code: amounts >= the word width
+// (or negative) give 0.
+template <class R>
+__device__ __forceinline__ R row_mask(float D, float slopeNm1, float slope, R full, uint32_t &npart)
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
     if (f1 && f2) return full;
-    if (!f1 && !f2) return 0u;
+    if (!f1 && !f2) return R(0);
     ++npart;
     const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
     const int k = __float2int_rz(ceilf(q));
-    uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
-    m -= 1u;
+    R m = ((unsigned)k >= (unsigned)RowWord<R>::kBits) ? R(0) : (R(1) << k);
+    m -= R(1);
     if (!f1) m = ~m;
     return m & full;
 }
@@ -73,7 +98,7 @@ __device__ __forceinline__ bool point_in_tri(f3 A, f3 B, f3 C, f3 P)
 // Staged triangle, 7 x float4:
 //  p0 = (aabb min x, min y, max x, max y)   p1 = (minz, v0)
 //  p2 = (v1, v2.x)   p3 = (v2.y, v2.z, n.x, n.y)   p4 = (n.z, e01)
-//  p5 = (e12, e20.x) p6 = (e20.y, e20.z, 0, 0)
+//  p5 = (e12, e20.x) p6 = (e20.y, e20.z, maxz, 0)
 struct StagedTri {
     float4 p[7];
 };
@@ -93,7 +118,7 @@ __device__ __forceinline__ void stage_triangle(StagedTri &dst, const float4 *__r
     dst.p[3] = make_float4(v2.y, v2.z, n.x, n.y);
     dst.p[4] = make_float4(n.z, e01.x, e01.y, e01.z);
     dst.p[5] = make_float4(e12.x, e12.y, e12.z, e20.x);
-    dst.p[6] = make_float4(e20.y, e20.z, 0.0f, 0.0f);
+    dst.p[6] = make_float4(e20.y, e20.z, q1.w, 0.0f);
 }
 
 struct LaneSample {
@@ -115,11 +140,39 @@ __device__ __forceinline__ void load_sample(LaneSample &s, const FrameDesc &fr, 
     s.L0Q = sub3(ld3(fr.light.ur), s.Q);
 }
 
-// One sample/triangle pair (K/Step5_2_shadowCalPerSample.inl:120-222).  Returns 1
-// if the pair passed the AABB pre-cull.
-__device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s, f3 xd, f3 yd,
-                                         float esp, float nm1, uint32_t FULL, uint32_t (*rows)[32],
-                                         int lane, uint32_t &fullRows, uint32_t &nrows, uint32_t &npart)
+// Light grid constants of a frame, in the form the pair tests use them.
+template <class R> struct GridC {
+    int NR, NC;             // rows (along x_delt), columns (along y_delt)
+    float nrm1, ncm1;       // NR - 1, NC - 1
+    R FR, FC;               // NR and NC low bits
+};
+template <class R> __device__ __forceinline__ GridC<R> grid_of(const FrameDesc &fr)
+{
+    GridC<R> g;
+    g.NR = fr.light.N;
+    g.NC = fr.light.NC;
+    g.nrm1 = (float)(g.NR - 1);
+    g.ncm1 = (float)(g.NC - 1);
+    g.FR = RowWord<R>::fullRows(fr.light);
+    g.FC = RowWord<R>::fullCols(fr.light);
+    return g;
+}
+
+// One sample/triangle pair (K/Step5_2_shadowCalPerSample.inl:120-222).  Rows r
+// step along x_delt (A), columns c along y_delt (B); the row filter bounds the
+// column term with B*(NC-1) and the rows with A*(NR-1), which for the
+// reference's square grids are its own expressions.  With the depth plane, a
+// fourth plane -n.(L - v0), oriented like the edges, keeps light samples on
+// the sample's side of the triangle unoccluded (the test of the reference's
+// per-bin kernel, K/Step5_2_shadowCal.inl:667-674, 838) for triangles that
+// reach the light plane (min depth <= 0: occluders behind the light) or the
+// sample's depth (the per-bin kernel's own condition); a triangle strictly
+// between them needs no such test.  Returns 1 if the pair passed the AABB
+// pre-cull.
+template <class R, int DEPTH>
+__device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s, f3 xd, f3 yd, f3 ur,
+                                         float esp, const GridC<R> &g, R (*rows)[32], int lane, R &fullRows,
+                                         uint32_t &nrows, uint32_t &npart)
 {
     const float4 p0 = T.p[0];
     const float4 p1 = T.p[1];
@@ -143,25 +196,39 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
     const float A0 = dot3(n0, t0), B0 = dot3(n0, t1), C0 = dot3(n0, lq);
     const float A1 = dot3(n1, t0), B1 = dot3(n1, t1), C1 = dot3(n1, lq);
     const float A2 = dot3(n2, t0), B2 = dot3(n2, t1), C2 = dot3(n2, lq);
-    const float An0 = __fmul_rn(A0, nm1), An1 = __fmul_rn(A1, nm1), An2 = __fmul_rn(A2, nm1);
-    const float Bn0 = __fmul_rn(B0, nm1), Bn1 = __fmul_rn(B1, nm1), Bn2 = __fmul_rn(B2, nm1);
+    const float An0 = __fmul_rn(A0, g.nrm1), An1 = __fmul_rn(A1, g.nrm1), An2 = __fmul_rn(A2, g.nrm1);
+    const float Bn0 = __fmul_rn(B0, g.ncm1), Bn1 = __fmul_rn(B1, g.ncm1), Bn2 = __fmul_rn(B2, g.ncm1);
     // row filter (:176-191)
-    const uint32_t N0 = row_mask(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, FULL, npart);
-    const uint32_t N1 = row_mask(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, FULL, npart);
-    const uint32_t N2 = row_mask(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, FULL, npart);
-    uint32_t vr = N0 & N1 & N2 & ~fullRows;
+    const R N0 = row_mask<R>(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, g.FR, npart);
+    const R N1 = row_mask<R>(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, g.FR, npart);
+    const R N2 = row_mask<R>(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, g.FR, npart);
+    R vr = N0 & N1 & N2 & ~fullRows;
+    const bool dp = DEPTH && (p1.x <= 0.0f || p6.z >= s.spZ);
+    float A3 = 0.0f, B3 = 0.0f, C3 = 0.0f, Bn3 = 0.0f;
+    if (dp && vr) {
+        const f3 m = mk3(-n.x, -n.y, -n.z);
+        const f3 lv0 = sub3(ur, v0);
+        const f3 lv = neg ? mk3(-lv0.x, -lv0.y, -lv0.z) : lv0;
+        A3 = dot3(m, t0);
+        B3 = dot3(m, t1);
+        C3 = dot3(m, lv);
+        Bn3 = __fmul_rn(B3, g.ncm1);
+        vr &= row_mask<R>(__fadd_rn(B3 > 0.0f ? Bn3 : 0.0f, C3), __fmul_rn(A3, g.nrm1), A3, g.FR, npart);
+    }
     // rows (:204-222)
     while (vr) {
-        const int r = __ffs(vr) - 1;
-        vr &= vr - 1u;
+        const int r = RowWord<R>::lowest(vr);
+        vr &= vr - R(1);
         ++nrows;
         const float fr = (float)r;
-        const uint32_t M0 = row_mask(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, FULL, npart);
-        const uint32_t M1 = row_mask(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, FULL, npart);
-        const uint32_t M2 = row_mask(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, FULL, npart);
-        const uint32_t nv = rows[r][lane] | (M0 & M1 & M2);
+        const R M0 = row_mask<R>(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, g.FC, npart);
+        const R M1 = row_mask<R>(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, g.FC, npart);
+        const R M2 = row_mask<R>(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, g.FC, npart);
+        R m = M0 & M1 & M2;
+        if (dp) m &= row_mask<R>(__fadd_rn(__fmul_rn(A3, fr), C3), Bn3, B3, g.FC, npart);
+        const R nv = rows[r][lane] | m;
         rows[r][lane] = nv;
-        if (nv == FULL) fullRows |= 1u << r;
+        if (nv == g.FC) fullRows |= R(1) << r;
     }
     return 1;
 }
@@ -177,9 +244,10 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
 // masks compare bit for bit.  Same pre-cull as the reference's checker: the
 // sample's rectangle inside the triangle's AABB and minz - 1e-3 (in double, as
 // the reference's double literal makes it) not above the sample's depth.
+template <class R>
 __device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample &s, f3 ur, f3 xd, f3 yd,
-                                            int N, uint32_t FULL, uint32_t (*rows)[32], int lane,
-                                            uint32_t &fullRows, uint32_t &nrows)
+                                            const GridC<R> &g, R (*rows)[32], int lane, R &fullRows,
+                                            uint32_t &nrows)
 {
     const float4 p0a = T.p[0];
     const float4 p1a = T.p[1];
@@ -192,14 +260,14 @@ __device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample
     const f3 n = cross3(e1, e0);
     const f3 q0 = sub3(v0, s.Q);
     const float tmin = 1e-3f;
-    for (int r = 0; r < N; ++r) {
-        const uint32_t have = rows[r][lane];
-        if (have == FULL) continue;
+    for (int r = 0; r < g.NR; ++r) {
+        const R have = rows[r][lane];
+        if (have == g.FC) continue;
         ++nrows;
         const f3 lr = add3(ur, mul3(xd, (float)r));   // upRight + x_delt * j
-        uint32_t add = 0u;
-        for (int c = 0; c < N; ++c) {
-            if (have & (1u << c)) continue;
+        R add = 0;
+        for (int c = 0; c < g.NC; ++c) {
+            if (have & (R(1) << c)) continue;
             const f3 lp = add3(lr, mul3(yd, (float)c));   // ... + y_delt * i
             const f3 L = sub3(lp, s.Q);
             const float dist = __fsqrt_rn(dot3(L, L));
@@ -211,70 +279,89 @@ __device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample
             const float gamma = dot3(iv, e0);
             const float t = dot3(n, e2);
             if ((t < dist) & (t > tmin) & (beta >= 0.0f) & (gamma >= 0.0f) & (__fadd_rn(beta, gamma) <= 1.0f))
-                add |= 1u << c;
+                add |= R(1) << c;
         }
         if (add) {
-            const uint32_t nv = have | add;
+            const R nv = have | add;
             rows[r][lane] = nv;
-            if (nv == FULL) fullRows |= 1u << r;
+            if (nv == g.FC) fullRows |= R(1) << r;
         }
     }
     return 1;
 }
 
-__device__ __forceinline__ void write_result(const FrameDesc &fr, int local, int N, uint32_t (*rows)[32],
+// Bits [pos, pos + n) of a packed mask (n <= 64), LSB first.
+__device__ __forceinline__ u64 mask_bits(const uint32_t *w, int pos, int n)
+{
+    u64 v = 0;
+    int got = 0;
+    while (got < n) {
+        const int wi = (pos + got) >> 5, o = (pos + got) & 31;
+        const int take = min(32 - o, n - got);
+        const uint32_t part = (w[wi] >> o) & (take == 32 ? 0xffffffffu : ((1u << take) - 1u));
+        v |= (u64)part << got;
+        got += take;
+    }
+    return v;
+}
+
+// Shadow = set bits / (rows * cols) (:226-231) and the packed mask, bit r * NC + c.
+template <class R>
+__device__ __forceinline__ void write_result(const FrameDesc &fr, int local, const GridC<R> &g, R (*rows)[32],
                                              int lane)
 {
     int cnt = 0;
-    for (int r = 0; r < N; ++r) cnt += __popc(rows[r][lane]);
-    fr.shadow[local] = __fdiv_rn((float)cnt, (float)(N * N));   // :226-231
+    for (int r = 0; r < g.NR; ++r) cnt += RowWord<R>::popc(rows[r][lane]);
+    fr.shadow[local] = __fdiv_rn((float)cnt, (float)(g.NR * g.NC));   // :226-231
     if (fr.masks) {
         uint32_t *mo = fr.masks + (size_t)local * fr.maskWords;
-        uint32_t acc = 0u;
+        u64 acc = 0;
         int bit = 0, wi = 0;
-        for (int r = 0; r < N; ++r) {
-            const uint32_t v = rows[r][lane];
-            acc |= v << bit;
-            const int nb = bit + N;
-            if (nb >= 32) {
-                mo[wi++] = acc;
-                acc = (nb > 32) ? (v >> (32 - bit)) : 0u;
-                bit = nb - 32;
-            } else {
-                bit = nb;
+        for (int r = 0; r < g.NR; ++r) {
+            u64 v = (u64)rows[r][lane];
+            int rem = g.NC;
+            while (rem > 0) {
+                const int take = min(rem, 32);
+                const u64 part = v & (take == 32 ? 0xffffffffull : ((1ull << take) - 1ull));
+                acc |= part << bit;
+                bit += take;
+                if (bit >= 32) {
+                    mo[wi++] = (uint32_t)acc;
+                    acc >>= 32;
+                    bit -= 32;
+                }
+                v >>= take;
+                rem -= take;
             }
         }
-        if (bit > 0) mo[wi] = acc;
+        if (bit > 0) mo[wi] = (uint32_t)acc;
     }
 }
 
-// Rows of a sample from its packed mask (bit r*N + j is row r, column j), for a
-// launch that accumulates into masks of an earlier triangle pass.  Returns the
-// set of full rows.
-__device__ __forceinline__ uint32_t load_rows(const FrameDesc &fr, int local, int N, uint32_t full,
-                                              uint32_t (*rows)[32], int lane)
+// Rows of a sample from its packed mask (bit r*NC + c is row r, column c), for
+// a launch that accumulates into masks of an earlier triangle pass.  Returns
+// the set of full rows.
+template <class R>
+__device__ __forceinline__ R load_rows(const FrameDesc &fr, int local, const GridC<R> &g, R (*rows)[32], int lane)
 {
     const uint32_t *mi = fr.masks + (size_t)local * fr.maskWords;
-    uint32_t fullRows = 0u;
-    for (int r = 0; r < N; ++r) {
-        const int bit = r * N, w = bit >> 5, o = bit & 31;
-        uint32_t v = mi[w] >> o;
-        if (o + N > 32) v |= mi[w + 1] << (32 - o);
-        v &= full;
+    R fullRows = 0;
+    for (int r = 0; r < g.NR; ++r) {
+        const R v = (R)mask_bits(mi, r * g.NC, g.NC) & g.FC;
         rows[r][lane] = v;
-        if (v == full) fullRows |= 1u << r;
+        if (v == g.FC) fullRows |= R(1) << r;
     }
     return fullRows;
 }
 
 // First contact of a sample with the pipeline's occlusion stage: rows cleared,
 // or loaded from the masks of an earlier triangle pass.
-__device__ __forceinline__ uint32_t init_rows(const FrameDesc &fr, int local, int N, uint32_t full,
-                                              uint32_t (*rows)[32], int lane)
+template <class R>
+__device__ __forceinline__ R init_rows(const FrameDesc &fr, int local, const GridC<R> &g, R (*rows)[32], int lane)
 {
-    if (fr.accumulate) return load_rows(fr, local, N, full, rows, lane);
-    for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
-    return 0u;
+    if (fr.accumulate) return load_rows<R>(fr, local, g, rows, lane);
+    for (int r = 0; r < g.NR; ++r) rows[r][lane] = 0;
+    return 0;
 }
 
 __device__ __forceinline__ void write_zero(const FrameDesc &fr, int local)
@@ -321,8 +408,11 @@ __global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restri
 }
 
 // RAYCAST = 1: the ray-cast cross-check instead of the edge-function masks.
-template <int RAYCAST>
-__global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
+// R: the row word (uint32_t for grids up to 32 x 32, u64 up to 64 x 64; the
+// 64-bit form runs 2 warps per block to keep its rows in shared memory).
+// DEPTH = 1: the edge-function masks also test the triangle's own plane.
+template <int RAYCAST, class R, int DEPTH>
+__global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlocks)
     k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
                 const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
@@ -330,10 +420,10 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                 const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
                 const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
 {
-    __shared__ StagedTri s_tri[kOccWarps][kOccChunk];
-    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
+    __shared__ StagedTri s_tri[RowWord<R>::kWarps][kOccChunk];
+    __shared__ R s_rows[RowWord<R>::kWarps][RowWord<R>::kBits][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t(*rows)[32] = s_rows[warp];
+    R(*rows)[32] = s_rows[warp];
     StagedTri *tris = s_tri[warp];
     unsigned long long tested = 0;
     uint32_t nrows = 0, npart = 0;
@@ -372,16 +462,14 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
             continue;
         }
 
-        const int N = fr.light.N;
-        const uint32_t FULL = fr.light.full;
-        const float nm1 = (float)(N - 1);
-        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd);
+        const GridC<R> g = grid_of<R>(fr);
+        const f3 xd = ld3(fr.light.xd), yd = ld3(fr.light.yd), ur = ld3(fr.light.ur);
         const float esp = fr.esp;
 
         LaneSample smp;
         int local = 0;
         int remaining = 0;
-        uint32_t fullRows = 0u;
+        R fullRows = 0;
         bool active = false;
         int next = sLo;
         // first fill
@@ -395,8 +483,8 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                     active = true;
                     remaining = nT;
                     load_sample(smp, fr, st, local);
-                    fullRows = init_rows(fr, local, N, FULL, rows, lane);
-                    if (fullRows == FULL) remaining = 0;
+                    fullRows = init_rows<R>(fr, local, g, rows, lane);
+                    if (fullRows == g.FR) remaining = 0;
                 }
             }
             next += 32;
@@ -423,19 +511,18 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                 if (remaining > 0) {
                     --remaining;
                     if (RAYCAST)
-                        tested += raycast_pair(tris[t], smp, ld3(fr.light.ur), xd, yd, N, FULL, rows, lane,
-                                               fullRows, nrows);
+                        tested += raycast_pair<R>(tris[t], smp, ur, xd, yd, g, rows, lane, fullRows, nrows);
                     else
-                        tested += pair_test(tris[t], smp, xd, yd, esp, nm1, FULL, rows, lane, fullRows, nrows,
-                                            npart);
-                    if (fullRows == FULL) remaining = 0;
+                        tested += pair_test<R, DEPTH>(tris[t], smp, xd, yd, ur, esp, g, rows, lane, fullRows,
+                                                      nrows, npart);
+                    if (fullRows == g.FR) remaining = 0;
                 }
             }
             cur += m;
             if (cur >= nT) cur -= nT;
             // retire finished lanes, then refill them with the item's next samples
             if (active && remaining == 0) {
-                write_result(fr, local, N, rows, lane);
+                write_result<R>(fr, local, g, rows, lane);
                 active = false;
             }
             const unsigned freeLanes = __ballot_sync(kFullWarp, !active);
@@ -457,8 +544,8 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC_MINBLOCKS)
                         active = true;
                         remaining = nT;
                         load_sample(smp, fr, st, local);
-                        fullRows = init_rows(fr, local, N, FULL, rows, lane);
-                        if (fullRows == FULL) remaining = 0;
+                        fullRows = init_rows<R>(fr, local, g, rows, lane);
+                        if (fullRows == g.FR) remaining = 0;
                     }
                 }
                 next += __popc(freeLanes);
@@ -589,7 +676,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
                       const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
 {
     __shared__ StagedTri s_tri[kOccWarps][kOccChunk];
-    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN][32];
+    __shared__ uint32_t s_rows[kOccWarps][kMaxLightN32][32];
     __shared__ uint32_t s_full[kOccWarps][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t(*rows)[32] = s_rows[warp];
@@ -657,7 +744,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
             }
         }
         uint32_t fr0 = FULL;
-        if (has) fr0 = init_rows(fr, local, N, FULL, rows, lane);
+        if (has) fr0 = init_rows<uint32_t>(fr, local, grid_of<uint32_t>(fr), rows, lane);
         else
             for (int r = 0; r < N; ++r) rows[r][lane] = 0u;
         sfull[lane] = fr0;
@@ -773,7 +860,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
             active = active && sfull[lane] != FULL;
         }
         __syncwarp();
-        if (has) write_result(fr, local, N, rows, lane);
+        if (has) write_result<uint32_t>(fr, local, grid_of<uint32_t>(fr), rows, lane);
     }
     unsigned long long t = tested, tr = nrows, tp = npart;
 #pragma unroll

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256)
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     const int words = fr.maskWords;
-    const int NN = fr.light.N * fr.light.N;
+    const int NN = fr.light.N * fr.light.NC;
     int nvalid = 0, nquirk = 0;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < S; base += stride) {
         const int p = base + lane;
@@ -823,18 +823,28 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
         b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
         b.items, b.itemCapacity, b.counters);
-    if (b.rayCast)
-        k_occlusion<1><<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
-            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
-            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
-    else if (b.occVariant == 1)
-        k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(
-            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
-            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
-    else
-        k_occlusion<0><<<sm * FDZB_OCC_MINBLOCKS, kOccThreads, 0, s>>>(
-            b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd,
-            b.binTriStart, b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf);
+    // 64-bit row words when some frame's grid exceeds 32 rows or columns; the
+    // lane-per-pair schedule only runs square 32-bit grids without the depth
+    // plane (the host falls back to lane per sample otherwise)
+    typedef RowWord<u64> W64;
+    const int g32 = sm * FDZB_OCC_MINBLOCKS, g64 = sm * W64::kMinBlocks, t64 = W64::kWarps * 32;
+#define FDZB_OCC_ARGS                                                                                        \
+    b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd, b.binTriStart, \
+        b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf
+    if (b.wide) {
+        if (b.rayCast) k_occlusion<1, u64, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
+        else if (b.depthPlane) k_occlusion<0, u64, 1><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
+        else k_occlusion<0, u64, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
+    } else if (b.rayCast) {
+        k_occlusion<1, uint32_t, 0><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+    } else if (b.occVariant == 1) {
+        k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+    } else if (b.depthPlane) {
+        k_occlusion<0, uint32_t, 1><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+    } else {
+        k_occlusion<0, uint32_t, 0><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+    }
+#undef FDZB_OCC_ARGS
     nl += 2;
     if (ev) cudaEventRecord(ev[STAGE_COUNT], s);
     if (launches) *launches = nl;

@@ -468,7 +468,7 @@ int fdzb_serve_submit(fdzb_server *s, const fdzb_request *q, uint64_t *ticket)
     if (q->bins != 0 && (q->bins < 1 || q->bins > fdzb::kMaxBins || (q->bins & (q->bins - 1))))
         return fdzb::set_error(FDZB_ERR_INVALID_ARG, "bin number must be 0 or a power of two in [1, 512]");
     const long long S = (long long)q->W * q->H;
-    r.outBytes = (size_t)S * 4 + (q->d_masks ? (size_t)S * 4 * ((r.spec.light.N * r.spec.light.N + 31) / 32) : 0);
+    r.outBytes = (size_t)S * 4 + (q->d_masks ? (size_t)S * 4 * ((r.spec.light.N * r.spec.light.NC + 31) / 32) : 0);
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (r.spec.bins == 0) r.spec.bins = fdzb::tuned_bins(s->tuned, r.spec);

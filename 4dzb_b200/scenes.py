@@ -58,7 +58,16 @@ class Light:
     position: tuple = (0.0, 0.0, 6.0)
     view_dir: tuple = (0.0, 0.0, -1.0)
     up_dir: tuple = (0.0, 1.0, 0.0)
-    n: int = 8
+    n: int = 8               # lightResWidth: rows of a sample's mask, along x_delt
+    nh: int = 0              # lightResHeight (0: square, = n): columns, along y_delt
+
+    @property
+    def rows(self) -> int:
+        return self.n
+
+    @property
+    def cols(self) -> int:
+        return self.nh if self.nh else self.n
 
 
 @dataclass
@@ -74,6 +83,7 @@ class Scene:
     esp: float = 1e-3
     cull: bool = False
     name: str = ""
+    depth_plane: bool = False   # also test each triangle's own plane (occluders not between)
     meta: dict = field(default_factory=dict)
 
     @property

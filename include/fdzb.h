@@ -16,9 +16,10 @@
  *  - samples are row-major float4[W*H] positions and normals (xyz, w unused),
  *    NaN position.x marks background (the reference's G-buffer clear value);
  *  - outputs: shadow float[W*H] at index y*W+x (fraction of occluded light
- *    samples, 1 - visibility) and, optionally, masks uint32[W*H][ceil(N*N/32)]
- *    with light sample (row i along the light's width, column j along its
- *    height) at bit i*N+j, least significant bit first.
+ *    samples, 1 - visibility) and, optionally, masks uint32[W*H][ceil(Lw*Lh/32)]
+ *    for an Lw x Lh light grid, with light sample (row i < Lw along the
+ *    light's width, column j < Lh along its height) at bit i*Lh+j, least
+ *    significant bit first (square grids: bit i*N+j).
  *
  * Reference-shaped global context: one process-wide context on the current CUDA
  * device, single-threaded like FD:: (K/FourD.cu:47-136).  The fdzb_ctx_* handle
@@ -45,7 +46,11 @@ extern "C" {
 #define FDZB_ERR_NOT_READY       -8   /* required inputs (view, samples, model, light, output) not set */
 
 /* Same 52-byte layout as AreaLightDes (4DZB/FDZB_Soft_Shadow/AreaLightDesc.h:3-14):
- * two floats, three glm::vec3, two ints.  lightResWidth == lightResHeight = N, 1..32. */
+ * two floats, three glm::vec3, two ints.  The reference runs square grids,
+ * lightResWidth == lightResHeight = N in 1..32; this library takes any
+ * lightResWidth x lightResHeight in 1..64 each.  A sample's mask has
+ * lightResWidth rows (light samples along x_delt) of lightResHeight bits (along
+ * y_delt): bit r * lightResHeight + c, LSB first, ceil(W*H/32) words. */
 typedef struct fdzb_area_light_desc {
     float rightRadius;      /* half width */
     float topRadius;        /* half height */
@@ -165,6 +170,16 @@ int fdzb_ctx_move_model(fdzb_ctx *ctx, const float m[16]);
 #define FDZB_SHADOW_RAY_CAST   1
 int fdzb_ctx_set_shadow_method(fdzb_ctx *ctx, int method);
 
+/* Depth plane (edge-function masks only; default off).  The reference's
+ * per-sample kernel assumes every occluder lies between the sample and the
+ * light (it has no triangle-plane test), and shadows wrongly with occluders
+ * beside or behind the light.  Enabled, a pair whose triangle reaches the
+ * light plane (min light depth <= 0) or the sample's depth also tests the
+ * triangle's own plane, as the reference's per-bin kernel does
+ * (K/Step5_2_shadowCal.inl:667-674, 838): light samples on the sample's side
+ * of that plane are not occluded by it. */
+int fdzb_ctx_set_depth_plane(fdzb_ctx *ctx, int enable);
+
 /* Model transform applied to model 0's vertices as they are read, leaving the
  * vertex buffer untouched (the reference's moveModel rewrites the VBO in place,
  * K/moveModel.inl:14-50).  m: column-major 4x4, NULL = none.  A launch with m
@@ -231,7 +246,8 @@ int fdzb_ctx_set_tri_order(fdzb_ctx *ctx, int order);
  *   FDZB_OCC_LANE_PER_SAMPLE (default): a lane per sample of a bin, the warp
  *     streaming the bin's triangles through shared memory;
  *   FDZB_OCC_LANE_PER_PAIR: the pairs that pass the AABB pre-cull, and then
- *     their (pair, light row) units, are dealt one per lane. */
+ *     their (pair, light row) units, are dealt one per lane.  Square grids up
+ *     to 32 x 32 without the depth plane; other launches run lane per sample. */
 #define FDZB_OCC_LANE_PER_SAMPLE 0
 #define FDZB_OCC_LANE_PER_PAIR   1
 int fdzb_ctx_set_occlusion_schedule(fdzb_ctx *ctx, int schedule);
@@ -319,12 +335,12 @@ typedef struct fdzb_frame_desc {
     size_t vtx_stride_bytes;
     const int32_t *d_idx;          /* int3 per triangle */
     size_t n_tri;
-    fdzb_area_light_desc light;    /* N x N grid, N in [1, 32] */
+    fdzb_area_light_desc light;    /* width x height grid, each in [1, 64] */
     int32_t bins;                  /* bins per side: power of two in [1, 512]; 0 = autotuned */
     int32_t cull;                  /* back-face culling of triangles (FDsetBackfaceCull) */
     float esp;                     /* FDsetScenesEsp */
     float *d_shadow;               /* float[W*H] at y*W+x */
-    uint32_t *d_masks;             /* nullable: uint32[W*H*ceil(N*N/32)], bit i*N+j */
+    uint32_t *d_masks;             /* nullable: uint32[W*H*ceil(Lw*Lh/32)], bit r*Lh+c */
     const float *model_transform;  /* nullable host pointer: 16 floats, see fdzb_ctx_set_model_transform */
 } fdzb_frame_desc;
 
@@ -351,6 +367,8 @@ int fdzb_batch_set_graph(fdzb_batch *batch, int enable);
 int fdzb_batch_set_profiling(fdzb_batch *batch, int enable);
 int fdzb_batch_set_tri_order(fdzb_batch *batch, int order);
 int fdzb_batch_set_occlusion_schedule(fdzb_batch *batch, int schedule);
+/* fdzb_ctx_set_depth_plane for every frame of the batch's launches. */
+int fdzb_batch_set_depth_plane(fdzb_batch *batch, int enable);
 /* Enqueue frames[0..n) (the descriptors are copied; buffers must stay valid until
  * fdzb_batch_sync returns). */
 int fdzb_batch_launch_async(fdzb_batch *batch, const fdzb_frame_desc *frames, int n);

@@ -19,6 +19,23 @@
  *    memory (K/Step5_2_shadowCalPerSample.inl:28-31,204-222).  Both events are
  *    counted (quirk_high_bits, quirk_rows_beyond_n);
  *  - a shift by >= 32 yields 0 (PTX shl semantics of the reference's device code).
+ *
+ * Beyond the reference's per-sample kernel (square grids, N <= 32,
+ * K/Step5_2_shadowCalPerSample.inl:249-254), the same arithmetic covers
+ * rectangular grids up to 64 x 64: rows r along x_delt (lightResWidth of
+ * them), columns c along y_delt (lightResHeight); the row filter bounds the
+ * column term with B*(cols-1) and the rows with A*(rows-1), the row masks are
+ * the reference's closed form on 64-bit words (its own template instantiated
+ * for U64), and for a square grid all of it reduces to the reference's
+ * formulas.  Optionally (depth_plane) a fourth plane, the triangle's own,
+ * keeps light samples on the sample's side of the triangle unoccluded -- the
+ * test of the reference's per-bin kernel (K/Step5_2_shadowCal.inl:667-674,
+ * 838) -- for triangles that reach the light plane (min depth <= 0: the
+ * occluders behind the light the per-sample kernel mis-handles) or the
+ * sample's depth (max depth >= the sample's, the per-bin kernel's own
+ * condition).  A triangle strictly between the light plane and the sample
+ * needs no such test: the segment from the sample to any light sample in its
+ * edge cone crosses it.
  */
 #include "fdzb_oracle.h"
 
@@ -56,6 +73,9 @@ static inline v3 norm3(v3 v)
 }
 
 int32_t orc_mask_words(int32_t N) { return (N * N + 31) / 32; }
+int32_t orc_mask_words_rc(int32_t rows, int32_t cols) { return (rows * cols + 31) / 32; }
+
+static inline uint64_t low_bits64(int n) { return n >= 64 ? ~(uint64_t)0 : (((uint64_t)1 << n) - 1u); }
 
 /* ---------------------------------------------------------------------------
  * A1 light setup: FS/api.cpp:303-400 (FDsetAreaLight) with GLM 0.9.8 lookAtRH
@@ -72,6 +92,8 @@ void orc_light_setup(const orc_light_desc *d, orc_light *L)
     L->resH = d->lightResHeight;
     L->resNum = d->lightResWidth * d->lightResHeight;
     L->fullBits = d->lightResWidth >= 32 ? 0xFFFFFFFFu : ((1u << d->lightResWidth) - 1u);
+    L->fullRows = low_bits64(d->lightResWidth);
+    L->fullCols = low_bits64(d->lightResHeight);
 
     v3 pos = ld3(d->position);
     v3 up = norm3(ld3(d->upDir));
@@ -179,9 +201,6 @@ static inline void plane_disc(float *A, float *B, float *C, v3 a, v3 b, v3 Q, v3
     *C = dot3(n, L0Q);
 }
 
-/* 1 << k with PTX shl.b32 semantics: amounts >= 32 (or negative) give 0. */
-static inline uint32_t shl1(int k) { return ((unsigned)k >= 32u) ? 0u : (1u << k); }
-
 /* float -> int32 with PTX cvt.rzi.s32.f32 saturation (NaN -> 0). */
 static inline int f2i_sat(float q)
 {
@@ -191,10 +210,12 @@ static inline int f2i_sat(float q)
     return (int)q;
 }
 
-/* K/Step5_2_shadowCalPerSample.inl:14-33, unmasked (bits >= N may be set). */
+/* K/Step5_2_shadowCalPerSample.inl:14-33, unmasked (bits >= N may be set), on a
+ * `bits`-wide word: 32 is the reference's U32, 64 its template's U64 form.  The
+ * shift has PTX shl semantics: amounts >= the width (or negative) give 0. */
 static _Thread_local int64_t tl_partial = 0, tl_rows = 0;
 
-static inline uint32_t row_mask_raw(float D, float s, unsigned nm1, uint32_t full)
+static inline uint64_t row_mask_raw(float D, float s, unsigned nm1, uint64_t full, int bits)
 {
     int f1 = (D >= 0.0f);
     int f2 = (s * (float)nm1 + D >= 0.0f);
@@ -202,9 +223,11 @@ static inline uint32_t row_mask_raw(float D, float s, unsigned nm1, uint32_t ful
     if (!f1 && !f2) return 0u;
     ++tl_partial;
     float q = (-1.0f * D) / s;
-    uint32_t m = shl1(f2i_sat(ceilf(q)));
+    int k = f2i_sat(ceilf(q));
+    uint64_t m = ((unsigned)k >= (unsigned)bits) ? 0u : ((uint64_t)1 << k);
     m -= 1u;
     if (!f1) m = ~m;
+    if (bits == 32) m &= 0xFFFFFFFFu;
     return m;
 }
 
@@ -216,10 +239,26 @@ typedef struct {
 
 typedef struct {
     float ur[3], xd[3], yd[3];
-    int N;
-    uint32_t full;
+    int NR, NC;              /* rows along x_delt, columns along y_delt */
+    int bits;                /* row word width: 32 when both fit, else 64 */
+    uint64_t fullr, fullc;   /* NR and NC low bits */
     float esp;
+    int depth;               /* test the triangle's own plane too */
 } pair_ctx;
+
+static void pair_ctx_init(pair_ctx *c, const orc_light *L, float esp, int depth)
+{
+    memcpy(c->ur, L->upRight, sizeof(c->ur));
+    memcpy(c->xd, L->x_delt, sizeof(c->xd));
+    memcpy(c->yd, L->y_delt, sizeof(c->yd));
+    c->NR = L->resW;
+    c->NC = L->resH;
+    c->bits = (L->resW <= 32 && L->resH <= 32) ? 32 : 64;
+    c->fullr = L->fullRows;
+    c->fullc = L->fullCols;
+    c->esp = esp;
+    c->depth = depth;
+}
 
 /* Ray-cast check of one sample/triangle pair (K/Step5_2_calRef.inl:1-126): for
  * every light sample not yet set, the ray from Q to the light sample (placed at
@@ -227,21 +266,20 @@ typedef struct {
  * intersect_triangle_branchless (1e-3 < t < dist, barycentric test).  Light
  * sample (i along the height, j along the width) is stored at row j, column i,
  * the edge-function masks' layout.  The caller applies the pre-cull. */
-static inline void raycast_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint32_t *mask, uint32_t *full_rows)
+static inline void raycast_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint64_t *mask, uint64_t *full_rows)
 {
-    const int N = c->N;
     v3 p0 = ld3(t->v0), p1 = ld3(t->v1), p2 = ld3(t->v2);
     v3 e0 = sub3(p1, p0), e1 = sub3(p0, p2);
     v3 n = cross3(e1, e0);
     v3 q0 = sub3(p0, Q);
     v3 ur = ld3(c->ur), xd = ld3(c->xd), yd = ld3(c->yd);
     const float tmin = 1e-3f;
-    for (int r = 0; r < N; ++r) {
-        if (mask[r] == c->full) continue;
+    for (int r = 0; r < c->NR; ++r) {
+        if (mask[r] == c->fullc) continue;
         v3 lr = add3(ur, mul3(xd, (float)r));
-        uint32_t add = 0;
-        for (int col = 0; col < N; ++col) {
-            if (mask[r] & (1u << col)) continue;
+        uint64_t add = 0;
+        for (int col = 0; col < c->NC; ++col) {
+            if (mask[r] & ((uint64_t)1 << col)) continue;
             v3 lp = add3(lr, mul3(yd, (float)col));
             v3 L = sub3(lp, Q);
             float dist = sqrtf(dot3(L, L));
@@ -251,18 +289,19 @@ static inline void raycast_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint3
             v3 iv = cross3(dir, e2);
             float beta = dot3(iv, e1), gamma = dot3(iv, e0), tt = dot3(n, e2);
             if ((tt < dist) & (tt > tmin) & (beta >= 0.0f) & (gamma >= 0.0f) & (beta + gamma <= 1.0f))
-                add |= 1u << col;
+                add |= (uint64_t)1 << col;
         }
         mask[r] |= add;
-        if (mask[r] == c->full) *full_rows |= 1u << r;
+        if (mask[r] == c->fullc) *full_rows |= (uint64_t)1 << r;
     }
 }
 
 /* One sample/triangle pair: K/Step5_2_shadowCalPerSample.inl:129-222.  `mask` holds
- * N rows, `full_rows` the rows already equal to FULL.  Returns 1 if the pair was
- * evaluated past the self-intersection skip.  Counters track reference quirks. */
-static inline int pair_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint32_t *mask,
-                            uint32_t *full_rows, int64_t *q_rows, int *q_high)
+ * NR rows of NC bits, `full_rows` the rows already full.  spZ is the sample's
+ * light depth (for the depth-plane rule).  Returns 1 if the pair was evaluated
+ * past the self-intersection skip.  Counters track reference quirks. */
+static inline int pair_test(const pair_ctx *c, v3 Q, float spZ, const tri_rec *t, uint64_t *mask,
+                            uint64_t *full_rows, int64_t *q_rows, int *q_high)
 {
     v3 v0 = ld3(t->v0), v1 = ld3(t->v1), v2 = ld3(t->v2);
     v3 n = cross3(sub3(v1, v0), sub3(v2, v1));
@@ -281,37 +320,53 @@ static inline int pair_test(const pair_ctx *c, v3 Q, const tri_rec *t, uint32_t 
     plane_disc(&A1, &B1, &C1, v1, v2, Q, t0, t1, L0Q);
     plane_disc(&A2, &B2, &C2, v2, v0, Q, t0, t1, L0Q);
 
-    const unsigned nm1 = (unsigned)(c->N - 1);
-    const uint32_t FULL = c->full;
-    uint32_t N0 = row_mask_raw((B0 > 0 ? B0 * (float)nm1 : 0.0f) + C0, A0, nm1, FULL);
-    uint32_t N1 = row_mask_raw((B1 > 0 ? B1 * (float)nm1 : 0.0f) + C1, A1, nm1, FULL);
-    uint32_t N2 = row_mask_raw((B2 > 0 ? B2 * (float)nm1 : 0.0f) + C2, A2, nm1, FULL);
-    uint32_t rows = N0 & N1 & N2;
-    if (rows & ~FULL) ++*q_rows;
-    rows &= FULL & ~*full_rows;
+    const unsigned nrm1 = (unsigned)(c->NR - 1), ncm1 = (unsigned)(c->NC - 1);
+    const uint64_t FR = c->fullr, FC = c->fullc;
+    const int bits = c->bits;
+    uint64_t N0 = row_mask_raw((B0 > 0 ? B0 * (float)ncm1 : 0.0f) + C0, A0, nrm1, FR, bits);
+    uint64_t N1 = row_mask_raw((B1 > 0 ? B1 * (float)ncm1 : 0.0f) + C1, A1, nrm1, FR, bits);
+    uint64_t N2 = row_mask_raw((B2 > 0 ? B2 * (float)ncm1 : 0.0f) + C2, A2, nrm1, FR, bits);
+    uint64_t rows = N0 & N1 & N2;
+    if (rows & ~FR) ++*q_rows;
+    /* the triangle's own plane: -n . (L - v0) >= 0 in the same orientation as
+     * the edges, i.e. the light sample lies on the far side of the triangle */
+    const int dp = c->depth && (t->minz <= 0.0f || t->maxz >= spZ);
+    float A3 = 0.0f, B3 = 0.0f, C3 = 0.0f;
+    if (dp) {
+        v3 m = mk3(-n.x, -n.y, -n.z);
+        v3 lv = sub3(L0, v0);
+        if (dir < 0) lv = mul3(lv, -1.0f);
+        A3 = dot3(m, t0);
+        B3 = dot3(m, t1);
+        C3 = dot3(m, lv);
+        rows &= row_mask_raw((B3 > 0 ? B3 * (float)ncm1 : 0.0f) + C3, A3, nrm1, FR, bits);
+    }
+    rows &= FR & ~*full_rows;
     while (rows) {
-        int r = __builtin_ctz(rows);
+        int r = __builtin_ctzll(rows);
         rows &= rows - 1u;
         ++tl_rows;
-        uint32_t M0 = row_mask_raw(A0 * (float)r + C0, B0, nm1, FULL);
-        uint32_t M1 = row_mask_raw(A1 * (float)r + C1, B1, nm1, FULL);
-        uint32_t M2 = row_mask_raw(A2 * (float)r + C2, B2, nm1, FULL);
-        uint32_t m = M0 & M1 & M2;
-        if (m & ~FULL) *q_high = 1;
-        mask[r] |= m & FULL;
-        if (mask[r] == FULL) *full_rows |= 1u << r;
+        uint64_t M0 = row_mask_raw(A0 * (float)r + C0, B0, ncm1, FC, bits);
+        uint64_t M1 = row_mask_raw(A1 * (float)r + C1, B1, ncm1, FC, bits);
+        uint64_t M2 = row_mask_raw(A2 * (float)r + C2, B2, ncm1, FC, bits);
+        uint64_t m = M0 & M1 & M2;
+        if (m & ~FC) *q_high = 1;
+        if (dp) m &= row_mask_raw(A3 * (float)r + C3, B3, ncm1, FC, bits);
+        mask[r] |= m & FC;
+        if (mask[r] == FC) *full_rows |= (uint64_t)1 << r;
     }
     return 1;
 }
 
-static void pack_mask(const uint32_t *rows, int N, uint32_t *out)
+/* rows[NR] of NC bits -> bit r * NC + c, LSB first */
+static void pack_mask(const uint64_t *rows, int NR, int NC, uint32_t *out)
 {
-    int words = orc_mask_words(N);
+    int words = orc_mask_words_rc(NR, NC);
     memset(out, 0, sizeof(uint32_t) * words);
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j)
+    for (int i = 0; i < NR; ++i)
+        for (int j = 0; j < NC; ++j)
             if ((rows[i] >> j) & 1u) {
-                int b = i * N + j;
+                int b = i * NC + j;
                 out[b >> 5] |= 1u << (b & 31);
             }
 }
@@ -363,9 +418,9 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
     const orc_light *L = in->light;
     const float *M = L->mat;
     const int W = in->W, H = in->H, S = W * H, T = in->T, V = in->V;
-    const int N = L->resW;
-    const int words = orc_mask_words(N);
-    if (W <= 0 || H <= 0 || N < 1 || N > 32 || L->resH != N || in->bins < 1) return -1;
+    const int NR = L->resW, NC = L->resH;
+    const int words = orc_mask_words_rc(NR, NC);
+    if (W <= 0 || H <= 0 || NR < 1 || NR > 64 || NC < 1 || NC > 64 || in->bins < 1) return -1;
 #ifdef _OPENMP
     if (in->nthreads > 0) omp_set_num_threads(in->nthreads);
 #endif
@@ -430,9 +485,9 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
                 backface[s] = 1;
                 if (o->shadow) o->shadow[s] = 1.0f;
                 if (o->masks) {
-                    uint32_t rows[32];
-                    for (int i = 0; i < N; ++i) rows[i] = L->fullBits;
-                    pack_mask(rows, N, o->masks + (size_t)s * words);
+                    uint64_t rows[64];
+                    for (int i = 0; i < NR; ++i) rows[i] = L->fullCols;
+                    pack_mask(rows, NR, NC, o->masks + (size_t)s * words);
                 }
             } else {
                 ++nvalid;
@@ -670,12 +725,7 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
     {
         const double t_occ0 = wall_s();
         pair_ctx c;
-        memcpy(c.ur, L->upRight, sizeof(c.ur));
-        memcpy(c.xd, L->x_delt, sizeof(c.xd));
-        memcpy(c.yd, L->y_delt, sizeof(c.yd));
-        c.N = N;
-        c.full = L->fullBits;
-        c.esp = in->esp;
+        pair_ctx_init(&c, L, in->esp, in->depth_plane);
         const int Sv = o->valid_samples;
         const int stride = in->occ_stride > 1 ? in->occ_stride : 1;
         int64_t tested = 0, qrows = 0, qhigh = 0, nrows = 0, npart = 0;
@@ -689,11 +739,11 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
             v3 Q = ld3(in->pos + 4 * s);
             float spx = rb[3 * s], spy = rb[3 * s + 1], spz = re[3 * s], spw = re[3 * s + 1];
             float spZ = re[3 * s + 2];
-            uint32_t rows[32];
+            uint64_t rows[64];
             memset(rows, 0, sizeof(rows));
-            uint32_t full_rows = 0;
+            uint64_t full_rows = 0;
             int high = 0;
-            for (int p = tstart[bin]; p < tend[bin] && full_rows != c.full; ++p) {
+            for (int p = tstart[bin]; p < tend[bin] && full_rows != c.fullr; ++p) {
                 const tri_rec *t = &rec[sptri[p]];
                 if (in->shadow_method == 1) {
                     /* refCal's pre-cull: rectangle containment, and the depth test
@@ -709,15 +759,15 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *o)
                       spw <= t->bmax[1] && t->minz <= spZ))
                     continue;
                 ++tested;
-                pair_test(&c, Q, t, rows, &full_rows, &qrows, &high);
+                pair_test(&c, Q, spZ, t, rows, &full_rows, &qrows, &high);
             }
             qhigh += high;
             nrows += tl_rows;
             npart += tl_partial;
             int cnt = 0;
-            for (int i = 0; i < N; ++i) cnt += __builtin_popcount(rows[i]);
-            if (o->shadow) o->shadow[s] = (float)cnt / (float)(N * N);
-            if (o->masks) pack_mask(rows, N, o->masks + s * words);
+            for (int i = 0; i < NR; ++i) cnt += __builtin_popcountll(rows[i]);
+            if (o->shadow) o->shadow[s] = (float)cnt / (float)(NR * NC);
+            if (o->masks) pack_mask(rows, NR, NC, o->masks + s * words);
         }
         o->pairs_tested = tested;
         o->quirk_rows_beyond_n = qrows;
@@ -782,19 +832,14 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
                             const int32_t *sample_ids, int32_t n, uint32_t *masks)
 {
     const orc_light *L = in->light;
-    const int N = L->resW, words = orc_mask_words(N);
+    const int NR = L->resW, NC = L->resH, words = orc_mask_words_rc(NR, NC);
     memset(masks, 0, sizeof(uint32_t) * (size_t)n * words);
     if (fr->state < 2) return 0;
     tri_rec *recs = NULL;
     int nt = build_tri_list(in, fr, &recs);
     if (nt < 0) return -1;
     pair_ctx c;
-    memcpy(c.ur, L->upRight, sizeof(c.ur));
-    memcpy(c.xd, L->x_delt, sizeof(c.xd));
-    memcpy(c.yd, L->y_delt, sizeof(c.yd));
-    c.N = N;
-    c.full = L->fullBits;
-    c.esp = in->esp;
+    pair_ctx_init(&c, L, in->esp, in->depth_plane);
     const float *M = L->mat;
     const float Bx = fr->lp_begin[0], By = fr->lp_begin[1], Ex = fr->lp_end[0], Ey = fr->lp_end[1];
     v3 ur = ld3(L->upRight), ul = ld3(L->upLeft), dl = ld3(L->downLeft), dr = ld3(L->downRight);
@@ -810,9 +855,9 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
         v3 p = ld3(pp), nv = ld3(nn);
         if (dot3(sub3(ur, p), nv) <= 0 && dot3(sub3(ul, p), nv) <= 0 &&
             dot3(sub3(dl, p), nv) <= 0 && dot3(sub3(dr, p), nv) <= 0) {
-            uint32_t rows[32];
-            for (int i = 0; i < N; ++i) rows[i] = c.full;
-            pack_mask(rows, N, masks + (size_t)k * words);
+            uint64_t rows[64];
+            for (int i = 0; i < NR; ++i) rows[i] = c.fullc;
+            pack_mask(rows, NR, NC, masks + (size_t)k * words);
             continue;
         }
         v3 r = make_rect(M, p);
@@ -821,20 +866,20 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
         float spZ = r.z;
         /* same validity as the sample key pass, K/Step3_bindSampleToBin.inl:35-38 */
         if ((spx > spz || spy > spw) || (spx < Bx || spy < By || spz > Ex || spw > Ey)) continue;
-        uint32_t rows[32];
+        uint64_t rows[64];
         memset(rows, 0, sizeof(rows));
-        uint32_t full_rows = 0;
+        uint64_t full_rows = 0;
         int64_t qr = 0;
         int hi = 0;
-        for (int t = 0; t < nt && full_rows != c.full; ++t) {
+        for (int t = 0; t < nt && full_rows != c.fullr; ++t) {
             const tri_rec *tr = &recs[t];
             if (!(tr->bmin[0] <= spx && tr->bmin[1] <= spy && spz <= tr->bmax[0] &&
                   spw <= tr->bmax[1] && tr->minz <= spZ))
                 continue;
             ++tested;
-            pair_test(&c, p, tr, rows, &full_rows, &qr, &hi);
+            pair_test(&c, p, spZ, tr, rows, &full_rows, &qr, &hi);
         }
-        pack_mask(rows, N, masks + (size_t)k * words);
+        pack_mask(rows, NR, NC, masks + (size_t)k * words);
     }
     free(recs);
     return tested;
@@ -842,14 +887,16 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
 
 /* O3: FP64 exhaustive per-light-sample test.  Same sample validity, same
  * triangle set (FP32 back-face predicate), same orientation and self-skip rules;
- * every light sample (i, j) at L0 + i*x_delt + j*y_delt is occluded iff all
- * three oriented edge functions are >= 0, evaluated in double. */
+ * every light sample (i, j) at L0 + i*x_delt + j*y_delt (i < resW, j < resH) is
+ * occluded iff all three oriented edge functions are >= 0 -- with depth_plane,
+ * and the triangle's max depth not below the sample's, also the oriented
+ * triangle plane -- evaluated in double. */
 void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                          const int32_t *sample_ids, int32_t n, uint32_t *masks,
                          double *edge_dist)
 {
     const orc_light *L = in->light;
-    const int N = L->resW, words = orc_mask_words(N), NN = N * N;
+    const int NR = L->resW, NC = L->resH, words = orc_mask_words_rc(NR, NC), NN = NR * NC;
     memset(masks, 0, sizeof(uint32_t) * (size_t)n * words);
     for (size_t i = 0; i < (size_t)n * NN; ++i) edge_dist[i] = 1e300;
     if (fr->state < 2) return;
@@ -918,7 +965,8 @@ void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                 if (!(d12 < 0.0) && !(d23 < 0.0)) continue;
             }
             double sg = dir < 0 ? -1.0 : 1.0;
-            double A[3], B[3], C[3], inv[3];
+            double A[4], B[4], C[4], inv[4];
+            const int planes = (in->depth_plane && (tr->minz <= 0.0f || tr->maxz >= r.z)) ? 4 : 3;
             for (int e = 0; e < 3; ++e) {
                 const double *a = V[e], *b = V[(e + 1) % 3];
                 double u[3] = {b[0] - Q[0], b[1] - Q[1], b[2] - Q[2]};
@@ -931,14 +979,23 @@ void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                 double g = sqrt(A[e] * A[e] + B[e] * B[e]);
                 inv[e] = g > 0 ? 1.0 / g : 1e300;
             }
-            for (int i = 0; i < N; ++i)
-                for (int j = 0; j < N; ++j) {
+            if (planes == 4) {
+                /* -n . (L - v0), oriented like the edges */
+                double lv[3] = {L0[0] - V[0][0], L0[1] - V[0][1], L0[2] - V[0][2]};
+                A[3] = -sg * (nrm[0] * XD[0] + nrm[1] * XD[1] + nrm[2] * XD[2]);
+                B[3] = -sg * (nrm[0] * YD[0] + nrm[1] * YD[1] + nrm[2] * YD[2]);
+                C[3] = -sg * (nrm[0] * lv[0] + nrm[1] * lv[1] + nrm[2] * lv[2]);
+                double g = sqrt(A[3] * A[3] + B[3] * B[3]);
+                inv[3] = g > 0 ? 1.0 / g : 1e300;
+            }
+            for (int i = 0; i < NR; ++i)
+                for (int j = 0; j < NC; ++j) {
                     double mn = 1e300;
-                    for (int e = 0; e < 3; ++e) {
+                    for (int e = 0; e < planes; ++e) {
                         double v = (A[e] * i + B[e] * j + C[e]) * inv[e];
                         if (v < mn) mn = v;
                     }
-                    int b = i * N + j;
+                    int b = i * NC + j;
                     if (mn >= 0.0) mk[b >> 5] |= 1u << (b & 31);
                     double mg = fabs(mn);
                     if (mg < ed[b]) ed[b] = mg;

@@ -48,6 +48,9 @@ typedef struct {
     float upRight[3], downLeft[3], upLeft[3], downRight[3];
     float mat[16];
     float RF[2];
+    /* light grid as the occlusion stage sees it: rows along x_delt (resW of them),
+     * columns along y_delt (resH); bit r * resH + c of a sample's mask */
+    uint64_t fullRows, fullCols;
 } orc_light;
 
 typedef struct {
@@ -68,6 +71,10 @@ typedef struct {
                                     exhaustive baselines, which rebuild their triangle list */
     int32_t shadow_method;       /* 0: edge-function row masks (K/Step5_2_shadowCalPerSample.inl);
                                     1: the reference's ray-cast check (K/Step5_2_calRef.inl) */
+    int32_t depth_plane;         /* 1: edge-function masks also test the triangle's own plane
+                                    (light samples on Q's side of it are not occluded) for
+                                    triangles that reach the light plane (min depth <= 0) or
+                                    the sample's depth (max depth >= the sample's) */
 } orc_frame_in;
 
 typedef struct {
@@ -102,6 +109,8 @@ typedef struct {
 } orc_frame_out;
 
 int32_t orc_mask_words(int32_t N);
+/* mask words of a rows x cols light grid (rows = lightResWidth, cols = lightResHeight) */
+int32_t orc_mask_words_rc(int32_t rows, int32_t cols);
 void orc_light_setup(const orc_light_desc *d, orc_light *out);
 /* returns 0 on success, negative on bad input / allocation failure */
 int32_t orc_frame(const orc_frame_in *in, orc_frame_out *out);
@@ -116,7 +125,7 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
 /* Exhaustive FP64 per-light-sample edge test (O3).  For each listed sample:
  * masks[n * words] and min_dist[n * N * N] = min over edges of the FP64
  * distance (light-grid units) from each light sample to the nearest projected
- * edge of any triangle that decides it. */
+ * edge of any triangle that decides it (n * rows * cols values). */
 void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                          const int32_t *sample_ids, int32_t n, uint32_t *masks,
                          double *edge_dist);

@@ -32,7 +32,8 @@ class Light(ctypes.Structure):
                 ("x_delt", ctypes.c_float * 3), ("y_delt", ctypes.c_float * 3),
                 ("upRight", ctypes.c_float * 3), ("downLeft", ctypes.c_float * 3),
                 ("upLeft", ctypes.c_float * 3), ("downRight", ctypes.c_float * 3),
-                ("mat", ctypes.c_float * 16), ("RF", ctypes.c_float * 2)]
+                ("mat", ctypes.c_float * 16), ("RF", ctypes.c_float * 2),
+                ("fullRows", ctypes.c_uint64), ("fullCols", ctypes.c_uint64)]
 
 
 class FrameIn(ctypes.Structure):
@@ -41,7 +42,7 @@ class FrameIn(ctypes.Structure):
                 ("idx", i32p), ("T", ctypes.c_int32), ("bins", ctypes.c_int32), ("cull", ctypes.c_int32),
                 ("esp", ctypes.c_float), ("light", ctypes.POINTER(Light)), ("nthreads", ctypes.c_int32),
                 ("occ_stride", ctypes.c_int32), ("setup_only", ctypes.c_int32),
-                ("shadow_method", ctypes.c_int32)]
+                ("shadow_method", ctypes.c_int32), ("depth_plane", ctypes.c_int32)]
 
 
 class FrameOut(ctypes.Structure):
@@ -93,8 +94,8 @@ def load() -> ctypes.CDLL:
     return lib
 
 
-def mask_words(n: int) -> int:
-    return (n * n + 31) // 32
+def mask_words(n: int, cols: int | None = None) -> int:
+    return (n * (cols if cols else n) + 31) // 32
 
 
 def _p(a: np.ndarray, t):
@@ -109,7 +110,7 @@ def light_desc(light) -> LightDesc:
     d.viewDir[:] = list(light.view_dir)
     d.upDir[:] = list(light.up_dir)
     d.lightResWidth = light.n
-    d.lightResHeight = light.n
+    d.lightResHeight = light.cols
     return d
 
 
@@ -150,6 +151,7 @@ def _frame_in(scene, light: Light, nthreads: int, keep: list, occ_stride: int = 
     fi.light = ctypes.pointer(light)
     fi.nthreads = nthreads
     fi.occ_stride = occ_stride
+    fi.depth_plane = int(bool(getattr(scene, "depth_plane", False)))
     return fi
 
 
@@ -179,7 +181,7 @@ def frame(scene, nthreads: int = 0, pair_capacity: int | None = None, occ_stride
                 sc[name] = list(v)
         return OrcFrame(scalars=sc, arrays={}, _in=fi, _out=fo, _keep=keep)
     S, T, NB = scene.W * scene.H, scene.T, scene.bins * scene.bins
-    words = mask_words(scene.light.n)
+    words = mask_words(scene.light.n, scene.light.cols)
     # first a counting run to size the pair buffers
     arrs = dict(
         keys=np.zeros(S, np.int32), vals=np.zeros(S, np.int32), sorted_keys=np.zeros(S, np.int32),
@@ -234,7 +236,7 @@ def exhaustive_fp32(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int =
     Returns (masks [n, words], pair tests executed)."""
     lib = load()
     ids = np.ascontiguousarray(sample_ids, dtype=np.int32)
-    words = mask_words(scene.light.n)
+    words = mask_words(scene.light.n, scene.light.cols)
     out = np.zeros(ids.size * words, np.uint32)
     fr._in.nthreads = nthreads
     n = lib.orc_exhaustive_fp32(ctypes.byref(fr._in), ctypes.byref(fr._out), _p(ids, i32p), ids.size,
@@ -243,14 +245,15 @@ def exhaustive_fp32(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int =
 
 
 def exhaustive_fp64(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int = 0):
-    """O3: FP64 per-light-sample test.  Returns (masks [n, words], edge distance [n, N*N])."""
+    """O3: FP64 per-light-sample test.  Returns (masks [n, words], edge distance
+    [n, rows * cols])."""
     lib = load()
     ids = np.ascontiguousarray(sample_ids, dtype=np.int32)
-    N = scene.light.n
-    words = mask_words(N)
+    NN = scene.light.rows * scene.light.cols
+    words = mask_words(scene.light.n, scene.light.cols)
     out = np.zeros(ids.size * words, np.uint32)
-    dist = np.zeros(ids.size * N * N, np.float64)
+    dist = np.zeros(ids.size * NN, np.float64)
     fr._in.nthreads = nthreads
     lib.orc_exhaustive_fp64(ctypes.byref(fr._in), ctypes.byref(fr._out), _p(ids, i32p), ids.size,
                             _p(out, u32p), dist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
-    return out.reshape(ids.size, words), dist.reshape(ids.size, N * N)
+    return out.reshape(ids.size, words), dist.reshape(ids.size, NN)

@@ -82,8 +82,9 @@ def preflight(scene, occ_stride: int = 64) -> dict:
     from . import orc
 
     n = scene.light.n
-    if not (1 < n <= 32):
-        raise PreflightError(f"light grid {n} x {n}: the per-sample kernel runs 2..32 square grids only")
+    if scene.light.cols != n or not (1 < n <= 32):
+        raise PreflightError(f"light grid {n} x {scene.light.cols}: the per-sample kernel runs 2..32 "
+                             "square grids only")
     s16 = dataclasses.replace(scene, bins=REF_BINS)
     fr = orc.frame(s16, occ_stride=occ_stride)
     sc = fr.scalars

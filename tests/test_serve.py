@@ -168,8 +168,8 @@ def test_bad_requests_fail_at_submission(cuda_ok, fdzb, scenes):
     with pytest.raises(fdzb.FdzbError):
         srv.submit(bad)
     bad = _req(fdzb, views, r, sh, mk)
-    bad.light.lightResWidth = 64
-    bad.light.lightResHeight = 64
+    bad.light.lightResWidth = 65       # grids are limited to 64 x 64
+    bad.light.lightResHeight = 8
     with pytest.raises(fdzb.FdzbError):
         srv.submit(bad)
     srv.close()
