@@ -59,6 +59,8 @@ EXPORTED = [
     "fdzb_ctx_set_occlusion_schedule", "fdzb_batch_set_occlusion_schedule", "fdzb_ctx_set_pair_capacity_limit",
     "fdzb_ctx_set_model_transform", "fdzb_ctx_set_shadow_method", "fdzb_light_sample_positions", "fdzb_shade",
     "fdzb_ctx_set_depth_plane", "fdzb_batch_set_depth_plane",
+    "fdzb_raster_create", "fdzb_raster_destroy", "fdzb_raster_set_stream", "fdzb_raster_draw",
+    "fdzb_raster_sync", "fdzb_raster_get_stats",
     "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
@@ -191,6 +193,25 @@ class ShadeDesc(ctypes.Structure):
                 ("d_light_samples", ctypes.c_void_p)]
 
 
+class RasterDesc(ctypes.Structure):
+    """fdzb_raster_desc."""
+    _fields_ = [("d_vtx", ctypes.c_void_p), ("n_vtx", ctypes.c_int32), ("vtx_stride_bytes", ctypes.c_int32),
+                ("pos_offset", ctypes.c_int32), ("nrm_offset", ctypes.c_int32), ("d_idx", ctypes.c_void_p),
+                ("n_tri", ctypes.c_int32), ("d_tri_material", ctypes.c_void_p), ("d_materials", ctypes.c_void_p),
+                ("n_materials", ctypes.c_int32), ("model", ctypes.c_float * 16), ("view_proj", ctypes.c_float * 16),
+                ("W", ctypes.c_int32), ("H", ctypes.c_int32), ("clear", ctypes.c_int32), ("d_g0", ctypes.c_void_p),
+                ("d_g1", ctypes.c_void_p), ("d_g2", ctypes.c_void_p), ("d_g3", ctypes.c_void_p),
+                ("d_depth", ctypes.c_void_p)]
+
+
+class RasterStats(ctypes.Structure):
+    """fdzb_raster_stats."""
+    _fields_ = [("triangles", ctypes.c_int64), ("sub_triangles", ctypes.c_int64), ("dropped", ctypes.c_int64),
+                ("tile_pairs", ctypes.c_int64), ("bad_indices", ctypes.c_int64), ("bad_materials", ctypes.c_int64),
+                ("tiles_x", ctypes.c_int32), ("tiles_y", ctypes.c_int32), ("ms", ctypes.c_float),
+                ("pad", ctypes.c_float)]
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -240,6 +261,9 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
         "fdzb_ctx_set_shadow_method": ([vp, i32], i32),
         "fdzb_ctx_set_depth_plane": ([vp, i32], i32), "fdzb_batch_set_depth_plane": ([vp, i32], i32),
+        "fdzb_raster_create": ([P(vp), i32], i32), "fdzb_raster_destroy": ([vp], i32),
+        "fdzb_raster_set_stream": ([vp, vp], i32), "fdzb_raster_draw": ([vp, P(RasterDesc)], i32),
+        "fdzb_raster_sync": ([vp], i32), "fdzb_raster_get_stats": ([vp, P(RasterStats)], i32),
         "fdzb_light_sample_positions": ([P(AreaLightDesc), P(ctypes.c_float)], i32),
         "fdzb_shade": ([P(ShadeDesc), vp], i32), "fdzb_batch_set_occlusion_schedule": ([vp, i32], i32),
         "fdzb_batch_create": ([P(vp), i32], i32), "fdzb_batch_destroy": ([vp], i32),
@@ -781,3 +805,66 @@ def shade(W: int, H: int, g0, g1, g2, g3, shadow, rgba, camera_pos, La, Ld, Ls, 
     d.n_light_samples = int(light_samples.shape[0])
     d.d_light_samples = _ptr(light_samples)
     _check(load().fdzb_shade(ctypes.byref(d), ctypes.c_void_p(stream)))
+
+
+# ---- G-buffer rasteriser ---------------------------------------------------
+
+
+def _mat16_list(m) -> list:
+    return [float(v) for v in np.asarray(m, dtype=np.float32).reshape(-1, order="F")] if np.asarray(m).ndim == 2 \
+        else [float(v) for v in np.asarray(m, dtype=np.float32).reshape(16)]
+
+
+def raster_desc(vtx, n_vtx: int, idx, n_tri: int, materials, n_materials: int, model, view_proj, W: int, H: int,
+                g0, g1, g2=None, g3=None, depth=None, clear: bool = True, tri_material=None,
+                stride_bytes: int = 32, pos_offset: int = 0, nrm_offset: int = 5) -> RasterDesc:
+    """fdzb_raster_desc from device tensors (or pointers).  model / view_proj:
+    4x4 matrices (numpy, mathematical row/column convention; stored column-major)
+    or 16 floats already column-major."""
+    d = RasterDesc()
+    d.d_vtx, d.n_vtx, d.vtx_stride_bytes = _ptr(vtx), int(n_vtx), int(stride_bytes)
+    d.pos_offset, d.nrm_offset = int(pos_offset), int(nrm_offset)
+    d.d_idx, d.n_tri = _ptr(idx), int(n_tri)
+    d.d_tri_material = _ptr(tri_material)
+    d.d_materials, d.n_materials = _ptr(materials), int(n_materials)
+    d.model[:] = _mat16_list(model)
+    d.view_proj[:] = _mat16_list(view_proj)
+    d.W, d.H, d.clear = int(W), int(H), int(bool(clear))
+    d.d_g0, d.d_g1, d.d_g2, d.d_g3 = _ptr(g0), _ptr(g1), _ptr(g2), _ptr(g3)
+    d.d_depth = _ptr(depth)
+    return d
+
+
+class Raster:
+    """fdzb_raster_*: the G-buffer rasteriser (the app's GL pass 0)."""
+
+    def __init__(self, device: int = -1):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        _check(self._lib.fdzb_raster_create(ctypes.byref(h), int(device)))
+        self._h = h
+
+    def set_stream(self, stream) -> None:
+        _check(self._lib.fdzb_raster_set_stream(self._h, ctypes.c_void_p(stream)))
+
+    def draw(self, desc: RasterDesc) -> None:
+        _check(self._lib.fdzb_raster_draw(self._h, ctypes.byref(desc)))
+
+    def sync(self) -> None:
+        _check(self._lib.fdzb_raster_sync(self._h))
+
+    def stats(self) -> dict:
+        st = RasterStats()
+        _check(self._lib.fdzb_raster_get_stats(self._h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_ if name != "pad"}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.fdzb_raster_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

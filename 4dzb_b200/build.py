@@ -17,7 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfdzb.so")
 
-SOURCES = ["fdzb_pipeline.cu", "fdzb_shade.cu", "fdzb_api.cpp", "fdzb_serve.cpp", "fdzb_light.cpp"]
+SOURCES = ["fdzb_pipeline.cu", "fdzb_shade.cu", "fdzb_raster.cu", "fdzb_api.cpp", "fdzb_serve.cpp",
+           "fdzb_light.cpp"]
 HEADERS = ["fdzb_internal.h", "fdzb_engine.h", "fdzb_device.cuh", "fdzb_sort.cuh", "fdzb_occlusion.cuh"]
 
 NVCC_FLAGS = [

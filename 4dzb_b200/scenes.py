@@ -175,3 +175,100 @@ def batch_frame(k: int, s_range=(256 * 256, 1920 * 1080), t_range=(10_000, 500_0
     s = make_scene(W, H, T, n=n, bins=0, seed=seed, sigma=0.1, zlo=0.5, zhi=3.0, radius=side / 2.0,
                    name=f"batch{k}")
     return s
+
+
+# ---- meshes for the G-buffer rasteriser ------------------------------------
+
+def look_at(eye, center, up) -> np.ndarray:
+    """gluLookAt view matrix (out = M @ v), float64."""
+    e, c, u = (np.asarray(v, np.float64) for v in (eye, center, up))
+    f = c - e
+    f /= np.linalg.norm(f)
+    s = np.cross(f, u)
+    s /= np.linalg.norm(s)
+    uu = np.cross(s, f)
+    m = np.eye(4)
+    m[0, :3], m[1, :3], m[2, :3] = s, uu, -f
+    m[:3, 3] = -m[:3, :3] @ e
+    return m
+
+
+def perspective(fovy_deg: float, aspect: float, near: float, far: float) -> np.ndarray:
+    """gluPerspective projection matrix (out = M @ v), float64."""
+    f = 1.0 / np.tan(np.radians(fovy_deg) / 2.0)
+    m = np.zeros((4, 4))
+    m[0, 0], m[1, 1] = f / aspect, f
+    m[2, 2], m[2, 3] = (far + near) / (near - far), 2.0 * far * near / (near - far)
+    m[3, 2] = -1.0
+    return m
+
+
+@dataclass
+class MeshScene:
+    """Triangle meshes in the MeshManager vertex layout (8 floats: position,
+    texcoord, normal) with per-triangle materials, a camera and an area light.
+    Triangles [0, n_receiver) are the receiver surface (the app's mesh 0, which
+    it leaves out of the shadow model, MeshManager.cpp:43); the rest occlude."""
+    W: int
+    H: int
+    vtx: np.ndarray            # float32 [V, 8]
+    idx: np.ndarray            # uint32 [T, 3]
+    tri_material: np.ndarray   # int32 [T]
+    materials: np.ndarray      # float32 [M, 10]: Ka, Kd, Ks, shininess
+    model: np.ndarray          # 4x4
+    view_proj: np.ndarray      # 4x4
+    eye: tuple
+    n_receiver: int
+    light: Light
+
+    @property
+    def T(self) -> int:
+        return int(self.idx.shape[0])
+
+
+def mesh_scene(W: int, H: int, grid: int = 48, T: int = 1500, seed: int = 5, sigma: float = 0.15,
+               eye=(0.0, -13.0, 11.0), center=(0.0, 0.0, 0.0), fovy: float = 50.0, near: float = 0.5,
+               far: float = 100.0, n: int = 8) -> MeshScene:
+    """A height-field receiver (z = 0.3 sin x cos y over [-8, 8]^2, grid x grid
+    cells, analytic normals) and T occluder triangles (the soup of occluders()
+    with face normals) seen by a perspective camera; light as make_scene's."""
+    xs = np.linspace(-8.0, 8.0, grid + 1)
+    X, Y = np.meshgrid(xs, xs)
+    Z = 0.3 * np.sin(X) * np.cos(Y)
+    N = np.stack([-0.3 * np.cos(X) * np.cos(Y), 0.3 * np.sin(X) * np.sin(Y), np.ones_like(X)], axis=-1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    rv = np.zeros(((grid + 1) ** 2, 8), np.float64)
+    rv[:, 0], rv[:, 1], rv[:, 2] = X.ravel(), Y.ravel(), Z.ravel()
+    rv[:, 5:8] = N.reshape(-1, 3)
+    i = np.arange(grid)
+    a = (i[:, None] * (grid + 1) + i[None, :]).ravel()
+    quads = np.stack([a, a + 1, a + grid + 2, a + grid + 1], axis=1)
+    ridx = np.concatenate([quads[:, [0, 1, 2]], quads[:, [0, 2, 3]]])
+    ov, oi = occluders(T, seed, sigma, 0.5, 3.0)
+    tri = ov[:, :3].astype(np.float64).reshape(-1, 3, 3)
+    fn = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    fn /= np.maximum(np.linalg.norm(fn, axis=1, keepdims=True), 1e-30)
+    sv = np.zeros((3 * T, 8), np.float64)
+    sv[:, :3] = tri.reshape(-1, 3)
+    sv[:, 5:8] = np.repeat(fn, 3, axis=0)
+    vtx = np.concatenate([rv, sv]).astype(np.float32)
+    idx = np.concatenate([ridx, oi.astype(np.int64) + rv.shape[0]]).astype(np.uint32)
+    mat = np.concatenate([np.zeros(len(ridx), np.int32), np.ones(T, np.int32)])
+    materials = np.array([[0.1, 0.1, 0.1, 0.6, 0.6, 0.55, 0.2, 0.2, 0.2, 16.0],
+                          [0.1, 0.05, 0.05, 0.7, 0.2, 0.2, 0.5, 0.5, 0.5, 32.0]], np.float32)
+    vp = perspective(fovy, W / H, near, far) @ look_at(eye, center, (0.0, 0.0, 1.0))
+    return MeshScene(W=W, H=H, vtx=vtx, idx=idx, tri_material=mat, materials=materials, model=np.eye(4),
+                     view_proj=vp, eye=tuple(eye), n_receiver=len(ridx), light=Light(n=n))
+
+
+def shadow_scene(ms: MeshScene, g0: np.ndarray, g1: np.ndarray, bins: int = 32, cull: bool = False) -> Scene:
+    """The shadow pipeline's input for a rasterised view: samples = the
+    G-buffer's world positions and normals, occluders = the mesh triangles
+    after the receiver, as xyz float4 vertices."""
+    occ = ms.idx[ms.n_receiver:]
+    used = ms.vtx[occ.reshape(-1), :3]
+    vtx = np.ones((used.shape[0], 4), np.float32)
+    vtx[:, :3] = used
+    idx = np.arange(used.shape[0], dtype=np.int32).reshape(-1, 3)
+    return Scene(W=ms.W, H=ms.H, pos=np.ascontiguousarray(g0, np.float32), nrm=np.ascontiguousarray(g1, np.float32),
+                 vtx=vtx, idx=idx, light=ms.light, bins=bins, cull=cull, name="raster")

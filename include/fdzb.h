@@ -307,6 +307,65 @@ typedef struct fdzb_shade_desc {
 /* Enqueued on `stream` (cudaStream_t, NULL = legacy default); no host sync. */
 int fdzb_shade(const fdzb_shade_desc *desc, void *stream);
 
+/* ---- G-buffer rasteriser (the view samples' producer) --------------------- */
+
+/* Replaces the app's GL G-buffer pass (4DZB/Render/Render.cpp:390-431,
+ * DrawModel :267-340, shaders 4DZB/Resources/shader/gatherData.shv/.shf) so
+ * that real meshes feed fdzb_* without a graphics stack.  One draw rasterises a
+ * triangle list (the MeshManager layout, 4DZB/ResourceManager/MeshManager.cpp:
+ * 35-89: 8 floats per vertex, position at 0, texcoord at 3, normal at 5) with
+ * the depth test GL_LESS; per pixel
+ *   g0 = (worldPos, Ks.r)  g1 = (worldN, Ks.g)  g2 = (Ka, Ks.b)  g3 = (Kd, shininess)
+ * with worldPos = model * (P, 1), worldN = model * (N, 0) interpolated
+ * perspective-correctly, and clip = view_proj * (worldPos, 1) -- the gatherData
+ * shaders' outputs, so g0 and g1 are this library's sample position and normal
+ * buffers.  Cleared pixels are NaN (the app's clear colour), depth 1.  Rows run
+ * bottom to top (row 0 is window y = 0, as in the GL textures the app hands to
+ * FDsetSampleGLTex).  The rasterisation rules GL leaves to the implementation
+ * are fixed here: near-plane clipping in clip space (far plane and viewport per
+ * fragment), window coordinates snapped to 1/16 pixel, coverage at pixel
+ * centres with exact 64-bit edge functions and a rule that gives a centre on a
+ * shared edge to exactly one triangle, both windings drawn, ties in depth won
+ * by the earlier triangle.  Textured materials (the shader's NaN colour ->
+ * texture lookup) are not supported: materials are constant colours.
+ * Sub-triangles with a vertex beyond 2^26 pixels of the viewport are dropped
+ * and counted. */
+typedef struct fdzb_raster fdzb_raster;
+typedef struct fdzb_raster_desc {
+    const float *d_vtx;            /* n_vtx vertices, vtx_stride_bytes apart */
+    int32_t n_vtx;
+    int32_t vtx_stride_bytes;      /* multiple of 4; 32 for the MeshManager layout */
+    int32_t pos_offset, nrm_offset;/* in floats: 0 and 5 for the MeshManager layout */
+    const uint32_t *d_idx;         /* 3 per triangle */
+    int32_t n_tri;
+    const int32_t *d_tri_material; /* nullable: every triangle uses material 0 */
+    const float *d_materials;      /* n_materials x 10 floats: Ka rgb, Kd rgb, Ks rgb, shininess */
+    int32_t n_materials;
+    float model[16];               /* column-major modelMatrix */
+    float view_proj[16];           /* column-major ViewAndPerspectiveMatrix */
+    int32_t W, H;                  /* 1..16384 */
+    int32_t clear;                 /* 1: clear the G-buffer (NaN) and depth (1) first; 0: draw on
+                                      top of an earlier draw (needs the same d_depth) */
+    float *d_g0, *d_g1;            /* float4[W*H], 16-byte aligned */
+    float *d_g2, *d_g3;            /* nullable float4[W*H] */
+    float *d_depth;                /* float[W*H] window depth; nullable only with clear */
+} fdzb_raster_desc;
+typedef struct fdzb_raster_stats {
+    int64_t triangles, sub_triangles, dropped, tile_pairs, bad_indices, bad_materials;
+    int32_t tiles_x, tiles_y;
+    float ms;                      /* last draw, device time */
+    float pad;
+} fdzb_raster_stats;
+int fdzb_raster_create(fdzb_raster **out, int device);
+int fdzb_raster_destroy(fdzb_raster *r);
+/* stream: a cudaStream_t; NULL = the rasteriser's own stream. */
+int fdzb_raster_set_stream(fdzb_raster *r, void *stream);
+/* Enqueues one draw.  Waits once on the stream for the tile-list size, then
+ * returns with the rasterisation in flight; fdzb_raster_sync waits for it. */
+int fdzb_raster_draw(fdzb_raster *r, const fdzb_raster_desc *desc);
+int fdzb_raster_sync(fdzb_raster *r);
+int fdzb_raster_get_stats(fdzb_raster *r, fdzb_raster_stats *stats);
+
 /* Library version string. */
 const char *fdzb_version(void);
 

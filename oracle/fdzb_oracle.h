@@ -130,6 +130,27 @@ void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                          const int32_t *sample_ids, int32_t n, uint32_t *masks,
                          double *edge_dist);
 
+/* G-buffer rasteriser oracle (fdzb_raster_oracle.c): one draw. */
+typedef struct {
+    const float *vtx;            /* V vertices of vtx_stride_floats floats */
+    int32_t vtx_stride_floats, pos_offset, nrm_offset;
+    const uint32_t *idx;         /* 3 per triangle */
+    int32_t n_tri;
+    const int32_t *tri_material; /* nullable: material 0 */
+    const float *materials;      /* 10 floats each: Ka, Kd, Ks, shininess */
+    float model[16], view_proj[16];  /* column-major */
+    int32_t W, H;
+    int32_t clear;               /* 1: G-buffers to NaN, depth to 1 first */
+} orc_raster_in;
+
+typedef struct {
+    float *g0, *g1, *g2, *g3;    /* float4[W*H] (g2, g3 nullable), row 0 = bottom */
+    float *depth;                /* float[W*H] */
+    int64_t sub_tris, dropped;
+} orc_raster_out;
+
+int32_t orc_raster(const orc_raster_in *in, orc_raster_out *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,7 +72,7 @@ def load() -> ctypes.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    src = [os.path.join(HERE, f) for f in ("fdzb_oracle.c", "fdzb_oracle.h", "Makefile")]
+    src = [os.path.join(HERE, f) for f in ("fdzb_oracle.c", "fdzb_raster_oracle.c", "fdzb_oracle.h", "Makefile")]
     if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in src):
         env = dict(os.environ)
         env.pop("CC", None)
@@ -257,3 +257,63 @@ def exhaustive_fp64(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int =
     lib.orc_exhaustive_fp64(ctypes.byref(fr._in), ctypes.byref(fr._out), _p(ids, i32p), ids.size,
                             _p(out, u32p), dist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     return out.reshape(ids.size, words), dist.reshape(ids.size, NN)
+
+
+# ---- G-buffer rasteriser oracle (fdzb_raster_oracle.c) ----------------------
+
+class RasterIn(ctypes.Structure):
+    _fields_ = [("vtx", f32p), ("vtx_stride_floats", ctypes.c_int32), ("pos_offset", ctypes.c_int32),
+                ("nrm_offset", ctypes.c_int32), ("idx", u32p), ("n_tri", ctypes.c_int32), ("tri_material", i32p),
+                ("materials", f32p), ("model", ctypes.c_float * 16), ("view_proj", ctypes.c_float * 16),
+                ("W", ctypes.c_int32), ("H", ctypes.c_int32), ("clear", ctypes.c_int32)]
+
+
+class RasterOut(ctypes.Structure):
+    _fields_ = [("g0", f32p), ("g1", f32p), ("g2", f32p), ("g3", f32p), ("depth", f32p),
+                ("sub_tris", ctypes.c_int64), ("dropped", ctypes.c_int64)]
+
+
+def col_major(m) -> list:
+    """A 4x4 matrix (out = m @ v) as 16 column-major floats."""
+    return [float(v) for v in np.asarray(m, dtype=np.float32).reshape(4, 4).reshape(-1, order="F")]
+
+
+def raster(vtx, idx, materials, model, view_proj, W: int, H: int, tri_material=None, clear: bool = True,
+           prev: dict | None = None, pos_offset: int = 0, nrm_offset: int = 5) -> dict:
+    """One draw through the rasteriser oracle.  vtx: float32 [V, floats per
+    vertex]; idx: [T, 3]; materials: float32 [M, 10].  With clear=False, `prev`
+    holds the earlier draw's g0..g3 and depth, which are drawn over."""
+    lib = load()
+    if not hasattr(lib, "_raster_ready"):
+        lib.orc_raster.argtypes = [ctypes.POINTER(RasterIn), ctypes.POINTER(RasterOut)]
+        lib.orc_raster.restype = ctypes.c_int32
+        lib._raster_ready = True
+    vtx = np.ascontiguousarray(vtx, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+    mats = np.ascontiguousarray(materials, np.float32).reshape(-1, 10)
+    S = W * H
+    if clear or prev is None:
+        out = {k: np.zeros((S, 4), np.float32) for k in ("g0", "g1", "g2", "g3")}
+        out["depth"] = np.zeros(S, np.float32)
+    else:
+        out = {k: np.array(prev[k], np.float32, copy=True) for k in ("g0", "g1", "g2", "g3", "depth")}
+    ri = RasterIn()
+    ri.vtx, ri.vtx_stride_floats = _p(vtx, f32p), vtx.shape[1]
+    ri.pos_offset, ri.nrm_offset = pos_offset, nrm_offset
+    ri.idx, ri.n_tri = _p(idx, u32p), idx.shape[0]
+    tm = None
+    if tri_material is not None:
+        tm = np.ascontiguousarray(tri_material, np.int32)
+        ri.tri_material = _p(tm, i32p)
+    ri.materials = _p(mats, f32p)
+    ri.model[:] = col_major(model)
+    ri.view_proj[:] = col_major(view_proj)
+    ri.W, ri.H, ri.clear = W, H, int(bool(clear))
+    ro = RasterOut()
+    for k in ("g0", "g1", "g2", "g3", "depth"):
+        setattr(ro, k, _p(out[k], f32p))
+    rc = lib.orc_raster(ctypes.byref(ri), ctypes.byref(ro))
+    if rc:
+        raise RuntimeError(f"orc_raster failed: {rc}")
+    out["sub_tris"], out["dropped"] = int(ro.sub_tris), int(ro.dropped)
+    return out

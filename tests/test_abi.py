@@ -114,4 +114,6 @@ def test_batch_struct_layouts(fdzb):
     assert ctypes.sizeof(fdzb.FrameStats) == 184
     assert ctypes.sizeof(fdzb.FrameDesc) == 152
     assert ctypes.sizeof(fdzb.BatchStats) == 232
+    assert ctypes.sizeof(fdzb.RasterDesc) == 240
+    assert ctypes.sizeof(fdzb.RasterStats) == 64
     assert fdzb.FrameDesc.light.offset == 64 and fdzb.FrameDesc.d_shadow.offset == 128
