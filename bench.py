@@ -559,6 +559,118 @@ def served_workload(fdzb, torch, stream, rates=(100, 500, 2000), counts=(120, 24
     return out
 
 
+def _device_ms(torch, stream, fn, reps: int, flush=None) -> float:
+    """Mean device time of fn() over reps runs (after one warm-up run), CUDA
+    events on `stream`, L2 flushed before each."""
+    fn()
+    stream.synchronize()
+    out = []
+    for _ in range(reps):
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        stream.synchronize()
+        out.append(a.elapsed_time(b))
+    return statistics.mean(out)
+
+
+def next_rows_workload(fdzb, torch, stream, reps: int = 3) -> dict:
+    """The rows after the hot path, each timed on the device (CUDA events, L2
+    flushed before every run):
+    F1  the HD frame with a rectangular 64 x 48 light (64-bit row words), and
+        with the depth plane on its 16 x 16 light;
+    F2  the HD frame with a model transform applied as the vertices are read;
+    F3  a 1920 x 1080 rasterised view (height-field receiver of 131k triangles
+        plus 200k occluders) -- G-buffer, shadows on it, Phong shading;
+    F4  the ray-cast check on a 480 x 270 frame of 20k triangles, and the
+        shading pass alone on the HD G-buffer."""
+    import dataclasses
+
+    import numpy as np
+    scenes = importlib.import_module("4dzb_b200.scenes")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    out = {}
+
+    def frame_ms(scene, setup=None):
+        ctx, t = fdzb.context_for_scene(scene, masks=True)
+        ctx.set_stream(stream.cuda_stream)
+        if setup:
+            setup(ctx)
+        ms = _device_ms(torch, stream, lambda: (ctx.launch_async(), ctx.sync()), reps, flush)
+        st = ctx.stats()
+        ctx.close()
+        return ms, st
+
+    hd = scenes.preset("hd")
+    base_ms, _ = frame_ms(hd)
+    wide = dataclasses.replace(hd, light=dataclasses.replace(hd.light, n=64, nh=48))
+    wide_ms, wst = frame_ms(wide)
+    dp_ms, _ = frame_ms(dataclasses.replace(hd, depth_plane=True))
+    ang = np.radians(3.0)
+    rot = np.array([[np.cos(ang), -np.sin(ang), 0, 0], [np.sin(ang), np.cos(ang), 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+    xf_ms, _ = frame_ms(hd, lambda c: c.set_model_transform(rot.reshape(-1, order="F")))
+    out["F1_F2"] = {"hd_ms": base_ms, "light_64x48_ms": wide_ms, "light_64x48_pair_tests": wst["pair_tests"],
+                    "depth_plane_ms": dp_ms, "model_transform_ms": xf_ms}
+
+    # F3: rasterised view -> shadows -> shading
+    ms_ = scenes.mesh_scene(1920, 1080, grid=256, T=200_000, sigma=0.1)
+    S = ms_.W * ms_.H
+    dev = dict(vtx=torch.from_numpy(ms_.vtx).cuda(),
+               idx=torch.from_numpy(np.ascontiguousarray(ms_.idx).view(np.int32)).cuda(),
+               tm=torch.from_numpy(ms_.tri_material).cuda(), mats=torch.from_numpy(ms_.materials).cuda())
+    g = {k: torch.empty((S, 4), dtype=torch.float32, device="cuda") for k in ("g0", "g1", "g2", "g3")}
+    depth = torch.empty(S, dtype=torch.float32, device="cuda")
+    r = fdzb.Raster()
+    r.set_stream(stream.cuda_stream)
+    desc = fdzb.raster_desc(dev["vtx"], ms_.vtx.shape[0], dev["idx"], ms_.T, dev["mats"], 2, ms_.model,
+                            ms_.view_proj, ms_.W, ms_.H, g["g0"], g["g1"], g["g2"], g["g3"], depth,
+                            tri_material=dev["tm"])
+    raster_ms = _device_ms(torch, stream, lambda: (r.draw(desc), r.sync()), reps, flush)
+    rst = r.stats()
+    occ = ms_.idx[ms_.n_receiver:]
+    ov = np.ones((occ.size, 4), np.float32)
+    ov[:, :3] = ms_.vtx[occ.reshape(-1), :3]
+    sc = scenes.Scene(W=ms_.W, H=ms_.H, pos=np.zeros((S, 4), np.float32), nrm=np.zeros((S, 4), np.float32), vtx=ov,
+                      idx=np.arange(occ.size, dtype=np.int32).reshape(-1, 3), light=ms_.light, bins=128)
+    ctx, t = fdzb.context_for_scene(sc, masks=False)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_sample_buffers(g["g0"], g["g1"])
+    shadow_ms = _device_ms(torch, stream, lambda: (ctx.launch_async(), ctx.sync()), reps, flush)
+    rgba = torch.empty((S, 4), dtype=torch.float32, device="cuda")
+    lights = torch.tensor([list(ms_.light.position)], dtype=torch.float32, device="cuda")
+    shade_ms = _device_ms(torch, stream, lambda: fdzb.shade(ms_.W, ms_.H, g["g0"], g["g1"], g["g2"], g["g3"],
+                                                              t["shadow"], rgba, ms_.eye, (0.2, 0.2, 0.2),
+                                                              (0.8, 0.8, 0.8), (0.5, 0.5, 0.5), lights,
+                                                              stream=stream.cuda_stream), reps, flush)
+
+    def whole():
+        r.draw(desc)
+        ctx.launch_async()
+        fdzb.shade(ms_.W, ms_.H, g["g0"], g["g1"], g["g2"], g["g3"], t["shadow"], rgba, ms_.eye, (0.2, 0.2, 0.2),
+                   (0.8, 0.8, 0.8), (0.5, 0.5, 0.5), lights, stream=stream.cuda_stream)
+        ctx.sync()
+
+    frame = _device_ms(torch, stream, whole, reps, flush)
+    out["F3_rasterised_frame"] = {"W": ms_.W, "H": ms_.H, "triangles": ms_.T, "sub_triangles": rst["sub_triangles"],
+                                  "tile_pairs": rst["tile_pairs"], "raster_ms": raster_ms, "shadow_ms": shadow_ms,
+                                  "shade_ms": shade_ms, "frame_ms": frame, "frames_per_s": 1e3 / frame}
+    ctx.close()
+    r.close()
+
+    # F4: ray cast and shading
+    small = scenes.make_scene(480, 270, 20_000, n=16, bins=32, seed=7, sigma=0.1)
+    edge_ms, _ = frame_ms(small)
+    ray_ms, rs = frame_ms(small, lambda c: c.set_shadow_method(fdzb.SHADOW_RAY_CAST))
+    out["F4"] = {"ray_cast_480x270_ms": ray_ms, "edge_masks_480x270_ms": edge_ms, "ray_cast_pair_tests": rs["pair_tests"],
+                 "shade_1080p_ms": shade_ms}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -572,6 +684,7 @@ def main():
     ap.add_argument("--batched-only", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-only", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the rows after the hot path (F1-F4)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -676,7 +789,9 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
-    batched = served = None
+    batched = served = nxt = None
+    if ws == 1 and not args.no_next:
+        nxt = next_rows_workload(fdzb, torch, stream)
     if ws == 1 and not args.no_batched:
         ctx.close()
         batched = batched_workload(fdzb, torch, stream)
@@ -720,6 +835,8 @@ def main():
         out["batched"] = batched
     if served:
         out["served"] = served
+    if nxt is not None:
+        out["next_rows"] = nxt
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
