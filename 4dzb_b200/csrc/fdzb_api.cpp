@@ -560,9 +560,11 @@ int engine_sync(Engine &e)
     if (!e.pending) return FDZB_OK;
     e.replans = 0;
     for (;;) {
-        cudaError_t w = cudaStreamSynchronize(e.stream);
+        // the launch's own end event, not the whole stream: work another
+        // context or the caller queued behind this launch is not waited for
+        cudaError_t w = cudaEventSynchronize(e.ev1);
         e.pending = false;
-        if (w != cudaSuccess) return fail(FDZB_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(w));
+        if (w != cudaSuccess) return fail(FDZB_ERR_CUDA, std::string("cudaEventSynchronize: ") + cudaGetErrorString(w));
         const fdzb::Counters &k = *e.hCounters;
         if (k.errorFlags & fdzb::ERR_LOOKBACK_TIMEOUT)
             return fail(FDZB_ERR_DEVICE_TIMEOUT, "a look-back wait exceeded its spin limit");
