@@ -576,16 +576,21 @@ int fdzb_raster_draw(fdzb_raster *r, const fdzb_raster_desc *d)
         depth = r->depthScratch;
     }
     if (int rc = grow((void **)&r->recs, r->recSlots, 2 * (size_t)std::max(d->n_tri, 1), kRecF4 * sizeof(float4))) return rc;
-    size_t tc = r->tileCap;
-    if (int rc = grow((void **)&r->tileCount, tc, nTiles, sizeof(int))) return rc;
-    if (tc != r->tileCap) {
-        size_t c2 = 0, c3 = 0;
+    if (nTiles > r->tileCap) {
+        // the three per-tile arrays share one capacity
+        cudaFree(r->tileCount);
         cudaFree(r->tileStart);
         cudaFree(r->tileFill);
-        r->tileStart = r->tileFill = nullptr;
-        if (int rc = grow((void **)&r->tileStart, c2, tc, sizeof(int))) return rc;
-        if (int rc = grow((void **)&r->tileFill, c3, tc, sizeof(int))) return rc;
-        r->tileCap = tc;
+        r->tileCount = r->tileStart = r->tileFill = nullptr;
+        r->tileCap = 0;
+        const size_t cap = nTiles + nTiles / 4 + 64;
+        if (cudaMalloc(&r->tileCount, cap * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&r->tileStart, cap * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&r->tileFill, cap * sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return rfail(FDZB_ERR_NO_MEMORY, "device allocation failed");
+        }
+        r->tileCap = cap;
     }
     cudaStream_t s = r->stream;
     int sm = 148;

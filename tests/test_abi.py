@@ -48,6 +48,19 @@ def test_light_setup_matches_oracle(fdzb, scenes, n, radius):
     assert np.array_equal(a["deltas"], np.array([b.x_delt, b.y_delt], np.float32))
 
 
+@pytest.mark.parametrize("w,h", [(8, 16), (64, 3), (33, 64), (1, 7)])
+def test_rectangular_light_setup_matches_oracle(fdzb, scenes, w, h):
+    light = scenes.Light(right_radius=1.5, top_radius=0.5, n=w, nh=h, position=(0.1, 0.4, 6.0))
+    a = fdzb.light_setup(light)
+    b = oracle.light_setup(light)
+    assert b.resW == w and b.resH == h
+    assert b.fullRows == (1 << w) - 1 and b.fullCols == (1 << h) - 1 or w == 64 or h == 64
+    assert np.array_equal(a["mat"].view(np.uint32), np.array(b.mat, np.float32).view(np.uint32))
+    assert np.array_equal(a["deltas"], np.array([b.x_delt, b.y_delt], np.float32))
+    corners = np.array([b.upRight, b.upLeft, b.downLeft, b.downRight], np.float32)
+    assert np.array_equal(a["corners"], corners)
+
+
 def test_light_setup_canonical_values(fdzb, scenes):
     """Light at (0,0,6) facing -z, up +y, 2x2, N=8: right=+x, top=+y, steps of
     -2r/N along each, corners at +-r(N-1)/N, perspective 1/tan(60 rad)."""

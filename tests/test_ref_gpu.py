@@ -78,6 +78,15 @@ def test_hd_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes):
 
 
 @needs_lib
+def test_large_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes):
+    # 3840 x 2160 samples, 2M triangles, 32 x 32 light (full 32-bit rows)
+    scene = scenes.preset("large")
+    ref_gpu.preflight(scene, occ_stride=256)
+    ref = ref_gpu.run(scene, fmad=False, checked=True)
+    _check(fdzb, scene, ref)
+
+
+@needs_lib
 def test_fmad_build_runs_and_stays_close(cuda_ok, fdzb, scenes):
     scene = scenes.preset("small")
     exact = ref_gpu.run(scene, fmad=False)
