@@ -173,3 +173,42 @@ def test_bad_requests_fail_at_submission(cuda_ok, fdzb, scenes):
     with pytest.raises(fdzb.FdzbError):
         srv.submit(bad)
     srv.close()
+
+
+def test_rectangular_and_wide_lights_are_served(cuda_ok, fdzb, scenes):
+    """Requests with rectangular and 64-bit-row light grids, batched with a
+    square one, equal their plain single-frame launches bit for bit."""
+    import torch
+    sc, geo, views = _world(fdzb, scenes, nscenes=1, nviews=3, seed=6400)
+    srv = fdzb.Server(slots=1, max_batch_frames=4)
+    vtx, idx, V, T = geo[0]
+    srv.add_scene(vtx, V, idx, T, cull=False, esp=1e-3)
+    lights = [scenes.Light(n=8), scenes.Light(n=12, nh=40), scenes.Light(n=24, nh=5)]
+    outs, tickets = [], []
+    for v, light in enumerate(lights):
+        W, H, pos, nrm = views[v]
+        sh = torch.full((W * H,), -1.0, dtype=torch.float32, device="cuda")
+        mk = torch.zeros(W * H * fdzb.mask_words(light.n, light.cols), dtype=torch.int32, device="cuda")
+        outs.append((sh, mk))
+        tickets.append(srv.submit(fdzb.request(0, pos, nrm, W, H, light, sh, mk, bins=16)))
+    for t in tickets:
+        assert srv.wait(t)["status"] == 0
+    for v, light in enumerate(lights):
+        W, H, pos, nrm = views[v]
+        ctx = fdzb.Context()
+        sh = torch.empty(W * H, dtype=torch.float32, device="cuda")
+        mk = torch.empty(W * H * fdzb.mask_words(light.n, light.cols), dtype=torch.int32, device="cuda")
+        ctx.set_view(W, H)
+        ctx.set_bin_num(16)
+        ctx.set_scenes_esp(1e-3)
+        ctx.set_backface_cull(False)
+        ctx.add_model(vtx, V, 16, idx, T)
+        ctx.set_sample_buffers(pos, nrm)
+        ctx.set_output_buffer(sh, mk)
+        ctx.set_area_light(light)
+        ctx.launch()
+        assert torch.equal(sh, outs[v][0]), f"light {v} shadow"
+        assert torch.equal(mk, outs[v][1]), f"light {v} masks"
+        assert float(sh.max()) > 0.0
+        ctx.close()
+    srv.close()
