@@ -67,7 +67,9 @@ typedef unsigned long long u64;
 // K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(count-1) precomputed (the
 // same product) and the result limited to the grid's bits.  The shift has the
 // PTX shl semantics of the reference's device code: amounts >= the word width
-// (or negative) give 0.
+// (or negative) give 0.  -1*D is the exact negation -D, and the reference's
+// truncating conversion of ceilf(q) is the round-up conversion of q (both
+// saturate out of range and map NaN to 0).
 template <class R>
 __device__ __forceinline__ R row_mask(float D, float slopeNm1, float slope, R full, uint32_t &npart)
 {
@@ -76,8 +78,8 @@ __device__ __forceinline__ R row_mask(float D, float slopeNm1, float slope, R fu
     if (f1 && f2) return full;
     if (!f1 && !f2) return R(0);
     ++npart;
-    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
-    const int k = __float2int_rz(ceilf(q));
+    const float q = __fdiv_rn(-D, slope);
+    const int k = __float2int_ru(q);
     R m = ((unsigned)k >= (unsigned)RowWord<R>::kBits) ? R(0) : (R(1) << k);
     m -= R(1);
     if (!f1) m = ~m;
@@ -621,8 +623,8 @@ __device__ __forceinline__ uint32_t row_mask_sel(float D, float slopeNm1, float 
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
-    const float q = __fdiv_rn(__fmul_rn(-1.0f, D), slope);
-    const int k = __float2int_rz(ceilf(q));
+    const float q = __fdiv_rn(-D, slope);
+    const int k = __float2int_ru(q);
     uint32_t m = ((unsigned)k >= 32u) ? 0u : (1u << k);
     m -= 1u;
     m = f1 ? m : ~m;
