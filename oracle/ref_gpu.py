@@ -46,7 +46,8 @@ class RefGpuOut(ctypes.Structure):
                 ("sub", ctypes.c_float * 2), ("lp_begin", ctypes.c_float * 3), ("lp_end", ctypes.c_float * 3),
                 ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 8),
                 ("model_aabb", ctypes.c_float * 8), ("first_error", ctypes.c_char * 160),
-                ("surf_handle", ctypes.c_int64), ("pos_tex_handle", ctypes.c_int64), ("view_error", ctypes.c_int64)]
+                ("surf_handle", ctypes.c_int64), ("pos_tex_handle", ctypes.c_int64), ("view_error", ctypes.c_int64),
+                ("masks", ctypes.POINTER(ctypes.c_uint32))]
 
 
 _libs: dict = {}
@@ -95,10 +96,14 @@ def preflight(scene, occ_stride: int = 64) -> dict:
     return sc
 
 
-def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool = False) -> dict:
+def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool = False,
+        masks: bool = False) -> dict:
     """Frames through the reference on the current GPU (device 0 of this process).
     The shadow buffer of the last launch is returned at y*W+x; launch_ms holds
-    the CUDA-event time of each timed FDLaunch (L2 flushed before each)."""
+    the CUDA-event time of each timed FDLaunch (L2 flushed before each).  With
+    masks, "mask_rows" holds each sample's N light-row words as the reference's
+    per-sample kernel left them ([S, N] uint32 at y*W+x) and "mask_written"
+    where that kernel ran (binned samples)."""
     if not checked:
         preflight(scene)
     lib = load(fmad)
@@ -125,6 +130,9 @@ def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool
     ri.lightRes = L.n
     ri.warmup, ri.reps = int(warmup), reps
     ro = RefGpuOut()
+    dump = np.zeros(scene.S * (L.n + 1) if masks else 1, np.uint32)
+    if masks:
+        ro.masks = dump.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
     ro.shadow = shadow.ctypes.data_as(f32p)
     ro.launch_ms = launch_ms.ctypes.data_as(f32p)
     ro.fdlaunch_ms = own_ms.ctypes.data_as(f32p)
@@ -139,4 +147,8 @@ def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool
             out[name] = np.array(list(v), np.float32)
     if rc:
         raise RuntimeError(f"reference GPU frame failed: {out['errors']} CUDA errors, first: {out['first_error']}")
+    if masks:
+        d = dump.reshape(scene.S, L.n + 1)
+        out["mask_written"] = d[:, 0] == 1
+        out["mask_rows"] = d[:, 1:]
     return out

@@ -23,7 +23,7 @@ the repository:
 * the kernel files K/*.inl are concatenated, in the order of K/FourD.cu:230-257,
   between harness_pre.cuh and harness_post.cuh into a temporary .cu under
   oracle/_ref/ that is deleted after compiling.  The concatenation changes
-  three things only, each checked to apply exactly once:
+  four things only, each checked to apply exactly once:
     - the nested includes of Step2_3 (already concatenated) are dropped and the
       backslash include path of moveModel.inl is normalised;
     - the unguarded per-frame pair dump `showBinTriPair(pairNum);`
@@ -32,7 +32,10 @@ the repository:
     - in the per-sample kernel's row loop
       (K/Step5_2_shadowCalPerSample.inl:204-222) a row index >= N is counted
       and skipped instead of indexing past the sample's N rows of shared
-      memory (inverted partial row filters can keep bits >= N set).
+      memory (inverted partial row filters can keep bits >= N set);
+    - after that kernel's shadow store (:231) the sample's final rows are
+      copied to a harness buffer when one is set (REFGPU_MASK_DUMP), so that
+      the reference's masks, not only its shadows, can be compared.
 """
 from __future__ import annotations
 
@@ -65,6 +68,9 @@ EDITS = [
      "/* per-frame pair dump removed by the harness */"),
     ("Step5_2_shadowCalPerSample.inl", "mask[rowID*32] |= M0 & M1 & M2;",
      "REFGPU_ROW_GUARD(rowID, lightResHeight) mask[rowID*32] |= M0 & M1 & M2;"),
+    ("Step5_2_shadowCalPerSample.inl", "shadowResult[sampleID] = (float)result / (float)lightResNum;",
+     "shadowResult[sampleID] = (float)result / (float)lightResNum; "
+     "REFGPU_MASK_DUMP(sampleID, mask, lightResHeight)"),
 ]
 
 

@@ -175,6 +175,10 @@ struct RefGpuOut {
     // diagnostics: surface and texture handles, the error state after FDsetView
     // (the reference leaves cudaCreateSurfaceObject unchecked), valid triangles
     int64_t surf_handle, pos_tex_handle, view_error;
+    // optional host [W*H*(N+1)] at y*W+x: per sample a written marker (1 where
+    // the per-sample kernel ran, else 0) and its N light-row words, from the
+    // last launch (REFGPU_MASK_DUMP)
+    uint32_t *masks;
 };
 
 static int refgpu_round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -246,6 +250,15 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     m_validSampleNum = 0;
     unsigned long long zero = 0;
     checkCudaErrors(cudaMemcpyToSymbol(refgpu_rows_beyond_n, &zero, sizeof(zero)));
+    // mask dump: N + 1 words per output slot of the reference's padded index
+    const size_t dumpWords = (size_t)(in->lightRes + 1);
+    const size_t dumpBytes = pitch * H * dumpWords * sizeof(uint32_t);
+    unsigned int *dDump = nullptr;
+    if (out->masks) {
+        checkCudaErrors(cudaMalloc(&dDump, dumpBytes));
+        checkCudaErrors(cudaMemset(dDump, 0, dumpBytes));
+    }
+    checkCudaErrors(cudaMemcpyToSymbol(refgpu_mask_out, &dDump, sizeof(dDump)));
 
     // between launches the L2 (126 MB on B200) is flushed by a 256 MB write,
     // outside the timed region, so no launch starts with the previous one's
@@ -309,6 +322,17 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     if (out->shadow)
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) out->shadow[(size_t)y * W + x] = pbo[((size_t)y << log2up) | x];
+    if (dDump) {
+        std::vector<uint32_t> dump(pitch * H * dumpWords, 0u);
+        checkCudaErrors(cudaMemcpy(dump.data(), dDump, dumpBytes, cudaMemcpyDeviceToHost));
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+                memcpy(out->masks + ((size_t)y * W + x) * dumpWords,
+                       dump.data() + (((size_t)y << log2up) | x) * dumpWords, dumpWords * sizeof(uint32_t));
+        unsigned int *none = nullptr;
+        checkCudaErrors(cudaMemcpyToSymbol(refgpu_mask_out, &none, sizeof(none)));
+        cudaFree(dDump);
+    }
     out->sub[0] = h_fdRectangleSubConstant.x;
     out->sub[1] = h_fdRectangleSubConstant.y;
     const FDLightPlaneParams &P = h_fdLightPlaneParams;

@@ -61,3 +61,15 @@ __device__ unsigned long long refgpu_rows_beyond_n;
         atomicAdd(&refgpu_rows_beyond_n, 1ull);           \
         continue;                                         \
     }
+
+// Harness mask dump: after the per-sample kernel's shadow store
+// (K/Step5_2_shadowCalPerSample.inl:231) the sample's final light rows, when
+// the harness has set refgpu_mask_out: per sample (at the kernel's output
+// index) a written marker 1 followed by its N row words, N + 1 words in all.
+__device__ unsigned int *refgpu_mask_out;
+#define REFGPU_MASK_DUMP(sid, m, rows)                                                  \
+    if (refgpu_mask_out) {                                                              \
+        unsigned int *o_ = refgpu_mask_out + (size_t)(sid) * (size_t)((rows) + 1);     \
+        o_[0] = 1u;                                                                     \
+        for (int r_ = 0; r_ < (rows); ++r_) o_[1 + r_] = (m)[r_ * 32];                  \
+    }

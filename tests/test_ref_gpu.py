@@ -5,7 +5,9 @@ K/*.inl) compiled for sm_100a with --fmad=false by
 oracle/ref_gpu/build_ref_gpu.py; FDLaunch runs its own kernels, Thrust sorts
 and host sequencing.  At the reference's 16 x 16 bins the product's shadows
 must equal the reference's bit for bit, and the light-plane setup and the
-binning counts must agree.  Every scene passes the CPU preflight (keys inside
+binning counts must agree; the reference's per-sample kernel also hands
+out its final light rows (a harness dump after its shadow store), which must
+equal the product's masks for every binned sample.  Every scene passes the CPU preflight (keys inside
 the bin grid, pairs inside the reference's pair buffers) before it reaches
 the GPU.  The --fmad=true build (the reference project's default) is run too:
 its shadows differ from the exact ones only where a fused multiply-add moved a
@@ -25,19 +27,41 @@ needs_lib = pytest.mark.skipif(not ref_gpu.available(), reason="reference GPU ha
 
 def _product(fdzb, scene):
     s16 = dataclasses.replace(scene, bins=ref_gpu.REF_BINS)
-    ctx, t = fdzb.context_for_scene(s16, masks=False, tri_order=fdzb.TRI_ORDER_REFERENCE)
+    ctx, t = fdzb.context_for_scene(s16, masks=True, tri_order=fdzb.TRI_ORDER_REFERENCE)
     ctx.launch()
     st = ctx.stats()
     sh = t["shadow"].cpu().numpy().copy()
+    mk = t["masks"].cpu().numpy().view(np.uint32).reshape(scene.S, -1).copy()
     ctx.close()
-    return sh, st
+    return sh, mk, st
+
+
+def _rows_of(words, n):
+    """Light rows of packed masks (bit r*n + c is row r, column c) as uint32[S, n]."""
+    w = np.concatenate([words, np.zeros((words.shape[0], 1), np.uint32)], axis=1).astype(np.uint64)
+    rows = np.empty((words.shape[0], n), np.uint32)
+    full = np.uint64((1 << n) - 1)
+    for r in range(n):
+        b = r * n
+        v = (w[:, b >> 5] | (w[:, (b >> 5) + 1] << np.uint64(32))) >> np.uint64(b & 31)
+        rows[:, r] = (v & full).astype(np.uint32)
+    return rows
 
 
 def _check(fdzb, scene, ref):
-    sh, st = _product(fdzb, scene)
+    sh, mk, st = _product(fdzb, scene)
     assert ref["rows_beyond_n"] == 0
     bad = np.flatnonzero(sh.view(np.uint32) != ref["shadow"].view(np.uint32))
     assert bad.size == 0, f"{bad.size} of {scene.S} shadows differ, first {bad[:5].tolist()}"
+    # masks: the reference's per-sample kernel ran for every binned sample;
+    # its rows (all 32 bits) equal the product's packed rows
+    n = scene.light.n
+    wr = ref["mask_written"]
+    assert int(wr.sum()) == ref["valid_samples"] == st["valid_samples"]
+    got = _rows_of(mk[wr], n)
+    exp = ref["mask_rows"][wr]
+    badm = np.flatnonzero((got != exp).any(axis=1))
+    assert badm.size == 0, f"{badm.size} of {int(wr.sum())} sample masks differ, first {np.flatnonzero(wr)[badm[:5]].tolist()}"
     assert st["valid_samples"] == ref["valid_samples"]
     assert st["valid_triangles"] == ref["valid_tris"]
     assert st["num_pairs"] == ref["num_pairs"]
@@ -56,7 +80,7 @@ def _check(fdzb, scene, ref):
 @pytest.mark.parametrize("cull", [False, True])
 def test_small_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes, cull):
     scene = scenes.preset("small", cull=cull)
-    ref = ref_gpu.run(scene, fmad=False)
+    ref = ref_gpu.run(scene, fmad=False, masks=True)
     _check(fdzb, scene, ref)
 
 
@@ -65,14 +89,14 @@ def test_odd_sizes_equal_reference_on_gpu(cuda_ok, fdzb, scenes):
     # non-power-of-two width (the reference's padded output rows), N = 5 and 32
     for W, H, T, n, seed in ((301, 77, 700, 5, 11), (200, 150, 1500, 32, 12)):
         scene = scenes.make_scene(W, H, T, n=n, bins=16, seed=seed, cull=True)
-        ref = ref_gpu.run(scene, fmad=False)
+        ref = ref_gpu.run(scene, fmad=False, masks=True)
         _check(fdzb, scene, ref)
 
 
 @needs_lib
 def test_hd_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes):
     scene = scenes.preset("hd")
-    ref = ref_gpu.run(scene, fmad=False)
+    ref = ref_gpu.run(scene, fmad=False, masks=True)
     sh = _check(fdzb, scene, ref)
     assert 0.0 < float(sh.mean()) <= 1.0
 
@@ -82,7 +106,7 @@ def test_large_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes):
     # 3840 x 2160 samples, 2M triangles, 32 x 32 light (full 32-bit rows)
     scene = scenes.preset("large")
     ref_gpu.preflight(scene, occ_stride=256)
-    ref = ref_gpu.run(scene, fmad=False, checked=True)
+    ref = ref_gpu.run(scene, fmad=False, checked=True, masks=True)
     _check(fdzb, scene, ref)
 
 
