@@ -61,7 +61,10 @@ static_assert(sizeof(fdzb_shade_desc) == 120, "fdzb_shade_desc layout");
 
 constexpr long long kMaxPairCapacity = 1ll << 29;
 constexpr long long kMaxTotalSamples = 0x7fffffffll / 2;
-constexpr long long kMaxTotalBins = 1ll << 27;   // leaves >= 5 depth bits in a 32-bit pair key
+constexpr long long kMaxTotalBins = 1ll << 27;
+// coverage bucket of the triangle order: log2 of the angular size in steps of
+// 1/25.6 octave (fdzb_pipeline.cu: coverage_bucket)
+constexpr int kCoverageBucketBits = 10;
 
 struct Model {
     const float *vtx = nullptr;
@@ -97,7 +100,7 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long
     b.states = (fdzb::FrameState *)take(sizeof(fdzb::FrameState) * nf);
     b.counters = (fdzb::Counters *)take(sizeof(fdzb::Counters));
     b.epochWord = (uint32_t *)take(sizeof(uint32_t));
-    b.sortHist = (uint32_t *)take(sizeof(uint32_t) * 8 * 256);
+    b.sortHist = (uint32_t *)take(sizeof(uint32_t) * 4 * fdzb::kSortSlots * 256);
     b.sampleBases = (int *)take(sizeof(int) * 3 * nf);
     b.triBases = b.sampleBases ? b.sampleBases + nf : nullptr;
     b.binBases = b.sampleBases ? b.sampleBases + 2 * nf : nullptr;
@@ -112,13 +115,17 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long
     b.triRec = (float4 *)take(64 * Ts);
     b.triCount = (int32_t *)take(4 * Ts);
     b.triScanStatus = (unsigned long long *)take(8 * ((Ts + fdzb::kTriTileHost - 1) / fdzb::kTriTileHost));
+    b.tkeysA = (uint32_t *)take(4 * Ts);
+    b.tvalsA = (uint32_t *)take(4 * Ts);
+    b.tkeysB = (uint32_t *)take(4 * Ts);
+    b.tvalsB = (uint32_t *)take(4 * Ts);
     b.pkeysA = (uint32_t *)take(4 * Ps);
     b.pvalsA = (uint32_t *)take(4 * Ps);
     b.pkeysB = (uint32_t *)take(4 * Ps);
     b.pvalsB = (uint32_t *)take(4 * Ps);
     b.binTriStart = (int32_t *)take(4 * (size_t)NB);
     b.binTriEnd = (int32_t *)take(4 * (size_t)NB);
-    const size_t tiles = (std::max(Ss, Ps) + fdzb::kSortTileHost - 1) / fdzb::kSortTileHost;
+    const size_t tiles = (std::max(std::max(Ss, Ps), Ts) + fdzb::kSortTileHost - 1) / fdzb::kSortTileHost;
     b.sortStatusTiles = tiles;
     b.sortStatus = (unsigned long long *)take(8 * 256 * tiles);
     b.itemCapacity = (int)(Ss / 32 + (size_t)NB + (size_t)nf + 1);
@@ -271,7 +278,7 @@ cudaError_t enqueue_body(Engine &e, int nf)
     if ((err = cudaMemcpyAsync(b.frames, e.hFrames, sizeof(fdzb::FrameDesc) * nf, cudaMemcpyHostToDevice, s))) return err;
     if ((err = cudaMemcpyAsync(b.sampleBases, e.hBases, 3 * sizeof(int) * nf, cudaMemcpyHostToDevice, s))) return err;
     if ((err = cudaMemsetAsync(b.counters, 0, sizeof(fdzb::Counters), s))) return err;
-    if ((err = cudaMemsetAsync(b.sortHist, 0, 8 * 256 * sizeof(uint32_t), s))) return err;
+    if ((err = cudaMemsetAsync(b.sortHist, 0, 4 * fdzb::kSortSlots * 256 * sizeof(uint32_t), s))) return err;
     if ((err = fdzb::run_pipeline(b, e.maxS, e.maxT, e.maxV, s, e.profile ? e.stageEv : nullptr, &e.launches))) return err;
     if ((err = cudaMemcpyAsync(e.hCounters, b.counters, sizeof(fdzb::Counters), cudaMemcpyDeviceToHost, s))) return err;
     return cudaMemcpyAsync(e.hStates, b.states, sizeof(fdzb::FrameState) * nf, cudaMemcpyDeviceToHost, s);
@@ -320,21 +327,15 @@ int engine_enqueue(Engine &e)
     b.depthPlane = e.depthPlane;
     b.rayCast = e.rayCast;
     b.occVariant = (e.occVariant == 1 && !wide && square && !e.depthPlane) ? 1 : 0;
-    // Triangle lists: reference order sorts pairs by bin only (stable, so ascending
-    // triangle id inside a bin, K/Step4_RasterizeTriangleToBin.inl:220-223).  Depth
-    // order appends a depth bucket below the bin so each bin lists its lowest
-    // triangles first, which fills the masks in far fewer pair tests; it uses the
-    // key bits left over in the last radix pass, at least 4.
-    {
-        const int binBits = ceil_log2(NB);
-        if (e.triOrder == FDZB_TRI_ORDER_COVERAGE) {
-            const int passes = (binBits + 4 + 7) / 8;
-            b.depthBits = std::min(10, passes * 8 - binBits);
-        } else {
-            b.depthBits = 0;
-        }
-        b.pairPasses = fdzb::sort_passes_for(NB << b.depthBits);
-    }
+    // Triangle lists: the pairs are sorted by bin only (stable, so a bin lists
+    // its triangles in the order the pairs were emitted,
+    // K/Step4_RasterizeTriangleToBin.inl:220-223).  Reference order emits them by
+    // ascending triangle id; coverage order first sorts the triangles (stably) by
+    // a coverage bucket and emits them in that order, so each bin lists its
+    // widest triangles first, which fills the masks in far fewer pair tests.
+    b.depthBits = e.triOrder == FDZB_TRI_ORDER_COVERAGE ? kCoverageBucketBits : 0;
+    b.triPasses = b.depthBits ? fdzb::sort_passes_for(1ll << b.depthBits) : 0;
+    b.pairPasses = fdzb::sort_passes_for(NB);
     int sb = 0, tb = 0, bb = 0;
     for (int i = 0; i < nf; ++i) {
         const FrameSpec &s = e.frames[i];
@@ -1228,14 +1229,11 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
     case FDZB_ARR_TRI_COUNT: src = b.triCount; avail = 4 * T; break;
     case FDZB_ARR_PAIR_BIN:
     case FDZB_ARR_SORTED_PAIR_BIN: {
-        // pair keys carry the depth bucket below the bin; export the bin
+        // pair keys are the global bins
         const uint32_t *s2 = what == FDZB_ARR_PAIR_BIN ? b.dbgPKeys : (pOdd ? b.pkeysB : b.pkeysA);
         if (!s2) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
         if (bytes > 4 * P) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
-        std::vector<uint32_t> v(bytes / 4);
-        if (!v.empty()) FDZB_CUDA(cudaMemcpy(v.data(), s2, 4 * v.size(), cudaMemcpyDeviceToHost));
-        for (uint32_t &x : v) x >>= b.depthBits;
-        std::memcpy(dst, v.data(), 4 * v.size());
+        if (bytes) FDZB_CUDA(cudaMemcpy(dst, s2, bytes, cudaMemcpyDeviceToHost));
         return FDZB_OK;
     }
     case FDZB_ARR_PAIR_TRI:

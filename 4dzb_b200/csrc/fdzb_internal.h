@@ -86,7 +86,7 @@ struct Counters {
     int triTileCounter;     // look-back scan tile ticket
     int errorFlags;         // bit 0: look-back wait gave up, bit 1: mbarrier wait gave up
     unsigned long long pairTests;
-    int sortTileCounter[8]; // one ticket per radix pass (4 sample + 4 pair)
+    int sortTileCounter[12]; // one ticket per radix pass (4 sample, 4 pair, 4 triangle)
     unsigned long long rowsEvaluated;   // light rows evaluated by pair tests
     unsigned long long partialMasks;    // row masks that needed the ceil(-D/B) threshold
     unsigned long long pairsExamined;   // sample/triangle pairs reaching the AABB pre-cull
@@ -119,8 +119,11 @@ struct DeviceBuffers {
     // pairs
     uint32_t *pkeysA, *pvalsA, *pkeysB, *pvalsB;  // [pairCapacity]
     int32_t *binTriStart, *binTriEnd;          // [totalBins]
+    // coverage order: (bucket, triangle) pairs sorted by bucket; the sorted
+    // values are the order in which k_tri_pairs emits the triangles' pairs
+    uint32_t *tkeysA, *tvalsA, *tkeysB, *tvalsB;  // [totalTris]
     // sort scratch
-    uint32_t *sortHist;                         // [8 * 256]: 4 sample passes, 4 pair passes
+    uint32_t *sortHist;                         // [12 * 256]: 4 sample, 4 pair, 4 triangle passes
     unsigned long long *sortStatus;             // [sortStatusTiles * 256] epoch-tagged
     size_t sortStatusTiles;
     int *sampleBases, *triBases, *binBases;     // [nframes] ascending global bases
@@ -128,8 +131,9 @@ struct DeviceBuffers {
     int4 *items;                                // [itemCapacity]
     int itemCapacity;
     // sorted data lands in the A buffers after an even number of passes, B after odd
-    int samplePasses, pairPasses;
-    int depthBits;                              // secondary (depth-bucket) bits of the pair key
+    int samplePasses, pairPasses, triPasses;
+    int depthBits;                              // coverage-bucket bits of the triangle order (0:
+                                                // the reference's order, no triangle sort)
     int occVariant;                             // 0: k_occlusion (lane per sample), 1: k_occlusion_pairs
     int rayCast;                                // 1: ray-cast cross-check (REF_CAL) instead of edge masks
     int wide;                                   // 1: some frame's light grid exceeds 32 rows or
@@ -164,5 +168,6 @@ cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cu
 #endif
 constexpr int kSortTileHost = 256 * FDZB_SORT_ITEMS;   // keys per radix-sort tile (fdzb_sort.cuh)
 constexpr int kTriTileHost = 256;     // triangles per pair-scan tile
+constexpr int kSortSlots = 3;        // radix sorts per launch: samples, pairs, triangles
 
 }  // namespace fdzb

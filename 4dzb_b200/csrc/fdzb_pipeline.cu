@@ -497,13 +497,27 @@ __device__ __forceinline__ uint32_t coverage_bucket(const float4 *__restrict__ r
     return (uint32_t)(int)fminf(fmaxf(q, 0.0f), nb - 1.0f);
 }
 
+// k_tri_order: the coverage order's sort input, (bucket, triangle id) for every
+// triangle; triangles of frames without a light plane go last (they emit no
+// pairs either way).
+__global__ void k_tri_order(const FrameState *__restrict__ states, const int *__restrict__ triBases, int nframes,
+                            int totalTris, const float4 *__restrict__ rec, int depthBits,
+                            uint32_t *__restrict__ keys, uint32_t *__restrict__ vals)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < totalTris; g += gridDim.x * blockDim.x) {
+        const FrameState &st = states[frame_of(triBases, nframes, g)];
+        keys[g] = (st.state == 2 && st.nValidTris > 0) ? coverage_bucket(rec, g, st.f, depthBits)
+                                                       : (1u << depthBits) - 1u;
+        vals[g] = (uint32_t)g;
+    }
+}
+
 // Candidate bins of a triangle, swept by a warp 32 at a time in row-major
 // order; returns the number accepted and, with write != nullptr, writes the
 // accepted (bin, triangle) pairs from position `pos` on, in order.
 __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, const TriBins &c, int bb, int l2,
                                           int lane, uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals,
-                                          unsigned long long pos, int capacity, int depthBits, uint32_t bucket,
-                                          int g, bool write)
+                                          unsigned long long pos, int capacity, int g, bool write)
 {
     const int w = c.cex - c.cbx, h = c.cey - c.cby;
     if (w <= 0 || h <= 0) return 0;
@@ -524,7 +538,7 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
         if (write && ok) {
             const unsigned long long p = pos + (unsigned long long)total + (unsigned)__popc(m & lanemask_lt());
             if (p < (unsigned long long)capacity) {
-                pkeys[p] = ((uint32_t)gb << depthBits) | bucket;
+                pkeys[p] = (uint32_t)gb;
                 pvals[p] = (uint32_t)g;
             }
         }
@@ -544,14 +558,15 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
 // one's candidate bins with its 32 lanes.  Count pass, block scan of the
 // per-triangle counts, decoupled look-back over tiles for the tile's global
 // offset, then the write pass in the same order: pairs come out in triangle
-// order, bins row-major -- the reference's layout.
+// order, bins row-major -- the reference's layout.  With `order` (the coverage
+// order) the i-th triangle processed is order[i] instead of i.
 __global__ void __launch_bounds__(kTriThreads)
     k_tri_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int *__restrict__ triBases, int nframes, int totalTris,
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
                 int32_t *__restrict__ triCount, unsigned long long *scanStatus, const uint32_t *epochWord,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
-                int depthBits, Counters *ctr)
+                const uint32_t *__restrict__ order, Counters *ctr)
 {
     constexpr int WARPS = kTriThreads / 32;
     __shared__ int s_tile;
@@ -570,9 +585,10 @@ __global__ void __launch_bounds__(kTriThreads)
         const int t0 = tile * kTriThreads;
         // count pass: warp per triangle
         for (int k = warp; k < kTriThreads; k += WARPS) {
-            const int g = t0 + k;
+            const int i = t0 + k;
+            const int g = (order && i < totalTris) ? (int)order[i] : i;
             int cnt = 0;
-            if (g < totalTris) {
+            if (i < totalTris && (unsigned)g < (unsigned)totalTris) {
                 const int fi = frame_of(triBases, nframes, g);
                 const FrameState &st = states[fi];
                 if (st.state == 2 && st.nValidTris > 0) {
@@ -581,7 +597,7 @@ __global__ void __launch_bounds__(kTriThreads)
                     const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
                     if (c.any)
                         cnt = sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals, 0,
-                                         capacity, depthBits, 0u, g, false);
+                                         capacity, g, false);
                 }
                 if (lane == 0) triCount[g] = cnt;
             }
@@ -645,8 +661,10 @@ __global__ void __launch_bounds__(kTriThreads)
         // write pass, same order
         const unsigned long long tileBase = s_excl;
         for (int k = warp; k < kTriThreads; k += WARPS) {
-            const int g = t0 + k;
-            if (g >= totalTris) continue;
+            const int i = t0 + k;
+            if (i >= totalTris) continue;
+            const int g = order ? (int)order[i] : i;
+            if ((unsigned)g >= (unsigned)totalTris) continue;
             const int fi = frame_of(triBases, nframes, g);
             const FrameState &st = states[fi];
             if (!(st.state == 2 && st.nValidTris > 0)) continue;
@@ -654,9 +672,8 @@ __global__ void __launch_bounds__(kTriThreads)
                          q3 = __ldg(rec + 4 * (size_t)g + 3);
             const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
             if (!c.any) continue;
-            const uint32_t bucket = coverage_bucket(rec, g, st.f, depthBits);
             sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals,
-                       tileBase + (unsigned long long)s_cnt[k], capacity, depthBits, bucket, g, true);
+                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true);
         }
     }
 }
@@ -719,7 +736,8 @@ static int grid_for(long long n, int threads, int cap)
 }
 
 // Sorts (kA, vA) with kB/vB as ping-pong buffers; `slot` selects the histogram
-// and ticket block (0 samples, 1 pairs).  Pass p uses tag 8*launch + 4*slot + p.
+// and ticket block (0 samples, 1 pairs, 2 triangles).  Pass p uses tag
+// 16*launch + 4*slot + p.
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
                      cudaStream_t s)
@@ -793,15 +811,24 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
         (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
     nl += 2 + b.samplePasses;
-    // (a) triangle/bin pairs
+    // (a) triangle/bin pairs, in the coverage order when one is asked for
     if (ev) cudaEventRecord(ev[STAGE_TRI_PAIRS], s);
+    const uint32_t *order = nullptr;
+    if (b.depthBits > 0 && b.totalTris > 0) {
+        k_tri_order<<<grid_for(b.totalTris, 256, sm * 8), 256, 0, s>>>(b.states, b.triBases, nf, b.totalTris,
+                                                                     b.triRec, b.depthBits, b.tkeysA, b.tvalsA);
+        run_sort(b, 2, b.tkeysA, b.tvalsA, b.tkeysB, b.tvalsB, nullptr, b.totalTris, b.totalTris, b.triPasses,
+                 sm, s);
+        order = (b.triPasses & 1) ? b.tvalsB : b.tvalsA;
+        nl += 2 + b.triPasses;
+    }
     {
         const int tiles = (b.totalTris + kTriThreads - 1) / kTriThreads;
         const int grid = tiles < sm * 4 ? (tiles > 0 ? tiles : 1) : sm * 4;
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 b.depthBits, b.counters);
+                                                 order, b.counters);
         nl += 1;
     }
     if (b.dbgPKeys) {
@@ -815,7 +842,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
     uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
-        pk, &b.counters->pairCount, 0, b.pairCapacity, b.depthBits, b.binTriStart, b.binTriEnd,
+        pk, &b.counters->pairCount, 0, b.pairCapacity, 0, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
     nl += 2 + b.pairPasses;
     // (c) + (d) occlusion and shading

@@ -76,9 +76,9 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
 
     const int n = sort_count(n_dev, n_static, cap);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // look-back tag of this pass: 8 x (launch number, a device word that k_init
-    // advances, so graph replays get fresh tags) + pass slot
-    const uint32_t epoch = (epochWord ? *epochWord * 8u : 0u) + epochLo;
+    // look-back tag of this pass: 16 x (launch number, a device word that k_init
+    // advances, so graph replays get fresh tags) + 4 x sort slot + pass
+    const uint32_t epoch = (epochWord ? *epochWord * 16u : 0u) + epochLo;
 
     // Exclusive scan of this pass's digit histogram (digit = tid).
     {
