@@ -164,7 +164,7 @@ int set_error(int code, const std::string &msg);
 int sort_passes_for(long long keyRangeExclusive);
 cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cudaStream_t stream);
 #ifndef FDZB_SORT_ITEMS
-#define FDZB_SORT_ITEMS 8
+#define FDZB_SORT_ITEMS 16
 #endif
 constexpr int kSortTileHost = 256 * FDZB_SORT_ITEMS;   // keys per radix-sort tile (fdzb_sort.cuh)
 constexpr int kTriTileHost = 256;     // triangles per pair-scan tile

@@ -19,7 +19,7 @@
 namespace fdzb {
 
 #ifndef FDZB_SORT_MINBLOCKS
-#define FDZB_SORT_MINBLOCKS 4
+#define FDZB_SORT_MINBLOCKS 3
 #endif
 constexpr int kSortThreads = 256;                      // = kRadix: thread d handles digit d
 constexpr int kSortItems = FDZB_SORT_ITEMS;

@@ -539,7 +539,7 @@ const char *fdzb_serve_last_worker_error(fdzb_server *server);
  * path, a host process that owns every allocation, a real-time loop that may
  * not synchronise for cudaFree -- this sorts n (key, value) uint32 pairs by key,
  * stably (equal keys keep their input order), keys < key_range, using only a
- * fixed scratch area built into the library (about 8.5 MB of device memory on
+ * fixed scratch area built into the library (about 8.9 MB of device memory on
  * every GPU that loads libfdzb.so, held until the process exits).  It is the
  * same radix sort the frame pipeline runs on its own arena.
  *  - n at most FDZB_NOALLOC_SORT_MAX_PAIRS; larger n is rejected
