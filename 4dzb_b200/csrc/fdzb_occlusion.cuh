@@ -217,20 +217,24 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
         Bn3 = __fmul_rn(B3, g.ncm1);
         vr &= row_mask<R>(__fadd_rn(B3 > 0.0f ? Bn3 : 0.0f, C3), __fmul_rn(A3, g.nrm1), A3, g.FR, npart);
     }
-    // rows (:204-222)
+    // rows (:204-222).  The row's mask is the AND of the edges' masks, so it only
+    // loses bits as edges are added: once it holds no bit the row lacks, the
+    // remaining edges cannot change the row and are not evaluated.
     while (vr) {
         const int r = RowWord<R>::lowest(vr);
         vr &= vr - R(1);
         ++nrows;
         const float fr = (float)r;
-        const R M0 = row_mask<R>(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, g.FC, npart);
-        const R M1 = row_mask<R>(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, g.FC, npart);
-        const R M2 = row_mask<R>(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, g.FC, npart);
-        R m = M0 & M1 & M2;
-        if (dp) m &= row_mask<R>(__fadd_rn(__fmul_rn(A3, fr), C3), Bn3, B3, g.FC, npart);
-        const R nv = rows[r][lane] | m;
-        rows[r][lane] = nv;
-        if (nv == g.FC) fullRows |= R(1) << r;
+        const R have = rows[r][lane];
+        R m = row_mask<R>(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, g.FC, npart);
+        if (m & ~have) m &= row_mask<R>(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, g.FC, npart);
+        if (m & ~have) m &= row_mask<R>(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, g.FC, npart);
+        if (dp && (m & ~have)) m &= row_mask<R>(__fadd_rn(__fmul_rn(A3, fr), C3), Bn3, B3, g.FC, npart);
+        if (m & ~have) {
+            const R nv = have | m;
+            rows[r][lane] = nv;
+            if (nv == g.FC) fullRows |= R(1) << r;
+        }
     }
     return 1;
 }
