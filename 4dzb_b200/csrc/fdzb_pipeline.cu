@@ -824,7 +824,9 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     }
     {
         const int tiles = (b.totalTris + kTriThreads - 1) / kTriThreads;
-        const int grid = tiles < sm * 4 ? (tiles > 0 ? tiles : 1) : sm * 4;
+        // up to 8 blocks per SM: the sweeps wait on bin-statistics loads, so
+        // more resident warps hide more of that latency (40 registers: 6 fit)
+        const int grid = tiles < sm * 8 ? (tiles > 0 ? tiles : 1) : sm * 8;
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
