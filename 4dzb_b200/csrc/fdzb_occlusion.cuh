@@ -39,6 +39,7 @@ namespace fdzb {
 constexpr int kOccWarps = 4;
 constexpr int kOccThreads = kOccWarps * 32;
 constexpr int kOccChunk = FDZB_OCC_CHUNK;
+static_assert(kOccChunk >= 1 && kOccChunk <= 32, "a chunk is staged one triangle per lane");
 constexpr int kItemSamples = FDZB_OCC_ITEM;
 
 // Row words: uint32_t (grids up to 32 x 32, the reference's U32) or
