@@ -476,7 +476,7 @@ __device__ __forceinline__ bool bin_accepts(const uint32_t *binStat, int gbin, c
     return maxz >= c.bz && c.bx < Rx && c.by < Ry && Rz < c.ex && Rw < c.ey;
 }
 
-// Coverage-order bucket of a triangle (secondary pair key): the triangle's
+// Coverage-order bucket of a triangle (the key of the triangle sort): the triangle's
 // angular size seen from below, world area / (f - minz)^2 with f - minz the
 // light-depth distance from the far plane (about the receivers' depth) to the
 // triangle's vertex nearest the light, as a log-scale bucket; the largest
