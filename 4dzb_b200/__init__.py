@@ -64,7 +64,11 @@ EXPORTED = [
     "fdzb_serve_default_config", "fdzb_serve_create", "fdzb_serve_destroy", "fdzb_serve_add_scene",
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
+    "fdzb_ctx_set_launch_epoch", "fdzb_ctx_get_launch_epoch",
 ]
+
+# Launch number at which the look-back status words are cleared (include/fdzb.h).
+LOOKBACK_EPOCH_LIMIT = 0x0FFFFFFF
 
 STAGES = ["setup", "sample_sort", "tri_pairs", "pair_sort", "occlusion"]
 
@@ -256,6 +260,8 @@ def load() -> ctypes.CDLL:
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
         "fdzb_ctx_set_graph": ([vp, i32], i32),
+        "fdzb_ctx_set_launch_epoch": ([vp, ctypes.c_uint32], i32),
+        "fdzb_ctx_get_launch_epoch": ([vp, vp], i32),
         "fdzb_ctx_set_occlusion_schedule": ([vp, i32], i32),
         "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32),
         "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
@@ -379,6 +385,16 @@ class Context:
     def set_graph(self, enable: bool) -> None:
         """Capture launches in a CUDA graph and replay it while the shape holds (default on)."""
         _check(self._lib.fdzb_ctx_set_graph(self._h, int(bool(enable))))
+
+    def set_launch_epoch(self, value: int) -> None:
+        """Testing aid: moves the launch number that tags the look-back words."""
+        _check(self._lib.fdzb_ctx_set_launch_epoch(self._h, int(value)))
+
+    def launch_epoch(self) -> int:
+        """The launch number after the pending launch (testing aid)."""
+        out = ctypes.c_uint32(0)
+        _check(self._lib.fdzb_ctx_get_launch_epoch(self._h, ctypes.byref(out)))
+        return int(out.value)
 
     def set_occlusion_schedule(self, schedule: int) -> None:
         """OCC_LANE_PER_SAMPLE (default) or OCC_LANE_PER_PAIR; results are identical."""

@@ -284,6 +284,27 @@ cudaError_t enqueue_body(Engine &e, int nf)
     return cudaMemcpyAsync(e.hStates, b.states, sizeof(fdzb::FrameState) * nf, cudaMemcpyDeviceToHost, s);
 }
 
+// Clears the look-back status words and the epoch word when the arena's layout
+// moved them or the launch count reached kEpochLimit, then counts this launch.
+// Enqueued on the engine's stream before the launch, outside any graph.
+cudaError_t refresh_lookback(Engine &e)
+{
+    const fdzb::DeviceBuffers &b = e.buf;
+    const auto where = std::make_tuple((const void *)b.sortStatus, b.sortStatusTiles, (const void *)b.triScanStatus,
+                                       b.totalTris, (const void *)b.epochWord);
+    if (where != e.statusLayout || e.epochCount >= kEpochLimit) {
+        const size_t triTiles = ((size_t)std::max(b.totalTris, 1) + fdzb::kTriTileHost - 1) / fdzb::kTriTileHost;
+        cudaError_t err;
+        if ((err = cudaMemsetAsync(b.sortStatus, 0, 8 * 256 * b.sortStatusTiles, e.stream))) return err;
+        if ((err = cudaMemsetAsync(b.triScanStatus, 0, 8 * triTiles, e.stream))) return err;
+        if ((err = cudaMemsetAsync(b.epochWord, 0, sizeof(uint32_t), e.stream))) return err;
+        e.epochCount = 0;
+        e.statusLayout = where;
+    }
+    ++e.epochCount;
+    return cudaSuccess;
+}
+
 }  // namespace
 
 int engine_enqueue(Engine &e)
@@ -392,6 +413,7 @@ int engine_enqueue(Engine &e)
         k.hFrames = e.hFrames;
         k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane;
         k.stream = e.stream;
+        FDZB_CUDA(refresh_lookback(e));
         if (!e.graph || !(k == e.graphKey)) {
             drop_graph(e);
             FDZB_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
@@ -420,6 +442,7 @@ int engine_enqueue(Engine &e)
         FDZB_CUDA(cudaEventRecord(e.ev1, e.stream));
         e.lastFromGraph = true;
     } else {
+        FDZB_CUDA(refresh_lookback(e));
         FDZB_CUDA(cudaEventRecord(e.ev0, e.stream));
         FDZB_CUDA(enqueue_body(e, nf));
         FDZB_CUDA(cudaEventRecord(e.ev1, e.stream));
@@ -981,6 +1004,28 @@ int fdzb_ctx_set_graph(fdzb_ctx *c, int enable)
     if (int rc = ctx_sync(c)) return rc;
     c->eng.useGraph = enable != 0;
     if (!c->eng.useGraph) drop_graph(c->eng);
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_launch_epoch(fdzb_ctx *c, uint32_t value)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (!c->eng.arena) return fail(FDZB_ERR_NOT_READY, "no launch yet");
+    if (value >= kEpochLimit) return fail(FDZB_ERR_INVALID_ARG, "epoch must be below FDZB_LOOKBACK_EPOCH_LIMIT");
+    if (int rc = ctx_sync(c)) return rc;
+    FDZB_CUDA(cudaMemcpyAsync(c->eng.buf.epochWord, &value, sizeof(value), cudaMemcpyHostToDevice, c->eng.stream));
+    FDZB_CUDA(cudaStreamSynchronize(c->eng.stream));
+    c->eng.epochCount = value;
+    return FDZB_OK;
+}
+
+int fdzb_ctx_get_launch_epoch(fdzb_ctx *c, uint32_t *out)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (!out) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    if (!c->eng.arena) return fail(FDZB_ERR_NOT_READY, "no launch yet");
+    if (int rc = ctx_sync(c)) return rc;
+    FDZB_CUDA(cudaMemcpy(out, c->eng.buf.epochWord, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return FDZB_OK;
 }
 

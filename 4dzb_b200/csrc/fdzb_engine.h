@@ -97,7 +97,18 @@ struct Engine {
     GraphKey graphKey{};
     bool lastFromGraph = false;
     long long graphCaptures = 0, graphReplays = 0;
+    // Look-back tags: launches since the status words were last cleared (the
+    // device epoch word, advanced by k_init, holds the same count).  The words
+    // are cleared when the arena is laid out anew (they may then hold other
+    // buffers' bytes) and before the count reaches kEpochLimit, so a tag never
+    // wraps round to the tag of a stale word.
+    uint32_t epochCount = 0;
+    std::tuple<const void *, size_t, const void *, int, const void *> statusLayout{};
 };
+
+// Launches between two clearings of the look-back words: the sort tags are
+// epoch * 16 + (4 x sort slot + pass) in 32 bits, so the epoch stays below 2^28.
+constexpr uint32_t kEpochLimit = FDZB_LOOKBACK_EPOCH_LIMIT;
 
 int engine_init(Engine &e, int device);
 void engine_release(Engine &e);

@@ -935,16 +935,19 @@ cudaError_t measure_alu_rate(double *rate)
 // allocation (and the device synchronisation cudaFree implies) is not allowed.
 // For them, fdzb_sort_pairs_noalloc sorts with a fixed scratch area compiled
 // into the library as a file-scope device array: every GPU that loads the
-// library holds it (about 8.5 MB) until the process exits.
+// library holds it (kNoAllocBytes = 8,917,264 bytes: 8.92 MB, 8.50 MiB)
+// until the process exits.
 //
 // The array is a device symbol: in host code its name is only a stand-in, so
 // the first call on each device looks up its device address with
 // cudaGetSymbolAddress (with that device current) and passes the pointer to the
 // kernels.  That first call should therefore come before any stream capture.
-// All calls share the array and it keeps the last call's contents: the
-// histogram, tickets and error word are cleared at the start of every call,
-// and the look-back words carry a per-call tag.  Calls that overlap on the GPU
-// (two streams, two host threads on one device) race on the array.
+// All calls share the array and it keeps the last call's contents, so every
+// call starts by clearing, on its stream, the histogram, tickets, error word
+// and the look-back words of the tiles it uses; the look-back tags are then
+// just the pass numbers, and nothing a call does depends on host-side state
+// left by earlier calls.  Calls that overlap on the GPU (two streams, two host
+// threads on one device) race on the array.
 // ---------------------------------------------------------------------------
 namespace fdzb {
 namespace {
@@ -953,22 +956,29 @@ constexpr int kNoAllocMaxPairs = 1 << 20;   // FDZB_NOALLOC_SORT_MAX_PAIRS
 constexpr int kNoAllocTiles = (kNoAllocMaxPairs + kSortTile - 1) / kSortTile;
 constexpr size_t kNoAllocKeysOff = 0;
 constexpr size_t kNoAllocValsOff = kNoAllocKeysOff + 4ull * kNoAllocMaxPairs;
-constexpr size_t kNoAllocStatusOff = kNoAllocValsOff + 4ull * kNoAllocMaxPairs;
-constexpr size_t kNoAllocHistOff = kNoAllocStatusOff + 8ull * kNoAllocTiles * kRadix;
+constexpr size_t kNoAllocHistOff = kNoAllocValsOff + 4ull * kNoAllocMaxPairs;
 constexpr size_t kNoAllocTicketOff = kNoAllocHistOff + 4ull * 4 * kRadix;
 constexpr size_t kNoAllocErrOff = kNoAllocTicketOff + 4ull * 4;
-constexpr size_t kNoAllocBytes = kNoAllocErrOff + 256;
+constexpr size_t kNoAllocStatusOff = kNoAllocErrOff + 256;
+constexpr size_t kNoAllocBytes = kNoAllocStatusOff + 8ull * kNoAllocTiles * kRadix;
+static_assert(kNoAllocBytes == 8917264, "scratch size quoted in the comments and the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[kNoAllocMaxDevices];
-uint32_t g_noalloc_epoch[kNoAllocMaxDevices];
 
 __global__ void k_noalloc_status(const int *err, int32_t *status)
 {
     *status = *err;
+}
+
+// True if the byte ranges [a, a + na) and [b, b + nb) share a byte.
+bool overlaps(const void *a, size_t na, const void *b, size_t nb)
+{
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return na && nb && x < y + nb && y < x + na;
 }
 
 }  // namespace
@@ -985,14 +995,22 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
     if (key_range == 0) return set_error(-1, "fdzb_sort_pairs_noalloc: key_range must be positive");
     if (n > 0 && (!d_keys_in || !d_vals_in || !d_keys_out || !d_vals_out))
         return set_error(-1, "fdzb_sort_pairs_noalloc: NULL buffer");
-    if (n > 0 && (d_keys_in == d_keys_out || d_vals_in == d_vals_out || d_keys_out == d_vals_out))
-        return set_error(-1, "fdzb_sort_pairs_noalloc: outputs must not alias the inputs or each other");
+    if (n > 0) {
+        // an output may share no byte with an input, the other output or the status word
+        const size_t nb = 4ull * (size_t)n;
+        const bool bad = overlaps(d_keys_out, nb, d_keys_in, nb) || overlaps(d_keys_out, nb, d_vals_in, nb) ||
+                         overlaps(d_keys_out, nb, d_vals_out, nb) || overlaps(d_vals_out, nb, d_keys_in, nb) ||
+                         overlaps(d_vals_out, nb, d_vals_in, nb) ||
+                         (d_status && (overlaps(d_keys_out, nb, d_status, 4) || overlaps(d_vals_out, nb, d_status, 4)));
+        if (bad)
+            return set_error(-1, "fdzb_sort_pairs_noalloc: outputs must not overlap the inputs, each other "
+                                 "or the status word");
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_error(-2, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(-7, "device index out of range");
     unsigned char *base = nullptr;
-    uint32_t epoch = 0;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
         if (!g_noalloc_ptr[dev]) {
@@ -1003,17 +1021,18 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
             g_noalloc_ptr[dev] = (unsigned char *)p;
         }
         base = g_noalloc_ptr[dev];
-        epoch = ++g_noalloc_epoch[dev];
     }
     cudaStream_t s = (cudaStream_t)stream;
     uint32_t *tmpK = (uint32_t *)(base + kNoAllocKeysOff);
     uint32_t *tmpV = (uint32_t *)(base + kNoAllocValsOff);
-    unsigned long long *status = (unsigned long long *)(base + kNoAllocStatusOff);
     uint32_t *hist = (uint32_t *)(base + kNoAllocHistOff);
     int *tickets = (int *)(base + kNoAllocTicketOff);
     int *err = (int *)(base + kNoAllocErrOff);
-    // histogram, tickets and error word start at zero every call
-    e = cudaMemsetAsync(hist, 0, kNoAllocErrOff + sizeof(int) - kNoAllocHistOff, s);
+    unsigned long long *status = (unsigned long long *)(base + kNoAllocStatusOff);
+    const long long tiles = ((long long)n + kSortTile - 1) / kSortTile;
+    // histogram, tickets, error word and the look-back words of the tiles in
+    // use start at zero every call (one contiguous range, at most 0.5 MiB)
+    e = cudaMemsetAsync(hist, 0, kNoAllocStatusOff - kNoAllocHistOff + 8ull * kRadix * (size_t)tiles, s);
     if (e != cudaSuccess) return set_error(-2, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     const int passes = sort_passes_for((long long)key_range);
     if (n > 0) {
@@ -1021,16 +1040,16 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
         k_radix_hist<<<grid_for(n, kSortThreads, sm * 4), kSortThreads, 0, s>>>(d_keys_in, nullptr, n, n,
                                                                                   passes, hist);
         // destinations alternate so that the last pass lands in the outputs
-        const long long tiles = ((long long)n + kSortTile - 1) / kSortTile;
         const int grid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
         const uint32_t *ki = d_keys_in, *vi = d_vals_in;
         for (int p = 0; p < passes; ++p) {
             const bool toOut = ((passes - 1 - p) % 2) == 0;
             uint32_t *ko = toOut ? d_keys_out : tmpK;
             uint32_t *vo = toOut ? d_vals_out : tmpV;
+            // tag p + 1: the cleared words (tag 0) and the words of this call's
+            // earlier passes both read as unpublished
             k_radix_pass<<<grid, kSortThreads, 0, s>>>(ki, vi, ko, vo, nullptr, n, n, 8 * p,
-                                                       hist + p * kRadix, status, nullptr,
-                                                       epoch * 8u + (uint32_t)p,
+                                                       hist + p * kRadix, status, nullptr, (uint32_t)p + 1u,
                                                        tickets + p, err);
             ki = ko;
             vi = vo;

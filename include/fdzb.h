@@ -377,6 +377,19 @@ const char *fdzb_version(void);
  * stream. */
 int fdzb_ctx_set_graph(fdzb_ctx *ctx, int enable);
 
+/* Testing aids, no counterpart in the reference.  The sorts' decoupled
+ * look-back tags its status words with the context's launch number (a device
+ * word advanced by every launch; FS/api.cpp:402-582 has no look-back: Thrust's
+ * sorts run there).  The words are never cleared between launches, except
+ * when the arena is laid out anew and before the launch number reaches
+ * FDZB_LOOKBACK_EPOCH_LIMIT, when they and the number restart from zero, so a
+ * tag never wraps round to a stale word's.  set_launch_epoch moves the number
+ * (after a first launch; value < the limit) so that tests can cross that
+ * point; get_launch_epoch reads it after the pending launch. */
+#define FDZB_LOOKBACK_EPOCH_LIMIT 0x0FFFFFFFu
+int fdzb_ctx_set_launch_epoch(fdzb_ctx *ctx, uint32_t value);
+int fdzb_ctx_get_launch_epoch(fdzb_ctx *ctx, uint32_t *out);
+
 /* ---- batches: many independent frames per launch ------------------------- */
 
 /* No counterpart in the reference, which renders one frame per FD::FDLaunch
@@ -539,20 +552,23 @@ const char *fdzb_serve_last_worker_error(fdzb_server *server);
  * path, a host process that owns every allocation, a real-time loop that may
  * not synchronise for cudaFree -- this sorts n (key, value) uint32 pairs by key,
  * stably (equal keys keep their input order), keys < key_range, using only a
- * fixed scratch area built into the library (about 8.9 MB of device memory on
- * every GPU that loads libfdzb.so, held until the process exits).  It is the
- * same radix sort the frame pipeline runs on its own arena.
+ * fixed scratch area built into the library (8,917,264 bytes = 8.92 MB =
+ * 8.50 MiB of device memory on every GPU that loads libfdzb.so, held until the
+ * process exits).  It is the same radix sort the frame pipeline runs on its own
+ * arena.
  *  - n at most FDZB_NOALLOC_SORT_MAX_PAIRS; larger n is rejected
  *    (FDZB_ERR_INVALID_ARG) before any work is enqueued;
- *  - inputs are not modified; outputs must not alias inputs or each other;
+ *  - inputs are not modified; an output that shares any byte with an input,
+ *    the other output or d_status is rejected (FDZB_ERR_INVALID_ARG);
  *  - work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
  *    stream) and the call returns without waiting; d_status (device int32,
  *    nullable) receives 0, or nonzero if a bounded device wait gave up;
  *  - the first call on a device looks up the scratch area's device address
  *    with cudaGetSymbolAddress, so make it before any stream capture;
- *  - every call reuses the same scratch area: calls that overlap on the GPU
- *    (other streams or threads on the same device) race and must be ordered by
- *    the caller;
+ *  - every call reuses the same scratch area and clears the parts it needs
+ *    (on `stream`, before its kernels); calls that overlap on the GPU (other
+ *    streams or threads on the same device) race and must be ordered by the
+ *    caller;
  *  - no cudaMalloc, cudaFree or other allocating routine is called. */
 #define FDZB_NOALLOC_SORT_MAX_PAIRS (1 << 20)
 int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t *d_vals_in,

@@ -20,11 +20,20 @@ def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0):
     ctx, t = fdzb.context_for_scene(scene, masks=masks, debug=True, tri_order=tri_order)
     ctx.set_occlusion_schedule(schedule)
     ms = ctx.launch()
+    res = collect(ctx, t, scene, ms=ms, tri_order=tri_order)
+    ctx.close()
+    return res
+
+
+def collect(ctx, t, scene, ms=None, tri_order: int = 0, intermediates: bool = True):
+    """(outputs dict, stats dict, exported intermediates dict) of the last launch
+    of a Context made by context_for_scene (t: its tensors); intermediates need
+    a debug Context."""
     st = ctx.stats()
     S, T, NB = scene.S, scene.T, scene.bins * scene.bins
     P = st["num_pairs"] if st["state"] == 2 else 0
     ex = {}
-    if st["state"] == 2:
+    if st["state"] == 2 and intermediates:
         for name, n in (("sample_keys", S), ("sorted_sample_keys", S), ("sorted_sample_ids", S),
                         ("bin_sample_start", NB + 1), ("bin_sample_end", NB + 1), ("bin_maxz", NB),
                         ("bin_range", 4 * NB), ("tri_count", T), ("pair_bin", P), ("pair_tri", P),
@@ -32,9 +41,8 @@ def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0):
                         ("bin_tri_end", NB), ("tri_aabb", 8 * T)):
             ex[name] = ctx.export(name, n)
     out = dict(shadow=t["shadow"].cpu().numpy(), ms=ms, tri_order=tri_order)
-    if masks:
+    if t.get("masks") is not None:
         out["masks"] = t["masks"].cpu().numpy().view(np.uint32).reshape(S, -1)
-    ctx.close()
     return out, st, ex
 
 

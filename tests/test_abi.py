@@ -130,3 +130,24 @@ def test_batch_struct_layouts(fdzb):
     assert ctypes.sizeof(fdzb.RasterDesc) == 240
     assert ctypes.sizeof(fdzb.RasterStats) == 64
     assert fdzb.FrameDesc.light.offset == 64 and fdzb.FrameDesc.d_shadow.offset == 128
+
+
+def test_noalloc_sort_rejects_overlapping_buffers(fdzb):
+    """The allocation-free sort refuses outputs that share bytes with an input,
+    the other output or the status word; the check runs before any CUDA call,
+    so plain addresses suffice here."""
+    lib = fdzb.load()
+    fn = lib.fdzb_sort_pairs_noalloc
+    fn.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    n = 16                       # 64 bytes per array
+    ki, vi, ko, vo = 0x100000, 0x200000, 0x300000, 0x400000
+    bad = [(ki, vi, ki + 32, vo, None),          # keys_out overlaps keys_in
+           (ki, vi, vi, vo, None),               # keys_out == vals_in
+           (ki, vi, ko, ki, None),               # vals_out == keys_in
+           (ki, vi, ko, vi + 60, None),          # vals_out overlaps the end of vals_in
+           (ki, vi, ko, ko + 4, None),           # outputs overlap each other
+           (ki, vi, ko, vo, vo + 8)]             # status word inside vals_out
+    for a, b, c, d, st in bad:
+        assert fn(a, b, c, d, n, 64, None, st) == -1
+        assert b"overlap" in lib.fdzb_last_error()
