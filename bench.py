@@ -204,12 +204,17 @@ def reference_arm(args, scene) -> dict:
             ref.run(crop, nthreads=threads)
             cal.append(time.time() - t0)
         t_cal = statistics.mean(cal)
-        times = []
+        times, walls = [], []
         for _ in range(args.steps):
             t0 = time.time()
             ref.run(crop, nthreads=threads)
-            times.append(t_full * (time.time() - t0) / t_cal)
+            walls.append(time.time() - t0)
+            times.append(t_full * walls[-1] / t_cal)
         kind = "reference"
+        steps_are = (f"extrapolated: each timed step runs the central {crop.W}x{crop.H} crop (1/16 of the "
+                     f"samples, all triangles) in {1e3 * statistics.mean(walls):.0f} ms of wall time and is "
+                     f"scaled to a full frame by the warm-up's measured full-frame / crop ratio "
+                     f"({t_full:.2f} s / {t_cal:.2f} s); ms_per_step is that full-frame estimate")
         sample = (f"reference sources on the CPU ({threads} threads, 16x16 bins): one full "
                   f"{scene.W}x{scene.H} frame in warm-up ({t_full:.1f} s), then {args.steps} central "
                   f"{crop.W}x{crop.H} crops (1/16 of the samples, all triangles) scaled to the full frame")
@@ -225,8 +230,11 @@ def reference_arm(args, scene) -> dict:
             if i >= args.warmup:
                 times.append((dt - t_occ) + t_occ * stride)
         kind = "port"
+        walls = list(times)
         sample = (f"binned FP32 port of the reference pipeline ({threads} threads); occlusion on every "
                   f"{stride}th binned sample, extrapolated")
+        steps_are = (f"extrapolated: each step runs the binned port with occlusion on every {stride}th binned "
+                     f"sample and scales the occlusion time by {stride}")
     ms = 1e3 * statistics.mean(times)
     v = 1e3 / ms
     gpu = reference_gpu(args, scene)
@@ -238,36 +246,70 @@ def reference_arm(args, scene) -> dict:
                        "light_grid": scene.light.n, "bins": scene.bins},
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "extrapolated": True, "steps_are": steps_are,
+            "measured_ms_per_step": 1e3 * statistics.mean(walls),
             "reference_gpu": gpu}
+
+
+def _ref_gpu_timing(ref_gpu, scene, args, fmad: bool, bins: int) -> dict:
+    """W untimed and K timed FDLaunch frames of one reference build."""
+    r = ref_gpu.run(scene, fmad=fmad, warmup=args.warmup, reps=args.steps, checked=True, bins=bins)
+    t = [float(x) for x in r["launch_ms"]]
+    st = r["stage_ms"]
+    stages = {}
+    for j, name in enumerate(ref_gpu.STAGES):
+        col = [float(v) for v in st[:, j] if v >= 0]
+        if col:
+            stages[name] = {"median_ms": statistics.median(col), "mean_ms": statistics.mean(col)}
+    med = statistics.median(t)
+    return {"value": 1e3 / med, "unit": "frames/s", "median_ms": med, "mean_ms": statistics.mean(t),
+            "min_ms": min(t), "max_ms": max(t), "frames": len(t), "bins": bins,
+            "fmad": fmad, "num_pairs": int(r["num_pairs"]), "stages": stages,
+            "frame_ms": [round(x, 3) for x in t]}
 
 
 def reference_gpu(args, scene) -> dict:
     """The reference's own CUDA sources (FS/api.cpp + K/*.inl) built for sm_100a
-    with nvcc's defaults (oracle/_ref/libref4dzb_gpu_fmad.so), run on this
-    process's GPU through FDLaunch on the same scene: W untimed and K timed
-    frames, each timed with CUDA events around FDLaunch after an L2 flush.  Its
-    bins are the compile-time 16 x 16.  The scene passes the CPU preflight first
-    (keys inside the bin grid, pairs inside the reference's pair buffers)."""
+    (oracle/_ref/libref4dzb_gpu*.so), run on this process's GPU through its own
+    FDLaunch on the same scene: W untimed and K timed frames, each timed with
+    CUDA events around FDLaunch after a 256 MB L2 flush, and per stage with
+    events around the five stage drivers FDLaunch calls.  Timed at the scene's
+    own bin grid (the product's configuration; the reference's compile-time
+    bin constant rebuilt to it) with nvcc's default --fmad=true, the build
+    the reference project ships, and with --fmad=false (the bit-exact build);
+    and at the reference's own 16 x 16 bins with --fmad=true.  The value is
+    the median frame; mean, min and max are beside it.  Each scene passes the
+    CPU preflight first (keys inside the bin grid, pairs inside the
+    reference's pair buffers)."""
     from oracle import ref_gpu
-    if not ref_gpu.available(fmad=True):
-        return {"unavailable": "oracle/_ref/libref4dzb_gpu_fmad.so not built (needs the reference sources)"}
     try:
         import torch
         if not torch.cuda.is_available():
             return {"unavailable": "no CUDA device"}
     except ImportError:
         return {"unavailable": "torch missing"}
-    try:
-        ref_gpu.preflight(scene, occ_stride=256)
-    except ref_gpu.PreflightError as e:
-        return {"unavailable": f"preflight refused the scene: {e}"}
-    r = ref_gpu.run(scene, fmad=True, warmup=args.warmup, reps=args.steps, checked=True)
-    t = [float(x) for x in r["launch_ms"]]
-    ms = statistics.mean(t)
-    return {"value": 1e3 / ms, "unit": "frames/s", "ms_per_frame": ms, "min_ms": min(t), "max_ms": max(t),
-            "frames": len(t), "bins": ref_gpu.REF_BINS, "num_pairs": int(r["num_pairs"]),
-            "build": "reference sources, nvcc 12.9 -O3 sm_100a, default --fmad=true",
-            "timing": "CUDA events around each FDLaunch; 256 MB L2 flush before each"}
+    runs = []
+    for fmad, bins in ((True, scene.bins), (False, scene.bins), (True, ref_gpu.REF_BINS)):
+        if not ref_gpu.available(fmad=fmad, bins=bins):
+            runs.append({"bins": bins, "fmad": fmad,
+                         "unavailable": f"oracle/_ref reference build at {bins}^2 bins not built"})
+            continue
+        try:
+            ref_gpu.preflight(scene, occ_stride=256, bins=bins)
+        except ref_gpu.PreflightError as e:
+            runs.append({"bins": bins, "fmad": fmad, "unavailable": f"preflight refused the scene: {e}"})
+            continue
+        runs.append(_ref_gpu_timing(ref_gpu, scene, args, fmad, bins))
+    head = runs[0]
+    if "unavailable" in head:
+        return {"unavailable": head["unavailable"], "runs": runs}
+    out = dict(head)
+    out["same_config"] = head["bins"] == scene.bins
+    out["build"] = "reference sources, nvcc 12.9 -O3 sm_100a, default --fmad=true"
+    out["timing"] = ("CUDA events around each FDLaunch and its five stage drivers; 256 MB L2 flush "
+                     "before each frame; value = 1000 / median frame ms")
+    out["runs"] = runs
+    return out
 
 
 def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> dict:

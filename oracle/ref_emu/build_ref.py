@@ -2,7 +2,7 @@
 """Build recipe of the reference harness: 4DZB's own soft-shadow sources,
 compiled for the CPU into oracle/_ref/libref4dzb.so (test infrastructure).
 
-Reads the reference where it lies (default /root/reference, or $FDZB_REFERENCE)
+Reads the reference where it lies (oracle/refpath.py: $FDZB_REFERENCE or its default)
 and writes only into oracle/_ref/.  Nothing from the reference is copied into
 the repository:
 
@@ -31,7 +31,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(ORACLE, "_ref")
 LIB = os.path.join(OUT_DIR, "libref4dzb.so")
-REF = os.environ.get("FDZB_REFERENCE", "/root/reference")
+sys.path.insert(0, ORACLE)
+from refpath import reference_root  # noqa: E402
+
+REF = reference_root()
 FS = os.path.join(REF, "4DZB", "FDZB_Soft_Shadow")
 K = os.path.join(FS, "cuda")
 

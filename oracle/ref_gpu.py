@@ -2,13 +2,15 @@
 soft-shadow sources (4DZB/FDZB_Soft_Shadow) compiled for sm_100a by
 oracle/ref_gpu/build_ref_gpu.py.  TEST INFRASTRUCTURE ONLY: it pins the product
 against the reference running on the same GPU, and times the reference's GPU
-frame.  Its bin grid is the reference's compile-time 16 x 16 (FS/constants.h:13).
+frame.  The reference fixes its bin grid at compile time (FS/constants.h:13,
+16 x 16); the harness is built at 16 x 16, 32 x 32 and 128 x 128 (BUILT_BINS),
+each with --fmad=false (exact) and nvcc's default --fmad=true.
 
 Every input is checked on the CPU first (preflight): the oracle, run with the
-same 16 x 16 bins and the reference's triangle order, must show that every
-sample key stays inside the bin grid and that the triangle/bin pairs fit the
-reference's fixed pair buffers (FS/constants.h:15, FS/api.cpp:132-138); the
-light must be square with N <= 32 (the only form the per-sample kernel runs,
+same bins and the reference's triangle order, must show that every sample key
+stays inside the bin grid and that the triangle/bin pairs fit the reference's
+fixed pair buffers (FS/constants.h:15, FS/api.cpp:132-138); the light must be
+square with N <= 32 (the only form the per-sample kernel runs,
 K/Step5_2_shadowCalPerSample.inl:249-254).  An input that fails is refused
 before anything reaches the GPU.
 """
@@ -20,9 +22,10 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_EXACT = os.path.join(HERE, "_ref", "libref4dzb_gpu.so")
-LIB_FMAD = os.path.join(HERE, "_ref", "libref4dzb_gpu_fmad.so")
-REF_BINS = 16
+REF_BINS = 16                 # the reference's own compile-time grid
+BUILT_BINS = (16, 32, 128)
+# the reference's five stage drivers, in FDLaunch's order (FS/api.cpp:495-552)
+STAGES = ["lightPlaneParamCal", "bindSampleToBin", "countTriBinPairNum", "bindTriToBin", "shadowCal_perSample"]
 # FD_MAX_BT_PIAR_Num * 1.4 (FS/constants.h:15, FS/api.cpp:132-138)
 PAIR_BUFFER = int(50 * 1024 * 1024 * 1.4)
 
@@ -47,37 +50,42 @@ class RefGpuOut(ctypes.Structure):
                 ("lp_factor", ctypes.c_float * 2), ("sample_aabb", ctypes.c_float * 8),
                 ("model_aabb", ctypes.c_float * 8), ("first_error", ctypes.c_char * 160),
                 ("surf_handle", ctypes.c_int64), ("pos_tex_handle", ctypes.c_int64), ("view_error", ctypes.c_int64),
-                ("masks", ctypes.POINTER(ctypes.c_uint32))]
+                ("masks", ctypes.POINTER(ctypes.c_uint32)), ("stage_ms", f32p), ("bins", ctypes.c_int32),
+                ("pad0", ctypes.c_int32)]
 
 
 _libs: dict = {}
 
 
-def lib_path(fmad: bool) -> str:
-    return LIB_FMAD if fmad else LIB_EXACT
+def lib_path(fmad: bool = False, bins: int = REF_BINS) -> str:
+    tag = "" if bins == REF_BINS else f"_b{bins}"
+    return os.path.join(HERE, "_ref", f"libref4dzb_gpu{tag}{'_fmad' if fmad else ''}.so")
 
 
-def available(fmad: bool = False) -> bool:
-    return os.path.exists(lib_path(fmad))
+def available(fmad: bool = False, bins: int = REF_BINS) -> bool:
+    return bins in BUILT_BINS and os.path.exists(lib_path(fmad, bins))
 
 
-def load(fmad: bool = False) -> ctypes.CDLL:
-    if fmad not in _libs:
-        lib = ctypes.CDLL(lib_path(fmad), mode=ctypes.RTLD_LOCAL)
+def load(fmad: bool = False, bins: int = REF_BINS) -> ctypes.CDLL:
+    key = (fmad, bins)
+    if key not in _libs:
+        if bins not in BUILT_BINS:
+            raise ValueError(f"no reference build at {bins} x {bins} bins (built: {BUILT_BINS})")
+        lib = ctypes.CDLL(lib_path(fmad, bins), mode=ctypes.RTLD_LOCAL)
         lib.ref_gpu_frame.argtypes = [ctypes.POINTER(RefGpuIn), ctypes.POINTER(RefGpuOut)]
         lib.ref_gpu_frame.restype = ctypes.c_int
-        _libs[fmad] = lib
-    return _libs[fmad]
+        _libs[key] = lib
+    return _libs[key]
 
 
 class PreflightError(RuntimeError):
     pass
 
 
-def preflight(scene, occ_stride: int = 64) -> dict:
-    """Check on the CPU, with the oracle at the reference's 16 x 16 bins, that a
-    scene stays inside the reference's buffers.  occ_stride thins the oracle's
-    occlusion stage (the checked quantities come from the binning stages)."""
+def preflight(scene, occ_stride: int = 64, bins: int = REF_BINS) -> dict:
+    """Check on the CPU, with the oracle at the build's bins, that a scene stays
+    inside the reference's buffers.  occ_stride thins the oracle's occlusion
+    stage (the checked quantities come from the binning stages)."""
     import dataclasses
 
     from . import orc
@@ -86,27 +94,31 @@ def preflight(scene, occ_stride: int = 64) -> dict:
     if scene.light.cols != n or not (1 < n <= 32):
         raise PreflightError(f"light grid {n} x {scene.light.cols}: the per-sample kernel runs 2..32 "
                              "square grids only")
-    s16 = dataclasses.replace(scene, bins=REF_BINS)
-    fr = orc.frame(s16, occ_stride=occ_stride)
+    if bins not in BUILT_BINS:
+        raise PreflightError(f"no reference build at {bins} x {bins} bins")
+    sb = dataclasses.replace(scene, bins=bins)
+    fr = orc.frame(sb, occ_stride=occ_stride)
     sc = fr.scalars
     if sc["quirk_key_range"]:
-        raise PreflightError(f"{sc['quirk_key_range']} sample keys outside the {REF_BINS} x {REF_BINS} grid")
-    if sc["num_pairs"] + REF_BINS * REF_BINS > PAIR_BUFFER:
+        raise PreflightError(f"{sc['quirk_key_range']} sample keys outside the {bins} x {bins} grid")
+    if sc["num_pairs"] + bins * bins > PAIR_BUFFER:
         raise PreflightError(f"{sc['num_pairs']} triangle/bin pairs exceed the reference's pair buffer")
     return sc
 
 
 def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool = False,
-        masks: bool = False) -> dict:
-    """Frames through the reference on the current GPU (device 0 of this process).
-    The shadow buffer of the last launch is returned at y*W+x; launch_ms holds
-    the CUDA-event time of each timed FDLaunch (L2 flushed before each).  With
+        masks: bool = False, bins: int = REF_BINS) -> dict:
+    """Frames through the reference on the current GPU (device 0 of this process),
+    built at bins x bins light-plane bins.  The shadow buffer of the last launch
+    is returned at y*W+x; launch_ms holds the CUDA-event time of each timed
+    FDLaunch (L2 flushed before each), stage_ms [reps, 5] the time of each of
+    its stage drivers (STAGES; -1 where one did not run).  With
     masks, "mask_rows" holds each sample's N light-row words as the reference's
     per-sample kernel left them ([S, N] uint32 at y*W+x) and "mask_written"
     where that kernel ran (binned samples)."""
     if not checked:
-        preflight(scene)
-    lib = load(fmad)
+        preflight(scene, bins=bins)
+    lib = load(fmad, bins)
     pos = np.ascontiguousarray(scene.pos, np.float32)
     nrm = np.ascontiguousarray(scene.nrm, np.float32)
     vtx = np.ascontiguousarray(scene.vtx, np.float32)
@@ -136,15 +148,20 @@ def run(scene, fmad: bool = False, warmup: int = 0, reps: int = 1, checked: bool
     ro.shadow = shadow.ctypes.data_as(f32p)
     ro.launch_ms = launch_ms.ctypes.data_as(f32p)
     ro.fdlaunch_ms = own_ms.ctypes.data_as(f32p)
+    stage_ms = np.full(reps * len(STAGES), -1.0, np.float32)
+    ro.stage_ms = stage_ms.ctypes.data_as(f32p)
     rc = lib.ref_gpu_frame(ctypes.byref(ri), ctypes.byref(ro))
     out = {"shadow": shadow, "launch_ms": launch_ms, "fdlaunch_ms": own_ms, "rc": rc,
+           "stage_ms": stage_ms.reshape(reps, len(STAGES)),
            "first_error": ro.first_error.decode(errors="replace")}
     for name, _ in RefGpuOut._fields_:
         v = getattr(ro, name)
         if isinstance(v, (int, float)):
             out[name] = v
-        elif hasattr(v, "_length_") and not hasattr(v, "contents") and name != "first_error":
+        elif hasattr(v, "_length_") and not hasattr(v, "contents") and name not in ("first_error", "stage_ms"):
             out[name] = np.array(list(v), np.float32)
+    if rc == 0 and out.get("bins") != bins:
+        raise RuntimeError(f"reference build reports {out.get('bins')} bins, expected {bins}")
     if rc:
         raise RuntimeError(f"reference GPU frame failed: {out['errors']} CUDA errors, first: {out['first_error']}")
     if masks:

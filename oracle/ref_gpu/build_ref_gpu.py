@@ -2,15 +2,24 @@
 """Build recipe of the reference GPU harness: 4DZB's own soft-shadow sources,
 compiled for sm_100a into oracle/_ref/ (test infrastructure).
 
-Two libraries, same sources:
+Six libraries, same sources, at three bin grids and two FMA settings:
 
 * libref4dzb_gpu.so      -- --fmad=false: every float expression is the IEEE
   sequence of operations the source spells, so its shadows can be compared
   bit for bit with the oracle and with libfdzb.so;
 * libref4dzb_gpu_fmad.so -- nvcc's default --fmad=true, as the reference's own
-  project builds it: the timing build.
+  project builds it: the timing build;
+* libref4dzb_gpu_b32[_fmad].so, libref4dzb_gpu_b128[_fmad].so -- the same at
+  32 x 32 and 128 x 128 light-plane bins.  The reference fixes its bin grid at
+  compile time (FD_MAX_LP_GRID_SIZE_LOG2 = 4, FS/constants.h:13); these builds
+  set it to 5 and 7, the grids of the small and HD workloads.  The edit is made
+  on a temporary copy of FS/constants.h, next to a temporary verbatim copy of
+  FS/api.cpp (its quoted #include "constants.h" then finds the edited copy;
+  the kernel translation unit includes it first, and the header's include
+  guard keeps the original out).  Both copies live under oracle/_ref/ while the
+  build runs and are deleted after it.
 
-Reads the reference where it lies (default /root/reference, or $FDZB_REFERENCE)
+Reads the reference where it lies (oracle/refpath.py: $FDZB_REFERENCE or its default)
 and writes only into oracle/_ref/.  Nothing from the reference is copied into
 the repository:
 
@@ -46,9 +55,21 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(ORACLE, "_ref")
-LIB_EXACT = os.path.join(OUT_DIR, "libref4dzb_gpu.so")
-LIB_FMAD = os.path.join(OUT_DIR, "libref4dzb_gpu_fmad.so")
-REF = os.environ.get("FDZB_REFERENCE", "/root/reference")
+sys.path.insert(0, ORACLE)
+from refpath import reference_root  # noqa: E402
+
+# log2 of the bins per side of each build: 16 (the reference's own), 32, 128
+BIN_LOG2S = (4, 5, 7)
+
+
+def lib_name(bins_log2: int, fmad: bool) -> str:
+    tag = "" if bins_log2 == 4 else f"_b{1 << bins_log2}"
+    return os.path.join(OUT_DIR, f"libref4dzb_gpu{tag}{'_fmad' if fmad else ''}.so")
+
+
+LIB_EXACT = lib_name(4, False)
+LIB_FMAD = lib_name(4, True)
+REF = reference_root()
 FS = os.path.join(REF, "4DZB", "FDZB_Soft_Shadow")
 K = os.path.join(FS, "cuda")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -107,6 +128,24 @@ def kernel_source() -> str:
     return "".join(parts)
 
 
+CONST_LINE = "const int FD_MAX_LP_GRID_SIZE_LOG2 = 4;"
+
+
+def constants_source(bins_log2: int) -> str:
+    """FS/constants.h with the bin-grid constant set to bins_log2 (the line must
+    appear exactly once)."""
+    text = _read(os.path.join(FS, "constants.h"))
+    out, hits = [], 0
+    for line in text.splitlines():
+        if line.strip().startswith(CONST_LINE):
+            line = line.replace(CONST_LINE, f"const int FD_MAX_LP_GRID_SIZE_LOG2 = {bins_log2};")
+            hits += 1
+        out.append(line)
+    if hits != 1:
+        raise RuntimeError(f"bin-grid constant matched {hits} times in constants.h (expected 1)")
+    return "\n".join(out) + "\n"
+
+
 def build(verbose: bool = False) -> list[str]:
     if not os.path.isdir(K):
         raise FileNotFoundError(f"reference sources not found under {REF}")
@@ -125,40 +164,66 @@ def build(verbose: bool = False) -> list[str]:
             raise RuntimeError(f"reference GPU harness build failed: {' '.join(cmd[:4])} ...")
 
     force = ["-include", os.path.join(HERE, "refgpu.h")]
-    host_objs = []
-    for src in HOST_SOURCES + [os.path.join(HERE, "gl_runtime.cpp")]:
-        o = os.path.join(OUT_DIR, "gpu_" + os.path.splitext(os.path.basename(src))[0] + ".o")
-        if os.path.basename(src) == "api.cpp":
+    work = os.path.join(OUT_DIR, "gpu_build")
+    os.makedirs(work, exist_ok=True)
+    kernels = kernel_source()
+    api_text = _read(os.path.join(FS, "api.cpp"))
+    libs, temps = [], []
+    try:
+        # host sources without the bin grid, once
+        common = []
+        for src in HOST_SOURCES[1:] + [os.path.join(HERE, "gl_runtime.cpp")]:
+            o = os.path.join(work, "gpu_" + os.path.splitext(os.path.basename(src))[0] + ".o")
+            run(["g++", "-std=c++17", *host_flags, *defs, *inc, "-I", "/usr/local/cuda/include", *force,
+                 "-c", src, "-o", o])
+            common.append(o)
+            temps.append(o)
+
+        def variant(bins_log2: int) -> list[tuple]:
+            d = os.path.join(work, f"b{bins_log2}")
+            os.makedirs(d, exist_ok=True)
+            files = {"constants.h": constants_source(bins_log2), "api.cpp": api_text,
+                     "ref_gpu_kernels.cu": '#include "constants.h"\n' + kernels}
+            for name, text in files.items():
+                with open(os.path.join(d, name), "w") as f:
+                    f.write(text)
+                temps.append(os.path.join(d, name))
             # FS/api.cpp takes AreaLightDes (three glm::vec3) by value from the
             # kernel translation unit; GLM declares its own copy constructor
             # under nvcc only, which changes how the struct is passed.  Both
             # sides are compiled by nvcc so that they agree.
+            api_o = os.path.join(d, "gpu_api.o")
             run([NVCC, *ARCH, "-std=c++17", "-O3", "-x", "cu", "-Xcompiler", ",".join(host_flags), "-w",
-                 "--expt-relaxed-constexpr", *defs, *inc, *force, "-c", src, "-o", o])
-        else:
-            run(["g++", "-std=c++17", *host_flags, *defs, *inc, "-I", "/usr/local/cuda/include", *force,
-                 "-c", src, "-o", o])
-        host_objs.append(o)
-    cu = os.path.join(OUT_DIR, "ref_gpu_kernels.cu")
-    with open(cu, "w") as f:
-        f.write(kernel_source())
-    libs = []
-    try:
-        for lib, fmad in ((LIB_EXACT, "false"), (LIB_FMAD, "true")):
-            o = os.path.join(OUT_DIR, f"gpu_kernels_fmad_{fmad}.o")
-            run([NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", f"--fmad={fmad}", "-Xcompiler",
-                 ",".join(host_flags), "-w", "--expt-relaxed-constexpr", *defs, *inc, *force, "-c", cu, "-o", o])
-            run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib + ".tmp", o, *host_objs,
+                 "--expt-relaxed-constexpr", *defs, *inc, *force, "-c", os.path.join(d, "api.cpp"), "-o", api_o])
+            temps.append(api_o)
+            out = []
+            for fmad in (False, True):
+                o = os.path.join(d, f"gpu_kernels_fmad_{str(fmad).lower()}.o")
+                run([NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", f"--fmad={str(fmad).lower()}", "-Xcompiler",
+                     ",".join(host_flags), "-w", "--expt-relaxed-constexpr", *defs, *inc, *force, "-c",
+                     os.path.join(d, "ref_gpu_kernels.cu"), "-o", o])
+                temps.append(o)
+                out.append((bins_log2, fmad, o, api_o))
+            return out
+
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=len(BIN_LOG2S)) as pool:
+            objs = [o for part in pool.map(variant, BIN_LOG2S) for o in part]
+        for bins_log2, fmad, o, api_o in objs:
+            lib = lib_name(bins_log2, fmad)
+            run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib + ".tmp", o, api_o, *common,
                  "-Xlinker", "-Bsymbolic"])
             os.replace(lib + ".tmp", lib)
-            os.remove(o)
             libs.append(lib)
     finally:
-        if os.path.exists(cu):
-            os.remove(cu)
-        for o in host_objs:
-            if os.path.exists(o):
-                os.remove(o)
+        for t in temps:
+            if os.path.exists(t):
+                os.remove(t)
+        for root, dirs, _ in os.walk(work, topdown=False):
+            for dname in dirs:
+                os.rmdir(os.path.join(root, dname))
+        if os.path.isdir(work):
+            os.rmdir(work)
     return libs
 
 

@@ -13,6 +13,51 @@
 #include <algorithm>
 #include <vector>
 
+// Stage wrappers (see harness_pre.cuh): event k is recorded on the default
+// stream before stage k and event 5 after the last one; a stage's time is the
+// span between its two events (device work and host gaps alike, as the
+// reference runs them: its drivers synchronise and read counts back).
+#undef lightPlaneParamCal
+#undef bindSampleToBin
+#undef countTriBinPairNum
+#undef bindTriToBin
+#undef shadowCal_perSample
+constexpr int kRefGpuStages = 5;   // lightPlaneParamCal .. shadowCal_perSample
+static cudaEvent_t refgpu_stage_ev[kRefGpuStages + 1];
+static unsigned refgpu_stage_seen;
+static void refgpu_mark(int k)
+{
+    if (refgpu_stage_ev[k] && cudaEventRecord(refgpu_stage_ev[k], 0) == cudaSuccess) refgpu_stage_seen |= 1u << k;
+}
+bool lightPlaneParamCal()
+{
+    refgpu_mark(0);
+    const bool none = refgpu_inner_lightPlaneParamCal();
+    refgpu_mark(1);
+    return none;
+}
+void bindSampleToBin()
+{
+    refgpu_inner_bindSampleToBin();
+    refgpu_mark(2);
+}
+int countTriBinPairNum()
+{
+    const int n = refgpu_inner_countTriBinPairNum();
+    refgpu_mark(3);
+    return n;
+}
+void bindTriToBin(int pairNum)
+{
+    refgpu_inner_bindTriToBin(pairNum);
+    refgpu_mark(4);
+}
+void shadowCal_perSample()
+{
+    refgpu_inner_shadowCal_perSample();
+    refgpu_mark(5);
+}
+
 void refgpu_gl_bind_buffer(GLuint name, void *dptr, size_t bytes);
 void refgpu_gl_bind_array(GLuint name, cudaArray_t arr);
 cudaArray_t refgpu_gl_array(GLuint name);
@@ -179,6 +224,12 @@ struct RefGpuOut {
     // the per-sample kernel ran, else 0) and its N light-row words, from the
     // last launch (REFGPU_MASK_DUMP)
     uint32_t *masks;
+    // optional host [reps * 5]: ms of each stage driver per timed launch
+    // (lightPlaneParamCal, bindSampleToBin, countTriBinPairNum, bindTriToBin,
+    // shadowCal_perSample); -1 where the stage did not run
+    float *stage_ms;
+    int32_t bins;                    // the build's bins per side (FD_MAX_LP_GRID_SIZE)
+    int32_t pad0;
 };
 
 static int refgpu_round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -269,6 +320,7 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     cudaEvent_t e0, e1;
     checkCudaErrors(cudaEventCreate(&e0));
     checkCudaErrors(cudaEventCreate(&e1));
+    for (auto &ev : refgpu_stage_ev) checkCudaErrors(cudaEventCreate(&ev));
     const int total = std::max(in->warmup, 0) + std::max(in->reps, 1);
     const bool trace = getenv("REFGPU_TRACE") != nullptr;
     for (int it = 0; it < total && refgpu_error_count() == 0; ++it) {
@@ -282,6 +334,7 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
         checkCudaErrors(cudaMemset(flush, it & 0xff, flushBytes));
         checkCudaErrors(cudaDeviceSynchronize());
         checkCudaErrors(cudaEventRecord(e0, 0));
+        refgpu_stage_seen = 0;
         const float own = FD::FDLaunch();
         if (trace) {
             float a[16] = {0};
@@ -307,10 +360,23 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
         if (k >= 0) {
             if (out->launch_ms) out->launch_ms[k] = ms;
             if (out->fdlaunch_ms) out->fdlaunch_ms[k] = own;
+            if (out->stage_ms)
+                for (int j = 0; j < kRefGpuStages; ++j) {
+                    float v = -1.f;
+                    const unsigned both = (1u << j) | (1u << (j + 1));
+                    if ((refgpu_stage_seen & both) == both &&
+                        cudaEventElapsedTime(&v, refgpu_stage_ev[j], refgpu_stage_ev[j + 1]) != cudaSuccess)
+                        v = -1.f;
+                    out->stage_ms[(size_t)k * kRefGpuStages + j] = v;
+                }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (auto &ev : refgpu_stage_ev) {
+        cudaEventDestroy(ev);
+        ev = nullptr;
+    }
     FD::FDunregisterGLres();
     unsigned long long rows = 0;
     checkCudaErrors(cudaMemcpyFromSymbol(&rows, refgpu_rows_beyond_n, sizeof(rows)));
@@ -343,6 +409,7 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     memcpy(out->sample_aabb, sampleRectangleAABB, sizeof(out->sample_aabb));
     memcpy(out->model_aabb, modelRectangleAABB, sizeof(out->model_aabb));
     out->num_bins = FD_MAX_LP_GRID_SIZE * FD_MAX_LP_GRID_SIZE;
+    out->bins = FD_MAX_LP_GRID_SIZE;
     out->valid_samples = m_validSampleNum;
     out->valid_tris = m_validTriangleNum;
     out->num_pairs = m_validBT_PairNum;

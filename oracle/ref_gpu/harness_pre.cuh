@@ -73,3 +73,13 @@ __device__ unsigned int *refgpu_mask_out;
         o_[0] = 1u;                                                                     \
         for (int r_ = 0; r_ < (rows); ++r_) o_[1 + r_] = (m)[r_ * 32];                  \
     }
+
+// Per-stage timing: the five stage drivers FDLaunch calls (FS/api.cpp:495-552,
+// declared in K/FourD.h:146-154 above this point) are defined by the kernel
+// files under these names; harness_post.cuh defines the original names as
+// wrappers that record a CUDA event on the default stream around each call.
+#define lightPlaneParamCal refgpu_inner_lightPlaneParamCal
+#define bindSampleToBin refgpu_inner_bindSampleToBin
+#define countTriBinPairNum refgpu_inner_countTriBinPairNum
+#define bindTriToBin refgpu_inner_bindTriToBin
+#define shadowCal_perSample refgpu_inner_shadowCal_perSample

@@ -40,6 +40,9 @@ def test_reference_arm_line_on_cpu():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert "unavailable" in d["reference_gpu"]
+    # each step is a bounded sample scaled to a full frame, and the line says so
+    assert d["extrapolated"] is True and "extrapolated" in d["steps_are"]
+    assert 0 < d["measured_ms_per_step"]
 
 
 def test_roofline_traffic_comes_from_the_committed_profile():

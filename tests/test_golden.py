@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import oracle
+from oracle.refpath import reference_present
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
@@ -76,7 +77,7 @@ def test_library_light_setup_matches_reference_fixture(fdzb, path):
     assert _same(L["corners"].ravel(), z["ref_corners"]) and _same(L["deltas"].ravel(), z["ref_deltas"])
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference sources not present")
+@pytest.mark.skipif(not reference_present(), reason="reference sources not present")
 def test_reference_harness_reproduces_fixtures():
     from oracle import ref
     if not ref.available():

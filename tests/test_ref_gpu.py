@@ -1,13 +1,16 @@
 """The reference's own GPU code, run on the same B200, against the product.
 
-oracle/_ref/libref4dzb_gpu.so is 4DZB's soft-shadow sources (FS/api.cpp and
+oracle/_ref/libref4dzb_gpu*.so is 4DZB's soft-shadow sources (FS/api.cpp and
 K/*.inl) compiled for sm_100a with --fmad=false by
-oracle/ref_gpu/build_ref_gpu.py; FDLaunch runs its own kernels, Thrust sorts
-and host sequencing.  At the reference's 16 x 16 bins the product's shadows
-must equal the reference's bit for bit, and the light-plane setup and the
-binning counts must agree; the reference's per-sample kernel also hands
+oracle/ref_gpu/build_ref_gpu.py, at the reference's own 16 x 16 bins and with
+its compile-time bin constant set to 32 x 32 and 128 x 128; FDLaunch runs its
+own kernels, Thrust sorts and host sequencing.  At the same bins the product's
+shadows must equal the reference's bit for bit, and the light-plane setup and
+the binning counts must agree; the reference's per-sample kernel also hands
 out its final light rows (a harness dump after its shadow store), which must
-equal the product's masks for every binned sample.  Every scene passes the CPU preflight (keys inside
+equal the product's masks for every binned sample -- in the reference's
+per-bin triangle order and in the coverage order the product runs by default
+(the small frame at its 32 x 32 bins, the HD frame at its 128 x 128).  Every scene passes the CPU preflight (keys inside
 the bin grid, pairs inside the reference's pair buffers) before it reaches
 the GPU.  The --fmad=true build (the reference project's default) is run too:
 its shadows differ from the exact ones only where a fused multiply-add moved a
@@ -25,9 +28,9 @@ pytestmark = pytest.mark.gpu
 needs_lib = pytest.mark.skipif(not ref_gpu.available(), reason="reference GPU harness not built (oracle/_ref)")
 
 
-def _product(fdzb, scene):
-    s16 = dataclasses.replace(scene, bins=ref_gpu.REF_BINS)
-    ctx, t = fdzb.context_for_scene(s16, masks=True, tri_order=fdzb.TRI_ORDER_REFERENCE)
+def _product(fdzb, scene, bins=ref_gpu.REF_BINS, tri_order=0):
+    sb = dataclasses.replace(scene, bins=bins)
+    ctx, t = fdzb.context_for_scene(sb, masks=True, tri_order=tri_order)
     ctx.launch()
     st = ctx.stats()
     sh = t["shadow"].cpu().numpy().copy()
@@ -48,8 +51,8 @@ def _rows_of(words, n):
     return rows
 
 
-def _check(fdzb, scene, ref):
-    sh, mk, st = _product(fdzb, scene)
+def _check(fdzb, scene, ref, bins=ref_gpu.REF_BINS, tri_order=0):
+    sh, mk, st = _product(fdzb, scene, bins, tri_order)
     assert ref["rows_beyond_n"] == 0
     bad = np.flatnonzero(sh.view(np.uint32) != ref["shadow"].view(np.uint32))
     assert bad.size == 0, f"{bad.size} of {scene.S} shadows differ, first {bad[:5].tolist()}"
@@ -108,6 +111,58 @@ def test_large_frame_equals_reference_on_gpu(cuda_ok, fdzb, scenes):
     ref_gpu.preflight(scene, occ_stride=256)
     ref = ref_gpu.run(scene, fmad=False, checked=True, masks=True)
     _check(fdzb, scene, ref)
+
+
+def _needs(bins, fmad=False):
+    if not ref_gpu.available(fmad=fmad, bins=bins):
+        pytest.skip(f"reference GPU harness at {bins} x {bins} bins not built (oracle/_ref)")
+
+
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("cull", [False, True])
+def test_small_frame_at_32_bins_equals_reference(cuda_ok, fdzb, scenes, cull, order):
+    """The small workload at its own 32 x 32 bins, both triangle orders."""
+    _needs(32)
+    scene = scenes.preset("small", cull=cull)
+    assert scene.bins == 32
+    ref = ref_gpu.run(scene, fmad=False, masks=True, bins=32)
+    assert ref["bins"] == 32 and ref["num_bins"] == 32 * 32
+    _check(fdzb, scene, ref, bins=32, tri_order=order)
+
+
+@pytest.mark.parametrize("bins", [32, 128])
+def test_odd_sizes_at_other_bins_equal_reference(cuda_ok, fdzb, scenes, bins):
+    _needs(bins)
+    for W, H, T, n, seed in ((301, 77, 700, 5, 11), (200, 150, 1500, 32, 12), (640, 360, 20000, 16, 13)):
+        scene = scenes.make_scene(W, H, T, n=n, bins=bins, seed=seed, cull=False, sigma=0.1)
+        ref = ref_gpu.run(scene, fmad=False, masks=True, bins=bins)
+        _check(fdzb, scene, ref, bins=bins, tri_order=1)
+
+
+def test_hd_frame_at_128_bins_equals_reference_every_mask(cuda_ok, fdzb, scenes):
+    """The headline configuration -- 1920 x 1080 samples, 200k triangles, a
+    16 x 16 light, 128 x 128 bins, coverage order -- against the reference's
+    own kernels built at 128 x 128 bins: every shadow and every binned
+    sample's 16 light rows bit for bit, and the same light plane, valid counts
+    and triangle/bin pair count."""
+    _needs(128)
+    scene = scenes.preset("hd")
+    assert scene.bins == 128
+    ref = ref_gpu.run(scene, fmad=False, masks=True, bins=128)
+    assert ref["bins"] == 128
+    sh = _check(fdzb, scene, ref, bins=128, tri_order=1)
+    assert 0.0 < float(sh.mean()) <= 1.0
+
+
+def test_reference_stage_times_cover_the_frame(cuda_ok, scenes):
+    """The harness's per-stage events (around the five stage drivers FDLaunch
+    calls) are recorded for every timed frame and add up to at most the frame."""
+    _needs(32, fmad=True)
+    scene = scenes.preset("small")
+    r = ref_gpu.run(scene, fmad=True, bins=32, warmup=1, reps=3)
+    st = r["stage_ms"]
+    assert st.shape == (3, 5) and (st >= 0).all()
+    assert (st.sum(axis=1) <= r["launch_ms"] * 1.001 + 1e-3).all()
 
 
 @needs_lib
