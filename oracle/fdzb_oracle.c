@@ -891,34 +891,228 @@ int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
  * occluded iff all three oriented edge functions are >= 0 -- with depth_plane,
  * and the triangle's max depth not below the sample's, also the oriented
  * triangle plane -- evaluated in double. */
+/* ---- O3: FP64 per-light-sample test ------------------------------------
+ *
+ * Light frame, in double: origin upRight, axes x_delt and y_delt (one light
+ * sample per unit: light sample (i, j) sits at a = i, b = j, d = 0) and the unit
+ * normal nv of the light plane, oriented along viewDir (towards the
+ * receivers).  (a, b, d) of a point P solve P - upRight = a x_delt + b y_delt +
+ * d nv.  Light-plane units are world units measured in the light's plane:
+ * a grid step along x_delt is |x_delt| of them. */
+typedef struct {
+    double o[3], inv[3][3];
+    double sx, sy;
+} o3_frame;
+
+static void o3_frame_init(o3_frame *F, const orc_light *L)
+{
+    double X[3], Y[3], N[3];
+    for (int k = 0; k < 3; ++k) {
+        F->o[k] = L->upRight[k];
+        X[k] = L->x_delt[k];
+        Y[k] = L->y_delt[k];
+    }
+    N[0] = X[1] * Y[2] - X[2] * Y[1];
+    N[1] = X[2] * Y[0] - X[0] * Y[2];
+    N[2] = X[0] * Y[1] - X[1] * Y[0];
+    double nn = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+    double sg = (N[0] * L->viewDir[0] + N[1] * L->viewDir[1] + N[2] * L->viewDir[2]) < 0 ? -1.0 : 1.0;
+    for (int k = 0; k < 3; ++k) N[k] *= sg / nn;
+    /* inverse of the column matrix [X Y N] by cofactors */
+    double m[3][3] = {{X[0], Y[0], N[0]}, {X[1], Y[1], N[1]}, {X[2], Y[2], N[2]}};
+    double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                 m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                 m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            int r1 = (c + 1) % 3, r2 = (c + 2) % 3, c1 = (r + 1) % 3, c2 = (r + 2) % 3;
+            F->inv[r][c] = (m[r1][c1] * m[r2][c2] - m[r1][c2] * m[r2][c1]) / det;
+        }
+    F->sx = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+    F->sy = sqrt(Y[0] * Y[0] + Y[1] * Y[1] + Y[2] * Y[2]);
+}
+
+static inline void o3_coords(const o3_frame *F, const double P[3], double out[3])
+{
+    double q[3] = {P[0] - F->o[0], P[1] - F->o[1], P[2] - F->o[2]};
+    for (int r = 0; r < 3; ++r) out[r] = F->inv[r][0] * q[0] + F->inv[r][1] * q[1] + F->inv[r][2] * q[2];
+}
+
+/* Triangles are visited in blocks of O3_BLOCK, spatially sorted, each block
+ * with the union of its members' frame bounds, so that one test skips a block
+ * that no segment from the sample to the light grid can reach. */
+#define O3_BLOCK 64
+/* Boundary distances are exact up to this many light-plane units; a light
+ * sample farther from every triangle's projected boundary keeps 1e300. */
+#define O3_MARGIN 1e-3
+
+typedef struct {
+    double lo[3], hi[3];   /* frame bounds (a, b, d) */
+} o3_box;
+
+/* Can a segment from a light sample of the [0, NR-1] x [0, NC-1] grid to the
+ * point q = (aQ, bQ, dQ) meet a point of box B?  A point at depth d of such a
+ * segment is (1 - s) (i, j, 0) + s q with s = d / dQ, so over the box's depth
+ * range its (a, b) lie in the hull of the grid's images at the two end values
+ * of s (the images are intervals whose ends move linearly in s).  The test
+ * widens them by mg grid units.  Conservative: false only when no segment can
+ * meet the box.  The cone test extends the segments beyond the light plane
+ * (d < 0, s < 0), which this covers too. */
+static inline int o3_reach(const o3_box *B, const double q[3], int NR, int NC, double mg)
+{
+    if (B->lo[2] >= q[2]) return 0;    /* at or behind the sample's depth */
+    double s0 = B->lo[2] / q[2], s1 = B->hi[2] / q[2];
+    if (s1 > 1.0) s1 = 1.0;
+    for (int ax = 0; ax < 2; ++ax) {
+        double ext = ax == 0 ? (double)(NR - 1) : (double)(NC - 1);
+        double l0 = s0 * q[ax], l1 = s1 * q[ax];
+        double h0 = (1.0 - s0) * ext + l0, h1 = (1.0 - s1) * ext + l1;
+        double lo = (l0 < l1 ? l0 : l1) - mg, hi = (h0 > h1 ? h0 : h1) + mg;
+        if (B->hi[ax] < lo || B->lo[ax] > hi) return 0;
+    }
+    return 1;
+}
+
+static uint32_t o3_morton(uint32_t x, uint32_t y, uint32_t z)
+{
+    uint32_t r = 0;
+    for (int k = 0; k < 10; ++k)
+        r |= ((x >> k) & 1u) << (3 * k) | ((y >> k) & 1u) << (3 * k + 1) | ((z >> k) & 1u) << (3 * k + 2);
+    return r;
+}
+
+typedef struct {
+    double key;
+    int blk;
+} o3_visit;
+
+static int o3_cmp_visit(const void *a, const void *b)
+{
+    const o3_visit *x = (const o3_visit *)a, *y = (const o3_visit *)b;
+    return x->key > y->key ? -1 : x->key < y->key ? 1 : x->blk - y->blk;
+}
+
+static const uint32_t *o3_sort_keys;
+static int o3_cmp(const void *a, const void *b)
+{
+    uint32_t x = o3_sort_keys[*(const int *)a], y = o3_sort_keys[*(const int *)b];
+    return x < y ? -1 : x > y ? 1 : (*(const int *)a - *(const int *)b);
+}
+
+static inline double o3_seg_dist(double px, double py, const double a[2], const double b[2])
+{
+    double dx = b[0] - a[0], dy = b[1] - a[1];
+    double L2 = dx * dx + dy * dy;
+    double t = L2 > 0 ? ((px - a[0]) * dx + (py - a[1]) * dy) / L2 : 0.0;
+    if (t < 0) t = 0;
+    if (t > 1) t = 1;
+    double ex = a[0] + t * dx - px, ey = a[1] + t * dy - py;
+    return sqrt(ex * ex + ey * ey);
+}
+
 void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                          const int32_t *sample_ids, int32_t n, uint32_t *masks,
-                         double *edge_dist)
+                         double *edge_dist, orc_o3_stats *stats)
 {
     const orc_light *L = in->light;
     const int NR = L->resW, NC = L->resH, words = orc_mask_words_rc(NR, NC), NN = NR * NC;
     memset(masks, 0, sizeof(uint32_t) * (size_t)n * words);
-    for (size_t i = 0; i < (size_t)n * NN; ++i) edge_dist[i] = 1e300;
+    if (edge_dist)
+        for (size_t i = 0; i < (size_t)n * NN; ++i) edge_dist[i] = 1e300;
+    if (stats) memset(stats, 0, sizeof(*stats));
     if (fr->state < 2) return;
     tri_rec *recs = NULL;
     int nt = build_tri_list(in, fr, &recs);
     if (nt < 0) return;
+    /* without distances a sample stops once every light sample is occluded:
+     * the mask is an OR over triangles and can gain nothing more */
+    const int need_dist = edge_dist != NULL;
+    o3_frame F;
+    o3_frame_init(&F, L);
+    const double mg = O3_MARGIN / (F.sx < F.sy ? F.sx : F.sy);
+    /* frame coordinates of every vertex; spatial order; block bounds */
+    double *fv = (double *)malloc(sizeof(double) * 9 * (size_t)(nt > 0 ? nt : 1));
+    o3_box *tb = (o3_box *)malloc(sizeof(o3_box) * (size_t)(nt > 0 ? nt : 1));
+    uint32_t *key = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(nt > 0 ? nt : 1));
+    int *order = (int *)malloc(sizeof(int) * (size_t)(nt > 0 ? nt : 1));
+    const int nblk = (nt + O3_BLOCK - 1) / O3_BLOCK;
+    o3_box *bb = (o3_box *)malloc(sizeof(o3_box) * (size_t)(nblk > 0 ? nblk : 1));
+    if (!fv || !tb || !key || !order || !bb) {
+        free(fv); free(tb); free(key); free(order); free(bb); free(recs);
+        return;
+    }
+    double glo[3] = {1e300, 1e300, 1e300}, ghi[3] = {-1e300, -1e300, -1e300};
+    for (int t = 0; t < nt; ++t) {
+        const float *vs[3] = {recs[t].v0, recs[t].v1, recs[t].v2};
+        o3_box *B = &tb[t];
+        for (int k = 0; k < 3; ++k) {
+            B->lo[k] = 1e300;
+            B->hi[k] = -1e300;
+        }
+        for (int v = 0; v < 3; ++v) {
+            double P[3] = {vs[v][0], vs[v][1], vs[v][2]};
+            double *c = fv + 9 * (size_t)t + 3 * v;
+            o3_coords(&F, P, c);
+            for (int k = 0; k < 3; ++k) {
+                if (c[k] < B->lo[k]) B->lo[k] = c[k];
+                if (c[k] > B->hi[k]) B->hi[k] = c[k];
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            double mid = 0.5 * (B->lo[k] + B->hi[k]);
+            if (mid < glo[k]) glo[k] = mid;
+            if (mid > ghi[k]) ghi[k] = mid;
+        }
+    }
+    for (int t = 0; t < nt; ++t) {
+        uint32_t q[3];
+        for (int k = 0; k < 3; ++k) {
+            double mid = 0.5 * (tb[t].lo[k] + tb[t].hi[k]);
+            double u = ghi[k] > glo[k] ? (mid - glo[k]) / (ghi[k] - glo[k]) : 0.0;
+            q[k] = (uint32_t)(u * 1023.0 + 0.5);
+        }
+        key[t] = o3_morton(q[0], q[1], q[2]);
+        order[t] = t;
+    }
+    o3_sort_keys = key;
+    qsort(order, (size_t)nt, sizeof(int), o3_cmp);
+    for (int b = 0; b < nblk; ++b) {
+        o3_box *B = &bb[b];
+        for (int k = 0; k < 3; ++k) {
+            B->lo[k] = 1e300;
+            B->hi[k] = -1e300;
+        }
+        for (int m = b * O3_BLOCK; m < nt && m < (b + 1) * O3_BLOCK; ++m)
+            for (int k = 0; k < 3; ++k) {
+                if (tb[order[m]].lo[k] < B->lo[k]) B->lo[k] = tb[order[m]].lo[k];
+                if (tb[order[m]].hi[k] > B->hi[k]) B->hi[k] = tb[order[m]].hi[k];
+            }
+    }
+
     const float *M = L->mat;
     const float Bx = fr->lp_begin[0], By = fr->lp_begin[1], Ex = fr->lp_end[0], Ey = fr->lp_end[1];
     v3 ur = ld3(L->upRight), ul = ld3(L->upLeft), dl = ld3(L->downLeft), dr = ld3(L->downRight);
     const double L0[3] = {L->upRight[0], L->upRight[1], L->upRight[2]};
     const double XD[3] = {L->x_delt[0], L->x_delt[1], L->x_delt[2]};
     const double YD[3] = {L->y_delt[0], L->y_delt[1], L->y_delt[2]};
-    const double desp = in->esp;
+    const double desp = in->esp, sx = F.sx, sy = F.sy;
+    int64_t cand = 0, evald = 0, fallback = 0, skipped_blocks = 0;
 #ifdef _OPENMP
     if (in->nthreads > 0) omp_set_num_threads(in->nthreads);
 #endif
-#pragma omp parallel for schedule(dynamic, 4)
+#pragma omp parallel reduction(+ : cand, evald, fallback, skipped_blocks)
+    {
+    /* reachable blocks of a sample, deepest (nearest the receivers, the
+     * largest seen from the sample) first, so that a sample in umbra fills
+     * its mask early when distances are not asked for */
+    o3_visit *visit = (o3_visit *)malloc(sizeof(o3_visit) * (size_t)(nblk > 0 ? nblk : 1));
+#pragma omp for schedule(dynamic, 4)
     for (int k = 0; k < n; ++k) {
         size_t s = (size_t)sample_ids[k];
         const float *pp = in->pos + 4 * s, *nn = in->nrm + 4 * s;
         uint32_t *mk = masks + (size_t)k * words;
-        double *ed = edge_dist + (size_t)k * NN;
+        double *ed = need_dist ? edge_dist + (size_t)k * NN : NULL;
+        int nset = 0;
         if (isnan(pp[0])) continue;
         v3 p = ld3(pp), nv = ld3(nn);
         if (dot3(sub3(ur, p), nv) <= 0 && dot3(sub3(ul, p), nv) <= 0 &&
@@ -931,76 +1125,166 @@ void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
             r.y + L->RF[1] / r.z - fr->sub[1] > Ey)
             continue;
         const double Q[3] = {p.x, p.y, p.z};
-        for (int t = 0; t < nt; ++t) {
-            const tri_rec *tr = &recs[t];
-            double V[3][3];
-            for (int a = 0; a < 3; ++a) {
-                V[0][a] = tr->v0[a];
-                V[1][a] = tr->v1[a];
-                V[2][a] = tr->v2[a];
+        double q[3];
+        o3_coords(&F, Q, q);
+        const int prefilter = q[2] > 0;   /* the sample in front of the light plane */
+        int nvisit = 0;
+        for (int blk = 0; blk < nblk; ++blk) {
+            if (prefilter && !o3_reach(&bb[blk], q, NR, NC, mg)) {
+                ++skipped_blocks;
+                continue;
             }
-            double e1[3], e2[3], nrm[3], qv[3];
-            for (int a = 0; a < 3; ++a) {
-                e1[a] = V[1][a] - V[0][a];
-                e2[a] = V[2][a] - V[1][a];
-                qv[a] = Q[a] - V[0][a];
-            }
-            nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
-            nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
-            nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
-            double dir = qv[0] * nrm[0] + qv[1] * nrm[1] + qv[2] * nrm[2];
-            if (fabs(dir) < desp) {
-                /* point-in-triangle in double, K/Step5_2_shadowCal.inl:213-222 */
-                double Nv[3][3];
-                for (int e = 0; e < 3; ++e) {
-                    const double *A = V[e], *B = V[(e + 1) % 3];
-                    double ba[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
-                    double pb[3] = {Q[0] - B[0], Q[1] - B[1], Q[2] - B[2]};
-                    Nv[e][0] = ba[1] * pb[2] - ba[2] * pb[1];
-                    Nv[e][1] = ba[2] * pb[0] - ba[0] * pb[2];
-                    Nv[e][2] = ba[0] * pb[1] - ba[1] * pb[0];
+            visit[nvisit].key = bb[blk].hi[2];
+            visit[nvisit].blk = blk;
+            ++nvisit;
+        }
+        qsort(visit, (size_t)nvisit, sizeof(o3_visit), o3_cmp_visit);
+        for (int vi = 0; vi < nvisit && (need_dist || nset < NN); ++vi) {
+            const int blk = visit[vi].blk;
+            for (int m = blk * O3_BLOCK; m < nt && m < (blk + 1) * O3_BLOCK && (need_dist || nset < NN); ++m) {
+                const int t = order[m];
+                if (prefilter && !o3_reach(&tb[t], q, NR, NC, mg)) continue;
+                ++cand;
+                const tri_rec *tr = &recs[t];
+                double V[3][3];
+                for (int a = 0; a < 3; ++a) {
+                    V[0][a] = tr->v0[a];
+                    V[1][a] = tr->v1[a];
+                    V[2][a] = tr->v2[a];
                 }
-                double d12 = Nv[0][0] * Nv[1][0] + Nv[0][1] * Nv[1][1] + Nv[0][2] * Nv[1][2];
-                double d23 = Nv[1][0] * Nv[2][0] + Nv[1][1] * Nv[2][1] + Nv[1][2] * Nv[2][2];
-                if (!(d12 < 0.0) && !(d23 < 0.0)) continue;
-            }
-            double sg = dir < 0 ? -1.0 : 1.0;
-            double A[4], B[4], C[4], inv[4];
-            const int planes = (in->depth_plane && (tr->minz <= 0.0f || tr->maxz >= r.z)) ? 4 : 3;
-            for (int e = 0; e < 3; ++e) {
-                const double *a = V[e], *b = V[(e + 1) % 3];
-                double u[3] = {b[0] - Q[0], b[1] - Q[1], b[2] - Q[2]};
-                double w[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
-                double nk[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
-                double lq[3] = {L0[0] - Q[0], L0[1] - Q[1], L0[2] - Q[2]};
-                A[e] = sg * (nk[0] * XD[0] + nk[1] * XD[1] + nk[2] * XD[2]);
-                B[e] = sg * (nk[0] * YD[0] + nk[1] * YD[1] + nk[2] * YD[2]);
-                C[e] = sg * (nk[0] * lq[0] + nk[1] * lq[1] + nk[2] * lq[2]);
-                double g = sqrt(A[e] * A[e] + B[e] * B[e]);
-                inv[e] = g > 0 ? 1.0 / g : 1e300;
-            }
-            if (planes == 4) {
-                /* -n . (L - v0), oriented like the edges */
-                double lv[3] = {L0[0] - V[0][0], L0[1] - V[0][1], L0[2] - V[0][2]};
-                A[3] = -sg * (nrm[0] * XD[0] + nrm[1] * XD[1] + nrm[2] * XD[2]);
-                B[3] = -sg * (nrm[0] * YD[0] + nrm[1] * YD[1] + nrm[2] * YD[2]);
-                C[3] = -sg * (nrm[0] * lv[0] + nrm[1] * lv[1] + nrm[2] * lv[2]);
-                double g = sqrt(A[3] * A[3] + B[3] * B[3]);
-                inv[3] = g > 0 ? 1.0 / g : 1e300;
-            }
-            for (int i = 0; i < NR; ++i)
-                for (int j = 0; j < NC; ++j) {
-                    double mn = 1e300;
-                    for (int e = 0; e < planes; ++e) {
-                        double v = (A[e] * i + B[e] * j + C[e]) * inv[e];
-                        if (v < mn) mn = v;
+                double e1[3], e2[3], nrm[3], qv[3];
+                for (int a = 0; a < 3; ++a) {
+                    e1[a] = V[1][a] - V[0][a];
+                    e2[a] = V[2][a] - V[1][a];
+                    qv[a] = Q[a] - V[0][a];
+                }
+                nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+                nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+                nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+                double dir = qv[0] * nrm[0] + qv[1] * nrm[1] + qv[2] * nrm[2];
+                if (fabs(dir) < desp) {
+                    /* point-in-triangle in double, K/Step5_2_shadowCal.inl:213-222 */
+                    double Nv[3][3];
+                    for (int e = 0; e < 3; ++e) {
+                        const double *A = V[e], *B = V[(e + 1) % 3];
+                        double ba[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+                        double pb[3] = {Q[0] - B[0], Q[1] - B[1], Q[2] - B[2]};
+                        Nv[e][0] = ba[1] * pb[2] - ba[2] * pb[1];
+                        Nv[e][1] = ba[2] * pb[0] - ba[0] * pb[2];
+                        Nv[e][2] = ba[0] * pb[1] - ba[1] * pb[0];
                     }
-                    int b = i * NC + j;
-                    if (mn >= 0.0) mk[b >> 5] |= 1u << (b & 31);
-                    double mg = fabs(mn);
-                    if (mg < ed[b]) ed[b] = mg;
+                    double d12 = Nv[0][0] * Nv[1][0] + Nv[0][1] * Nv[1][1] + Nv[0][2] * Nv[1][2];
+                    double d23 = Nv[1][0] * Nv[2][0] + Nv[1][1] * Nv[2][1] + Nv[1][2] * Nv[2][2];
+                    if (!(d12 < 0.0) && !(d23 < 0.0)) continue;
                 }
+                double sg = dir < 0 ? -1.0 : 1.0;
+                double A[4], B[4], C[4], inv[4], pn[4];
+                const int planes = (in->depth_plane && (tr->minz <= 0.0f || tr->maxz >= r.z)) ? 4 : 3;
+                for (int e = 0; e < 3; ++e) {
+                    const double *a = V[e], *b = V[(e + 1) % 3];
+                    double u[3] = {b[0] - Q[0], b[1] - Q[1], b[2] - Q[2]};
+                    double w[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+                    double nk[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+                    double lq[3] = {L0[0] - Q[0], L0[1] - Q[1], L0[2] - Q[2]};
+                    A[e] = sg * (nk[0] * XD[0] + nk[1] * XD[1] + nk[2] * XD[2]);
+                    B[e] = sg * (nk[0] * YD[0] + nk[1] * YD[1] + nk[2] * YD[2]);
+                    C[e] = sg * (nk[0] * lq[0] + nk[1] * lq[1] + nk[2] * lq[2]);
+                }
+                if (planes == 4) {
+                    /* -n . (L - v0), oriented like the edges */
+                    double lv[3] = {L0[0] - V[0][0], L0[1] - V[0][1], L0[2] - V[0][2]};
+                    A[3] = -sg * (nrm[0] * XD[0] + nrm[1] * XD[1] + nrm[2] * XD[2]);
+                    B[3] = -sg * (nrm[0] * YD[0] + nrm[1] * YD[1] + nrm[2] * YD[2]);
+                    C[3] = -sg * (nrm[0] * lv[0] + nrm[1] * lv[1] + nrm[2] * lv[2]);
+                }
+                for (int e = 0; e < planes; ++e) {
+                    double g = sqrt(A[e] * A[e] + B[e] * B[e]);
+                    inv[e] = g > 0 ? 1.0 / g : 1e300;
+                    /* light-plane units per unit of A i + B j + C */
+                    double h = sqrt((A[e] / sx) * (A[e] / sx) + (B[e] / sy) * (B[e] / sy));
+                    pn[e] = h > 0 ? 1.0 / h : 1e300;
+                }
+                /* the triangle seen from Q on the light plane: each vertex
+                 * closer to the light than Q projects at q + t (v - q),
+                 * t = dQ / (dQ - dv) > 0 */
+                int proj = planes == 3 && prefilter;
+                double pv[3][2];
+                for (int v = 0; v < 3 && proj; ++v) {
+                    const double *c = fv + 9 * (size_t)t + 3 * v;
+                    if (!(c[2] < q[2])) {
+                        proj = 0;
+                        break;
+                    }
+                    double tt = q[2] / (q[2] - c[2]);
+                    pv[v][0] = q[0] + tt * (c[0] - q[0]);
+                    pv[v][1] = q[1] + tt * (c[1] - q[1]);
+                }
+                int i0 = 0, i1 = NR - 1, j0 = 0, j1 = NC - 1;
+                if (proj) {
+                    double amin = pv[0][0], amax = pv[0][0], bmin = pv[0][1], bmax = pv[0][1];
+                    for (int v = 1; v < 3; ++v) {
+                        if (pv[v][0] < amin) amin = pv[v][0];
+                        if (pv[v][0] > amax) amax = pv[v][0];
+                        if (pv[v][1] < bmin) bmin = pv[v][1];
+                        if (pv[v][1] > bmax) bmax = pv[v][1];
+                    }
+                    double fa0 = floor(amin - mg), fa1 = ceil(amax + mg), fb0 = floor(bmin - mg), fb1 = ceil(bmax + mg);
+                    if (fa0 > i0) i0 = fa0 > (double)NR ? NR : (int)fa0;
+                    if (fa1 < i1) i1 = fa1 < -1.0 ? -1 : (int)fa1;
+                    if (fb0 > j0) j0 = fb0 > (double)NC ? NC : (int)fb0;
+                    if (fb1 < j1) j1 = fb1 < -1.0 ? -1 : (int)fb1;
+                    /* vertices in light-plane units for the boundary distance */
+                    for (int v = 0; v < 3; ++v) {
+                        pv[v][0] *= sx;
+                        pv[v][1] *= sy;
+                    }
+                } else {
+                    ++fallback;
+                }
+                if (i0 > i1 || j0 > j1) continue;
+                ++evald;
+                for (int i = i0; i <= i1; ++i)
+                    for (int j = j0; j <= j1; ++j) {
+                        double mn = 1e300, dmin = 1e300;
+                        for (int e = 0; e < planes; ++e) {
+                            double val = A[e] * i + B[e] * j + C[e];
+                            double v = val * inv[e];
+                            if (v < mn) mn = v;
+                            double dl = fabs(val) * pn[e];
+                            if (dl < dmin) dmin = dl;
+                        }
+                        int b = i * NC + j;
+                        double dist;
+                        if (mn >= 0.0) {
+                            if (!(mk[b >> 5] & (1u << (b & 31)))) ++nset;
+                            mk[b >> 5] |= 1u << (b & 31);
+                            dist = dmin;             /* inside: distance to the nearest edge */
+                        } else if (!need_dist) {
+                            continue;
+                        } else if (proj) {
+                            double px = i * sx, py = j * sy;
+                            dist = o3_seg_dist(px, py, pv[0], pv[1]);
+                            double d2 = o3_seg_dist(px, py, pv[1], pv[2]);
+                            double d3 = o3_seg_dist(px, py, pv[2], pv[0]);
+                            if (d2 < dist) dist = d2;
+                            if (d3 < dist) dist = d3;
+                        } else {
+                            dist = 1e300;            /* outside an unbounded section: not attributed */
+                        }
+                        if (ed && dist < ed[b]) ed[b] = dist;
+                    }
+            }
         }
     }
+    free(visit);
+    }
+    if (stats) {
+        stats->candidates = cand;
+        stats->evaluated = evald;
+        stats->fallback = fallback;
+        stats->skipped_blocks = skipped_blocks;
+        stats->triangles = nt;
+    }
+    free(fv); free(tb); free(key); free(order); free(bb);
     free(recs);
 }

@@ -122,13 +122,25 @@ int32_t orc_frame(const orc_frame_in *in, orc_frame_out *out);
 int64_t orc_exhaustive_fp32(const orc_frame_in *in, const orc_frame_out *fr,
                             const int32_t *sample_ids, int32_t n, uint32_t *masks);
 
-/* Exhaustive FP64 per-light-sample edge test (O3).  For each listed sample:
- * masks[n * words] and min_dist[n * N * N] = min over edges of the FP64
- * distance (light-grid units) from each light sample to the nearest projected
- * edge of any triangle that decides it (n * rows * cols values). */
+/* Exhaustive FP64 per-light-sample edge test (O3).  For each listed sample,
+ * every triangle of the frame (no binning, no AABB pre-cull) decides every
+ * light sample in double: occluded iff all oriented edge planes (and the
+ * triangle's own plane in depth-plane mode) hold, the reference's test in
+ * exact arithmetic.  masks[n * words]; edge_dist[n * rows * cols] = for each
+ * light sample, the distance in light-plane units (world units in the light's
+ * plane) from the light sample to the boundary of the nearest triangle's
+ * region seen from the sample -- inside a region the distance to its nearest
+ * edge, outside the distance to the projected triangle -- exact up to
+ * 1e-3 units, 1e300 where no boundary is that close (edge_dist NULL: masks
+ * only, and a sample stops once all its light samples are occluded).  A conservative
+ * prefilter in the light's frame skips triangles that no segment from the
+ * sample to the light grid can reach; stats (nullable) counts the work. */
+typedef struct {
+    int64_t triangles, candidates, evaluated, fallback, skipped_blocks;
+} orc_o3_stats;
 void orc_exhaustive_fp64(const orc_frame_in *in, const orc_frame_out *fr,
                          const int32_t *sample_ids, int32_t n, uint32_t *masks,
-                         double *edge_dist);
+                         double *edge_dist, orc_o3_stats *stats);
 
 /* G-buffer rasteriser oracle (fdzb_raster_oracle.c): one draw. */
 typedef struct {

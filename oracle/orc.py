@@ -88,7 +88,7 @@ def load() -> ctypes.CDLL:
                                         ctypes.c_int32, u32p]
     lib.orc_exhaustive_fp32.restype = ctypes.c_int64
     lib.orc_exhaustive_fp64.argtypes = [ctypes.POINTER(FrameIn), ctypes.POINTER(FrameOut), i32p,
-                                        ctypes.c_int32, u32p, ctypes.POINTER(ctypes.c_double)]
+                                        ctypes.c_int32, u32p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
     lib.orc_exhaustive_fp64.restype = None
     _lib = lib
     return lib
@@ -244,19 +244,37 @@ def exhaustive_fp32(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int =
     return out.reshape(ids.size, words), int(n)
 
 
-def exhaustive_fp64(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int = 0):
-    """O3: FP64 per-light-sample test.  Returns (masks [n, words], edge distance
-    [n, rows * cols])."""
+class O3Stats(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_int64), ("candidates", ctypes.c_int64), ("evaluated", ctypes.c_int64),
+                ("fallback", ctypes.c_int64), ("skipped_blocks", ctypes.c_int64)]
+
+
+def exhaustive_fp64(scene, fr: OrcFrame, sample_ids: np.ndarray, nthreads: int = 0, stats: bool = False,
+                    distances: bool = True):
+    """O3: FP64 per-light-sample test.  Returns (masks [n, words], boundary
+    distance [n, rows * cols] in light-plane units, or None without distances)
+    and, with stats, a dict of the work counts."""
     lib = load()
     ids = np.ascontiguousarray(sample_ids, dtype=np.int32)
     NN = scene.light.rows * scene.light.cols
     words = mask_words(scene.light.n, scene.light.cols)
-    out = np.zeros(ids.size * words, np.uint32)
-    dist = np.zeros(ids.size * NN, np.float64)
+    out = np.zeros(max(ids.size * words, 1), np.uint32)
+    dist = np.zeros(max(ids.size * NN, 1), np.float64) if distances else None
+    st = O3Stats()
     fr._in.nthreads = nthreads
     lib.orc_exhaustive_fp64(ctypes.byref(fr._in), ctypes.byref(fr._out), _p(ids, i32p), ids.size,
-                            _p(out, u32p), dist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
-    return out.reshape(ids.size, words), dist.reshape(ids.size, NN)
+                            _p(out, u32p), dist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if distances
+                            else None, ctypes.byref(st))
+    res = (out[:ids.size * words].reshape(ids.size, words),
+           dist[:ids.size * NN].reshape(ids.size, NN) if distances else None)
+    if stats:
+        return res + ({n: int(getattr(st, n)) for n, _ in O3Stats._fields_},)
+    return res
+
+
+def light_plane_units(light) -> float:
+    """World units per light-grid step along x_delt (= 2 * right radius / rows)."""
+    return 2.0 * light.right_radius / light.rows
 
 
 # ---- G-buffer rasteriser oracle (fdzb_raster_oracle.c) ----------------------
