@@ -65,7 +65,12 @@ EXPORTED = [
     "fdzb_serve_submit", "fdzb_serve_poll", "fdzb_serve_wait", "fdzb_serve_drain", "fdzb_serve_autotune",
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
     "fdzb_ctx_set_launch_epoch", "fdzb_ctx_get_launch_epoch",
+    "fdzb_ctx_set_occlusion_shape", "fdzb_batch_frame_shape", "fdzb_batch_set_occlusion_shape",
 ]
+
+# Occlusion shapes (staged triangles per chunk, samples per warp item).
+OCC_CHUNKS = (8, 16, 32)
+OCC_ITEMS = (32, 64, 128)
 
 # Launch number at which the look-back status words are cleared (include/fdzb.h).
 LOOKBACK_EPOCH_LIMIT = 0x0FFFFFFF
@@ -263,6 +268,9 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_set_launch_epoch": ([vp, ctypes.c_uint32], i32),
         "fdzb_ctx_get_launch_epoch": ([vp, vp], i32),
         "fdzb_ctx_set_occlusion_schedule": ([vp, i32], i32),
+        "fdzb_ctx_set_occlusion_shape": ([vp, i32, i32], i32),
+        "fdzb_batch_frame_shape": ([vp, i32, vp, vp, vp], i32),
+        "fdzb_batch_set_occlusion_shape": ([vp, i32, i32], i32),
         "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32),
         "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
         "fdzb_ctx_set_shadow_method": ([vp, i32], i32),
@@ -395,6 +403,11 @@ class Context:
         out = ctypes.c_uint32(0)
         _check(self._lib.fdzb_ctx_get_launch_epoch(self._h, ctypes.byref(out)))
         return int(out.value)
+
+    def set_occlusion_shape(self, chunk: int, item: int) -> None:
+        """Triangles staged per chunk (OCC_CHUNKS) and samples per warp item
+        (OCC_ITEMS); results are identical for every shape."""
+        _check(self._lib.fdzb_ctx_set_occlusion_shape(self._h, int(chunk), int(item)))
 
     def set_occlusion_schedule(self, schedule: int) -> None:
         """OCC_LANE_PER_SAMPLE (default) or OCC_LANE_PER_PAIR; results are identical."""
@@ -695,6 +708,17 @@ class Batch:
         st = BatchStats()
         _check(self._lib.fdzb_batch_get_stats(self._h, ctypes.byref(st)))
         return st.as_dict()
+
+    def frame_shape(self, i: int) -> tuple:
+        """(bins per side, staging chunk, samples per item) of frame i of the last launch."""
+        b, c, it = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(self._lib.fdzb_batch_frame_shape(self._h, int(i), ctypes.byref(b), ctypes.byref(c),
+                                                ctypes.byref(it)))
+        return b.value, c.value, it.value
+
+    def set_occlusion_shape(self, chunk: int = 0, item: int = 0) -> None:
+        """One occlusion shape for every frame of later launches (0, 0: tuned or default)."""
+        _check(self._lib.fdzb_batch_set_occlusion_shape(self._h, int(chunk), int(item)))
 
     def frame_bins(self, i: int) -> int:
         rc = self._lib.fdzb_batch_frame_bins(self._h, i)

@@ -265,6 +265,8 @@ int check_frame(const FrameSpec &f, int i)
         return fail(FDZB_ERR_INVALID_ARG, at + "bin number must be a power of two in [1, 512]");
     if (f.light.N < 1 || f.light.N > fdzb::kMaxLightN || f.light.NC < 1 || f.light.NC > fdzb::kMaxLightN)
         return fail(FDZB_ERR_UNSUPPORTED, at + "light grid width and height must be in [1, 64]");
+    if (!valid_occ_shape(f.occChunk, f.occItem))
+        return fail(FDZB_ERR_INVALID_ARG, at + "occlusion shape: chunk in {8, 16, 32}, item in {32, 64, 128}");
     return FDZB_OK;
 }
 
@@ -387,6 +389,9 @@ int engine_enqueue(Engine &e)
         f.light = s.light;
         f.hasXform = s.hasXform ? 1 : 0;
         if (s.hasXform) std::memcpy(f.xform, s.xform, sizeof(f.xform));
+        f.occChunk = s.occChunk;
+        // the lane-per-pair schedule deals one item of 32 samples to a warp
+        f.occItem = b.occVariant == 1 ? 32 : s.occItem;
         e.hBases[i] = sb;
         e.hBases[nf + i] = tb;
         e.hBases[2 * nf + i] = bb;
@@ -735,6 +740,7 @@ struct fdzb_ctx {
     fdzb_frame_stats stats{};
     bool hasXform = false;
     float xform[16] = {};
+    int occChunk = 32, occItem = 32;   // occlusion shape (fdzb_ctx_set_occlusion_shape)
 };
 
 // ---- batch: a list of independent frames per launch --------------------------
@@ -743,8 +749,9 @@ struct fdzb_batch {
     Engine eng;
     int triOrder = FDZB_TRI_ORDER_COVERAGE;
     TuneTable tuned;
-    std::vector<int> chosenBins;
+    std::vector<TuneChoice> chosen;
     long long tuneLaunches = 0;
+    int occChunk = 0, occItem = 0;   // a shape set for every frame (0: tuned or default)
 };
 
 namespace {
@@ -786,6 +793,8 @@ int ctx_frame(fdzb_ctx *c, FrameSpec &f)
     f.masks = c->masks;
     f.hasXform = c->hasXform;
     if (c->hasXform) std::memcpy(f.xform, c->xform, sizeof(f.xform));
+    f.occChunk = c->occChunk;
+    f.occItem = c->occItem;
     return FDZB_OK;
 }
 
@@ -797,7 +806,19 @@ int ctx_sync(fdzb_ctx *c)
     return FDZB_OK;
 }
 
-int batch_bins_for(fdzb_batch *b, const FrameSpec &f) { return tuned_bins(b->tuned, f); }
+// A frame without a bin grid takes its class's tuned grid and shape; a shape set
+// on the batch applies to every frame.
+void batch_shape_for(fdzb_batch *b, FrameSpec &f)
+{
+    if (f.bins == 0) {
+        const TuneChoice c = tuned_shape(b->tuned, f);
+        f.bins = c.bins;
+        f.occChunk = c.chunk;
+        f.occItem = c.item;
+    }
+    if (b->occChunk) f.occChunk = b->occChunk;
+    if (b->occItem) f.occItem = b->occItem;
+}
 
 }  // namespace
 
@@ -862,17 +883,28 @@ fdzb::TuneKey fdzb::tune_key(long long S, long long T, int N)
     return TuneKey(ceil_log2(std::max(S, 1ll)), ceil_log2(std::max(T, 1ll)), N);
 }
 
-int fdzb::tuned_bins(const TuneTable &table, const FrameSpec &f)
+fdzb::TuneChoice fdzb::tuned_shape(const TuneTable &table, const FrameSpec &f)
 {
     const long long S = (long long)f.W * f.H;
     auto it = table.find(tune_key(S, (long long)f.nt, f.light.N * 128 + f.light.NC));
-    return it != table.end() ? it->second : heuristic_bins(S);
+    if (it != table.end()) return it->second;
+    TuneChoice c;
+    c.bins = heuristic_bins(S);
+    return c;
 }
 
-// For every size class of `frames` not in `table`: times the grids h/2, h, 2h
-// around the heuristic h, each as a launch of up to 8 copies of the class's
-// first frame (shadows into `scratch`, no masks) so that the GPU is as full as
-// inside a batch, twice; the faster of the two counts.
+bool fdzb::valid_occ_shape(int chunk, int item)
+{
+    return (chunk == 8 || chunk == 16 || chunk == 32) && (item == 32 || item == 64 || item == 128);
+}
+
+// For every size class of `frames` not in `table`, three steps, each candidate
+// timed as a launch of up to 8 copies of the class's first frame (shadows into
+// `scratch`, no masks) so that the GPU is as full as inside a batch, twice,
+// the faster of the two counting: the grids h/2, h, 2h around the heuristic h
+// (32 staged triangles, items of 32 samples); then, at the best grid, staging
+// chunks of 16; then, at the best grid and chunk, items of 64 samples (half as
+// many warps per bin).  Each step keeps a candidate only if it is faster.
 int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec> &frames, float *scratch,
                         size_t scratchFloats, long long *launches)
 {
@@ -898,13 +930,16 @@ int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec
         const int reps = (int)std::max(1ll, std::min<long long>({8, (2'000'000 + S - 1) / S, 1'000'000 / T,
                                                                  (long long)(scratchFloats / S)}));
         const int h = heuristic_bins(S);
-        int best = h;
+        TuneChoice best;
+        best.bins = h;
         float bestMs = 1e30f;
-        for (int cand : {h / 2, h, h * 2}) {
-            if (cand < 4 || cand > kMaxBins) continue;
+        std::vector<TuneChoice> cands;
+        auto timeit = [&](const TuneChoice &c) -> float {
             std::vector<FrameSpec> specs((size_t)reps, f);
             for (int r = 0; r < reps; ++r) {
-                specs[r].bins = cand;
+                specs[r].bins = c.bins;
+                specs[r].occChunk = c.chunk;
+                specs[r].occItem = c.item;
                 specs[r].shadow = scratch + (size_t)r * S;
                 specs[r].masks = nullptr;
             }
@@ -918,12 +953,30 @@ int fdzb::autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec
             }
             if (rc == FDZB_ERR_CAPACITY) {   // too many pairs at this grid: not a candidate
                 rc = FDZB_OK;
-                continue;
+                return 1e30f;
             }
+            return t;
+        };
+        for (int cand : {h / 2, h, h * 2}) {
+            if (cand < 4 || cand > kMaxBins) continue;
+            TuneChoice c;
+            c.bins = cand;
+            const float t = timeit(c);
             if (rc) break;
             if (t < bestMs) {
                 bestMs = t;
-                best = cand;
+                best = c;
+            }
+        }
+        for (int step = 0; step < 2 && rc == FDZB_OK && bestMs < 1e30f; ++step) {
+            TuneChoice c = best;
+            if (step == 0) c.chunk = 16;
+            else c.item = 64;
+            const float t = timeit(c);
+            if (rc) break;
+            if (t < bestMs) {
+                bestMs = t;
+                best = c;
             }
         }
         if (rc) break;
@@ -1033,6 +1086,16 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second)
 {
     if (!lane_ops_per_second) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
     FDZB_CUDA(fdzb::measure_alu_rate(lane_ops_per_second));
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_occlusion_shape(fdzb_ctx *c, int chunk, int item)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (!valid_occ_shape(chunk, item))
+        return fail(FDZB_ERR_INVALID_ARG, "occlusion shape: chunk in {8, 16, 32}, item in {32, 64, 128}");
+    c->occChunk = chunk;
+    c->occItem = item;
     return FDZB_OK;
 }
 
@@ -1303,7 +1366,8 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
     }
     case FDZB_ARR_WORK_COUNTERS: {
         const fdzb::Counters &k = *c->eng.hCounters;
-        const uint64_t v[6] = {k.pairTests, k.rowsEvaluated, k.partialMasks, k.pairsExamined, k.chunks, k.rounds};
+        const uint64_t v[7] = {k.pairTests, k.rowsEvaluated, k.partialMasks, k.pairsExamined, k.chunks, k.rounds,
+                               k.boxSkips};
         if (bytes > sizeof(v)) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
         std::memcpy(dst, v, bytes);
         return FDZB_OK;
@@ -1436,11 +1500,13 @@ int fdzb_batch_launch_async(fdzb_batch *b, const fdzb_frame_desc *frames, int n)
     if (!frames || n <= 0) return fail(FDZB_ERR_INVALID_ARG, "empty frame list");
     if (int rc = engine_sync(b->eng)) return rc;
     std::vector<FrameSpec> specs((size_t)n);
-    b->chosenBins.assign((size_t)n, 0);
+    b->chosen.assign((size_t)n, TuneChoice{});
     for (int i = 0; i < n; ++i) {
         if (int rc = desc_to_spec(frames[i], specs[i], i)) return rc;
-        if (specs[i].bins == 0) specs[i].bins = batch_bins_for(b, specs[i]);
-        b->chosenBins[i] = specs[i].bins;
+        batch_shape_for(b, specs[i]);
+        b->chosen[i].bins = specs[i].bins;
+        b->chosen[i].chunk = specs[i].occChunk;
+        b->chosen[i].item = specs[i].occItem;
     }
     b->eng.frames.swap(specs);
     return engine_launch(b->eng);
@@ -1490,8 +1556,28 @@ int fdzb_batch_get_stats(fdzb_batch *b, fdzb_batch_stats *out)
 int fdzb_batch_frame_bins(fdzb_batch *b, int i)
 {
     if (int rc = batch_check(b)) return rc;
-    if (i < 0 || i >= (int)b->chosenBins.size()) return fail(FDZB_ERR_INVALID_ARG, "frame index out of range");
-    return b->chosenBins[i];
+    if (i < 0 || i >= (int)b->chosen.size()) return fail(FDZB_ERR_INVALID_ARG, "frame index out of range");
+    return b->chosen[i].bins;
+}
+
+int fdzb_batch_frame_shape(fdzb_batch *b, int i, int *bins, int *chunk, int *item)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (i < 0 || i >= (int)b->chosen.size()) return fail(FDZB_ERR_INVALID_ARG, "frame index out of range");
+    if (bins) *bins = b->chosen[i].bins;
+    if (chunk) *chunk = b->chosen[i].chunk;
+    if (item) *item = b->chosen[i].item;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_occlusion_shape(fdzb_batch *b, int chunk, int item)
+{
+    if (int rc = batch_check(b)) return rc;
+    if ((chunk || item) && !valid_occ_shape(chunk ? chunk : 32, item ? item : 32))
+        return fail(FDZB_ERR_INVALID_ARG, "occlusion shape: chunk in {8, 16, 32}, item in {32, 64, 128}");
+    b->occChunk = chunk;
+    b->occItem = item;
+    return FDZB_OK;
 }
 
 // Times candidate bin resolutions for every size class present in `frames`

@@ -33,6 +33,8 @@ struct FrameSpec {
     int accumulate = 0;   // OR into `masks` (a later triangle pass of the same frame)
     bool hasXform = false;  // vertices read through xform (column-major 4x4)
     float xform[16] = {};
+    int occChunk = 32;      // occlusion shape (FrameDesc::occChunk, occItem)
+    int occItem = 32;
 };
 
 // Host-side parameters that a captured graph bakes in; a launch whose key
@@ -134,15 +136,23 @@ void drop_graph(Engine &e);
 // Waits for the engine's stream and frees its arena (the next launch allocates anew).
 void engine_free_arena(Engine &e);
 
-// Autotuner table: bins per side for a size class (ceil(log2 samples),
-// ceil(log2 triangles), light grid N).
+// Autotuner table: for a size class (ceil(log2 samples), ceil(log2 triangles),
+// light grid), the bins per side and the occlusion shape (staged triangles per
+// chunk, samples per warp item).
 using TuneKey = std::tuple<int, int, int>;
-using TuneTable = std::map<TuneKey, int>;
+struct TuneChoice {
+    int bins = 0;
+    int chunk = 32;
+    int item = 32;
+};
+using TuneTable = std::map<TuneKey, TuneChoice>;
 TuneKey tune_key(long long S, long long T, int N);
-// The tuned grid of f's class, else the heuristic.
-int tuned_bins(const TuneTable &table, const FrameSpec &f);
+// The tuned choice of f's class, else the heuristic grid and the default shape.
+TuneChoice tuned_shape(const TuneTable &table, const FrameSpec &f);
 // Tunes every class of `frames` missing from `table` (runs launches on e).
 int autotune_bins(Engine &e, TuneTable &table, const std::vector<FrameSpec> &frames, float *scratch,
                   size_t scratchFloats, long long *launches);
+// True for a supported occlusion shape.
+bool valid_occ_shape(int chunk, int item);
 
 }  // namespace fdzb

@@ -51,6 +51,10 @@ struct FrameDesc {
     LightParams light;
     int hasXform;           // 1: vertices are read through `xform`
     float xform[16];        // column-major model transform (K/moveModel.inl:4-12), applied on read
+    // occlusion shape of the frame: triangles staged per chunk (8, 16 or 32)
+    // and samples per warp work item (32, 64 or 128: a warp takes the item's
+    // samples 32 at a time, so larger items mean fewer warps per bin)
+    int occChunk, occItem;
 };
 
 // Slots of FrameState::acc (order-preserving uint32 encodings of floats).
@@ -92,6 +96,7 @@ struct Counters {
     unsigned long long pairsExamined;   // sample/triangle pairs reaching the AABB pre-cull
     unsigned long long chunks;          // staged triangle chunks (warp-level)
     unsigned long long rounds;          // compute rounds of 32 pair slots (k_occlusion_pairs)
+    unsigned long long boxSkips;        // pairs past the pre-cull skipped by the open-box cull
 };
 
 // Stage boundaries recorded when per-stage timing is on.

@@ -35,6 +35,9 @@ namespace fdzb {
 #ifndef FDZB_OCC_VOTE
 #define FDZB_OCC_VOTE 1
 #endif
+#ifndef FDZB_OCC_REFINE
+#define FDZB_OCC_REFINE 1
+#endif
 
 constexpr int kOccWarps = 4;
 constexpr int kOccThreads = kOccWarps * 32;
@@ -128,6 +131,100 @@ struct LaneSample {
     f3 Q, L0Q;
     float spx, spy, spz, spw, spZ;
 };
+
+// ---------------------------------------------------------------------------
+// Open-box cull (lane per sample, edge-function masks).
+//
+// Seen from the light's upRight corner (the projection M of the light setup),
+// a point X has u = M-projected x and depth w.  Light sample (r, c) lies at
+// camera x = -r |x_delt|, depth 0, so a point P on the segment from light
+// sample row r to the receiver Q satisfies u_P + k_r / w_P = u_Q + k_r / w_Q,
+// k_r = RF.x r / (rows - 1) (RF.x = P00 (rows - 1) |x_delt| / 2, the
+// reference's RectangleFactor).  For rows r in [r0, r1] it follows that some
+// point of the triangle has u + k_r0 / w <= u_Q + k_r0 / w_Q and some point has
+// u + k_r1 / w >= u_Q + k_r1 / w_Q; over a triangle in front of the light
+// plane (every w > 0) u + k / w is linear-fractional, so its extremes are at
+// the vertices.  The same holds for v and the columns.  With r0 = 0 and
+// r1 = rows - 1 this is the reference's own pre-cull (the triangle's AABB
+// against the sample's rectangle, K/Step5_2_shadowCalPerSample.inl:120-128).
+//
+// A sample's unset mask bits lie in a box: rows [r0, r1] (the rows not yet
+// full) by columns [c0, c1] (the columns unset in some open row).  A pair
+// whose triangle fails the test for that box, by a margin of 1e-3 of the
+// sample's rectangle plus 1e-5, cannot set an unset bit: bits outside the box
+// are set already, and inside it the pair's FP32 row masks could only set a
+// bit within FP32 rounding (about 1e-7 of these coordinates) of the exact
+// triangle boundary.  Skipping the pair leaves the mask -- the OR over the
+// bin's triangles -- unchanged.  The box is refreshed at every staged chunk
+// (a stale box is larger, so the test stays conservative), and triangles that
+// reach the light plane (minz <= 0) are never skipped.
+// ---------------------------------------------------------------------------
+struct StagedPrj {
+    float4 a, b;   // (u0, v0, 1/w0, u1), (v1, 1/w1, u2, v2)
+    float c;       // 1/w2
+};
+
+__device__ __forceinline__ void stage_projection(StagedPrj &dst, const float *M, const float4 *__restrict__ rec,
+                                                 int tri)
+{
+    const float4 q0 = __ldg(rec + 4 * (size_t)tri);
+    const float4 q1 = __ldg(rec + 4 * (size_t)tri + 1);
+    const float4 q2 = __ldg(rec + 4 * (size_t)tri + 2);
+    const f3 p0 = light_project(M, mk3(q0.x, q0.y, q0.z));
+    const f3 p1 = light_project(M, mk3(q1.x, q1.y, q1.z));
+    const f3 p2 = light_project(M, mk3(q2.x, q2.y, q2.z));
+    dst.a = make_float4(p0.x, p0.y, __frcp_rn(p0.z), p1.x);
+    dst.b = make_float4(p1.y, __frcp_rn(p1.z), p2.x, p2.y);
+    dst.c = __frcp_rn(p2.z);
+}
+
+// A lane's open box as thresholds: (k_r0, k_r1, u_Q + k_r0/w_Q + mu, u_Q + k_r1/w_Q - mu)
+// and the same for columns and v.
+struct OpenBox {
+    float4 u, v;
+};
+
+template <class R>
+__device__ __forceinline__ int highest_bit(R v)
+{
+    return (int)(8 * sizeof(R)) - 1 - (sizeof(R) == 8 ? __clzll((long long)v) : __clz((int)v));
+}
+
+template <class R>
+__device__ __forceinline__ void open_box(OpenBox &box, const LaneSample &s, const LightParams &L, int NR, int NC,
+                                        R FR, R FC, R fullRows, R (*rows)[32], int lane)
+{
+    const R orow = FR & ~fullRows;
+    R ocol = 0;
+    for (R m = orow; m; m &= m - R(1)) ocol |= ~rows[RowWord<R>::lowest(m)][lane];
+    ocol &= FC;
+    if (!orow || !ocol) {
+        // nothing open: every test fails (the walk ends at this chunk)
+        box.u = make_float4(0.f, 0.f, -kF32Max, kF32Max);
+        box.v = box.u;
+        return;
+    }
+    const float iwq = __frcp_rn(s.spZ);
+    const int r0 = RowWord<R>::lowest(orow), r1 = highest_bit<R>(orow);
+    const int c0 = RowWord<R>::lowest(ocol), c1 = highest_bit<R>(ocol);
+    const float su = NR > 1 ? L.RF[0] / (float)(NR - 1) : 0.f, sv = NC > 1 ? L.RF[1] / (float)(NC - 1) : 0.f;
+    const float ku0 = su * (float)r0, ku1 = su * (float)r1, kv0 = sv * (float)c0, kv1 = sv * (float)c1;
+    const float mu = 1e-3f * L.RF[0] * iwq + 1e-5f, mv = 1e-3f * L.RF[1] * iwq + 1e-5f;
+    box.u = make_float4(ku0, ku1, s.spx + ku0 * iwq + mu, s.spx + ku1 * iwq - mu);
+    box.v = make_float4(kv0, kv1, s.spy + kv0 * iwq + mv, s.spy + kv1 * iwq - mv);
+}
+
+// True if the triangle may set a bit inside the lane's open box.
+__device__ __forceinline__ bool box_reach(const StagedPrj &P, const OpenBox &b)
+{
+    const float4 a = P.a, c = P.b;
+    const float w2 = P.c;
+    const float umin = fminf(fminf(__fmaf_rn(b.u.x, a.z, a.x), __fmaf_rn(b.u.x, c.y, a.w)), __fmaf_rn(b.u.x, w2, c.z));
+    const float umax = fmaxf(fmaxf(__fmaf_rn(b.u.y, a.z, a.x), __fmaf_rn(b.u.y, c.y, a.w)), __fmaf_rn(b.u.y, w2, c.z));
+    const float vmin = fminf(fminf(__fmaf_rn(b.v.x, a.z, a.y), __fmaf_rn(b.v.x, c.y, c.x)), __fmaf_rn(b.v.x, w2, c.w));
+    const float vmax = fmaxf(fmaxf(__fmaf_rn(b.v.y, a.z, a.y), __fmaf_rn(b.v.y, c.y, c.x)), __fmaf_rn(b.v.y, w2, c.w));
+    return umin <= b.u.z && umax >= b.u.w && vmin <= b.v.z && vmax >= b.v.w;
+}
 
 __device__ __forceinline__ void load_sample(LaneSample &s, const FrameDesc &fr, const FrameState &st,
                                             int local)
@@ -380,19 +477,41 @@ __device__ __forceinline__ void write_zero(const FrameDesc &fr, int local)
     }
 }
 
-// k_items: one thread per bin; a bin with n samples yields ceil(n / kItemSamples)
-// items (bin, first sample offset, frame, triangle count).
-__global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restrict__ bse,
-                        const int32_t *__restrict__ bts, const int32_t *__restrict__ bte,
-                        const int *__restrict__ binBases, int nframes, int totalBins,
-                        int4 *__restrict__ items, int capacity, Counters *ctr)
+// Samples per work item of a frame (FrameDesc::occItem; 32 if out of range).
+__device__ __forceinline__ int item_samples(const FrameDesc &fr)
+{
+    const int v = fr.occItem;
+    return (v == 64 || v == 128) ? v : kItemSamples;
+}
+
+// Triangles staged per chunk of a frame (FrameDesc::occChunk, within [1, kOccChunk]).
+__device__ __forceinline__ int chunk_of(const FrameDesc &fr)
+{
+    const int v = fr.occChunk;
+    return (v >= 1 && v <= kOccChunk) ? v : kOccChunk;
+}
+
+// k_items: one thread per bin; a bin with n samples yields ceil(n / item) items
+// (bin, first sample offset, frame, triangle count), item = the frame's samples
+// per work item.
+__global__ void k_items(const FrameDesc *__restrict__ frames, const int32_t *__restrict__ bss,
+                        const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
+                        const int32_t *__restrict__ bte, const int *__restrict__ binBases, int nframes,
+                        int totalBins, int4 *__restrict__ items, int capacity, Counters *ctr)
 {
     const int lane = threadIdx.x & 31;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < totalBins;
          base += gridDim.x * blockDim.x) {
         const int b = base + lane;
-        int n = 0;
-        if (b < totalBins) n = (bse[b] - bss[b] + kItemSamples - 1) / kItemSamples;
+        int n = 0, f = 0, isz = kItemSamples;
+        if (b < totalBins) {
+            const int cnt = bse[b] - bss[b];
+            if (cnt > 0) {
+                f = frame_of(binBases, nframes, b);
+                isz = item_samples(frames[f]);
+                n = (cnt + isz - 1) / isz;
+            }
+        }
         int x = n;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -404,11 +523,10 @@ __global__ void k_items(const int32_t *__restrict__ bss, const int32_t *__restri
         if (lane == 0 && tot) wbase = atomicAdd(&ctr->itemCount, tot);
         wbase = __shfl_sync(kFullWarp, wbase, 0);
         if (n) {
-            const int f = frame_of(binBases, nframes, b);
             const int nt = bte[b] - bts[b];
             for (int k = 0; k < n; ++k) {
                 const int slot = wbase + x - n + k;
-                if (slot < capacity) items[slot] = make_int4(b, kItemSamples * k, f, nt);
+                if (slot < capacity) items[slot] = make_int4(b, isz * k, f, nt);
             }
         }
     }
@@ -429,9 +547,13 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
 {
     __shared__ StagedTri s_tri[RowWord<R>::kWarps][kOccChunk];
     __shared__ R s_rows[RowWord<R>::kWarps][RowWord<R>::kBits][32];
+    constexpr bool kRefine = FDZB_OCC_REFINE && !RAYCAST;
+    __shared__ StagedPrj s_prj[kRefine ? RowWord<R>::kWarps : 1][kRefine ? kOccChunk : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     R(*rows)[32] = s_rows[warp];
     StagedTri *tris = s_tri[warp];
+    StagedPrj *prj = s_prj[kRefine ? warp : 0];
+    unsigned long long boxSkips = 0;
     unsigned long long tested = 0;
     uint32_t nrows = 0, npart = 0;
     int nitems = *(volatile const int *)&ctr->itemCount;
@@ -452,9 +574,10 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
         const FrameState &st = states[fi];
         const int S = fr.W * fr.H;
         const int sLo = bss[bin] + item.y;
-        const int sHi = min(sLo + kItemSamples, bse[bin]);
+        const int sHi = min(sLo + item_samples(fr), bse[bin]);
         const int tS = bts[bin];
         const int nT = bte[bin] - tS;
+        const int chunk = chunk_of(fr);
 
         if (nT <= 0) {
             // no triangle in this bin: shadow 0 -- or, in a later triangle pass,
@@ -474,6 +597,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
         const float esp = fr.esp;
 
         LaneSample smp;
+        OpenBox box;
         int local = 0;
         int remaining = 0;
         R fullRows = 0;
@@ -498,7 +622,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
         }
         int cur = 0;  // offset of the next staged chunk within the bin's list
         while (__any_sync(kFullWarp, active)) {
-            const int m = min(kOccChunk, nT);
+            const int m = min(chunk, nT);
             __syncwarp();
             if (lane < m) {
                 int off = cur + lane;
@@ -509,7 +633,9 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                     tri = 0;
                 }
                 stage_triangle(tris[lane], rec, tri);
+                if (kRefine) stage_projection(prj[lane], fr.light.mat, rec, tri);
             }
+            if (kRefine && remaining > 0) open_box<R>(box, smp, fr.light, g.NR, g.NC, g.FR, g.FC, fullRows, rows, lane);
             __syncwarp();
             for (int t = 0; t < m; ++t) {
 #if FDZB_OCC_VOTE
@@ -517,11 +643,14 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
 #endif
                 if (remaining > 0) {
                     --remaining;
-                    if (RAYCAST)
+                    if (RAYCAST) {
                         tested += raycast_pair<R>(tris[t], smp, ur, xd, yd, g, rows, lane, fullRows, nrows);
-                    else
+                    } else if (kRefine && tris[t].p[1].x > 0.0f && !box_reach(prj[t], box)) {
+                        ++boxSkips;
+                    } else {
                         tested += pair_test<R, DEPTH>(tris[t], smp, xd, yd, ur, esp, g, rows, lane, fullRows,
                                                       nrows, npart);
+                    }
                     if (fullRows == g.FR) remaining = 0;
                 }
             }
@@ -559,18 +688,20 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
             }
         }
     }
-    unsigned long long t = tested, tr = nrows, tp = npart;
+    unsigned long long t = tested, tr = nrows, tp = npart, tb = boxSkips;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         t += __shfl_xor_sync(kFullWarp, t, o);
         tr += __shfl_xor_sync(kFullWarp, tr, o);
         tp += __shfl_xor_sync(kFullWarp, tp, o);
+        tb += __shfl_xor_sync(kFullWarp, tb, o);
     }
     if (lane == 0 && t) {
         atomicAdd(&ctr->pairTests, t);
         atomicAdd(&ctr->rowsEvaluated, tr);
         atomicAdd(&ctr->partialMasks, tp);
     }
+    if (lane == 0 && tb) atomicAdd(&ctr->boxSkips, tb);
 }
 
 

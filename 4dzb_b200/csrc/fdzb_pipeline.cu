@@ -850,7 +850,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     // (c) + (d) occlusion and shading
     if (ev) cudaEventRecord(ev[STAGE_OCCLUSION], s);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
-        b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
+        b.frames, b.binSampleStart, b.binSampleEnd, b.binTriStart, b.binTriEnd, b.binBases, nf, b.totalBins,
         b.items, b.itemCapacity, b.counters);
     // 64-bit row words when some frame's grid exceeds 32 rows or columns; the
     // lane-per-pair schedule only runs square 32-bit grids without the depth

@@ -471,7 +471,12 @@ int fdzb_serve_submit(fdzb_server *s, const fdzb_request *q, uint64_t *ticket)
     r.outBytes = (size_t)S * 4 + (q->d_masks ? (size_t)S * 4 * ((r.spec.light.N * r.spec.light.NC + 31) / 32) : 0);
     {
         std::lock_guard<std::mutex> g(s->mu);
-        if (r.spec.bins == 0) r.spec.bins = fdzb::tuned_bins(s->tuned, r.spec);
+        if (r.spec.bins == 0) {
+            const fdzb::TuneChoice c = fdzb::tuned_shape(s->tuned, r.spec);
+            r.spec.bins = c.bins;
+            r.spec.occChunk = c.chunk;
+            r.spec.occItem = c.item;
+        }
         r.tSubmit = now_s();
         if (s->tFirstSubmit < 0) s->tFirstSubmit = r.tSubmit;
         const uint64_t t = s->nextTicket++;

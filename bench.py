@@ -347,9 +347,10 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
     t0 = time.time()
     bat.autotune(d_tune, scratch)
     tune_s = time.time() - t0
-    bat.launch(d_tune)                       # bins from the tuner; captures the graph
-    bins = [bat.frame_bins(i) for i in range(nframes)]
-    d_batch = [desc(i, bins[i]) for i in range(nframes)]
+    bat.launch(d_tune)                       # bins and shapes from the tuner; captures the graph
+    shapes = [bat.frame_shape(i) for i in range(nframes)]
+    bins = [sh[0] for sh in shapes]
+    d_batch = d_tune
     for _ in range(2):
         bat.launch(d_batch)
 
@@ -372,16 +373,21 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
     plain.set_stream(stream.cuda_stream)
     plain.set_graph(False)                   # every frame has a new shape: nothing to replay
     d_plain = [[desc(i, bins[i], plain=True)] for i in range(nframes)]
-    for d in d_plain:                        # warm-up: grows the arena to the largest frame
-        plain.launch(d)
+
+    def plain_launch(i):                     # the frame's tuned grid and occlusion shape
+        plain.set_occlusion_shape(shapes[i][1], shapes[i][2])
+        plain.launch(d_plain[i])
+
+    for i in range(nframes):                 # warm-up: grows the arena to the largest frame
+        plain_launch(i)
     plain_ms = []
     pair_tests = 0
     for _ in range(max(2, steps // 2)):
         a, b = ev(), ev()
         a.record(stream)
         pair_tests = 0
-        for d in d_plain:
-            plain.launch(d)
+        for i in range(nframes):
+            plain_launch(i)
             pair_tests += plain.frame_stats(0)["pair_tests"]
         b.record(stream)
         stream.synchronize()
@@ -389,10 +395,38 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
     same = all(torch.equal(t["masks"], t["pmasks"]) and torch.equal(t["shadow"], t["pshadow"]) for t in dev)
     ms_b = statistics.mean(batch_ms)
     ms_p = statistics.mean(plain_ms)
+    # Where the time goes (stage events; one extra pass of each form): the
+    # occlusion stage of the plain loop, frame by frame, and of the batch.  A
+    # batch can remove launch gaps and the short stages and fill the GPU during
+    # small frames, but it runs the same pair tests; if everything but its own
+    # occlusion stage took no time, it would run plain_ms / batch_occlusion_ms
+    # times faster than the plain loop -- the cap on its speed-up.
+    plain.set_profiling(True)
+    p_occ = p_all = 0.0
+    for i in range(nframes):
+        plain_launch(i)
+        st = plain.frame_stats(0)["stage_ms"]
+        p_occ += st[4]
+        p_all += sum(st)
+    plain.set_profiling(False)
+    bat.set_profiling(True)
+    bat.launch(d_batch)
+    b_stage = bat.stats()["totals"]["stage_ms"]
+    bat.set_profiling(False)
+    bat.launch(d_batch)
+    amdahl = {"plain_stage_ms": p_all, "plain_occlusion_ms": p_occ,
+              "plain_occlusion_share": p_occ / ms_p, "batch_stage_ms": [round(x, 3) for x in b_stage],
+              "batch_occlusion_ms": b_stage[4], "batch_occlusion_share": b_stage[4] / ms_b,
+              "speedup_cap": ms_p / b_stage[4] if b_stage[4] > 0 else None,
+              "note": "speedup_cap = plain loop ms / the batch's own occlusion-stage ms: the batched form "
+                      "cannot beat it without making the pair tests themselves faster"}
     sxt = sum(s.S * s.T for s in frames)
-    hist = {}
+    hist, shist = {}, {}
     for g in bins:
         hist[str(g)] = hist.get(str(g), 0) + 1
+    for sh in shapes:
+        k = f"bins {sh[0]}, chunk {sh[1]}, item {sh[2]}"
+        shist[k] = shist.get(k, 0) + 1
     out = {
         "workload": f"{nframes} frames: samples log-uniform [256^2, 1920x1080], triangles log-uniform "
                     "[10k, 500k], N in {8, 16}, light side uniform [0.5, 4], seeds 1000+k",
@@ -405,7 +439,8 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
         "plain_pair_tests": pair_tests, "batch_pair_tests": bst["totals"]["pair_tests"],
         "masks_identical": bool(same), "graph": bool(bst["from_graph"]),
         "graph_replays": bst["graph_replays"], "kernel_launches_per_batch": bst["totals"]["kernel_launches"],
-        "tuned_bins": hist, "tuned_classes": bst["tuned_classes"], "autotune_s": tune_s,
+        "amdahl": amdahl,
+        "tuned_bins": hist, "tuned_shapes": shist, "tuned_classes": bst["tuned_classes"], "autotune_s": tune_s,
         "autotune_launches": bst["tune_launches"], "generate_s": gen_s, "steps": steps,
         "timing": "CUDA events on the launch stream; inputs > L2",
     }
@@ -437,7 +472,8 @@ def receiver_on_device(torch, W: int, H: int, seed: int, offset=(0.0, 0.0)):
     return pos, nrm
 
 
-def served_workload(fdzb, torch, stream, rates=(100, 500, 2000), counts=(120, 240, 360)) -> dict:
+def served_workload(fdzb, torch, stream, rates=(25, 25, 50, 100, 500, 2000),
+                    counts=(100, 200, 200, 120, 240, 360)) -> dict:
     """8 resident scenes (triangles log-uniform in [50k, 1M], seeds 2000+k);
     requests (seed 3000) arrive Poisson at each rate, each with a scene id, a
     camera-jittered view buffer of 512^2 .. 3840x2160 samples (a pool of 12
@@ -587,10 +623,15 @@ def served_workload(fdzb, torch, stream, rates=(100, 500, 2000), counts=(120, 24
         same = same and r["status"] == 0 and torch.equal(outs[2][0][:W * H], outs[3][0][:W * H]) and \
             torch.equal(outs[2][1][:W * H * nw], outs[3][1][:W * H * nw])
     sat = max(p["frames_per_s"] for p in per_rate)
+    # below capacity (arrival rate under the saturated frame rate) latency is
+    # service time, not backlog: p99 should not grow with the request count
+    below = [p for p in per_rate if p["rate_req_s"] < 0.8 * sat]
     out = {
         "workload": "8 resident scenes (50k..1M triangles), Poisson requests, views 512^2..3840x2160 "
                     "(12-view pool, camera-jittered), light side U[0.5, 4], N in {8, 16}, 150 GB budget",
         "slots": 2, "max_batch_frames": 16, "rates": per_rate,
+        "below_capacity": [{"rate_req_s": p["rate_req_s"], "requests": p["requests"], "p50_ms": p["p50_ms"],
+                            "p99_ms": p["p99_ms"]} for p in below],
         "saturated_frames_per_s": sat, "plain_frames_per_s": plain_fps, "speedup_vs_plain": sat / plain_fps,
         "results_identical_to_plain": bool(same), "tuned_classes": srv.stats()["tuned_classes"],
         "autotune_s": tune_s, "generate_s": gen_s,

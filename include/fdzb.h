@@ -215,10 +215,10 @@ enum fdzb_array_id {
     FDZB_ARR_BIN_TRI_START,         /* int32[num_bins] */
     FDZB_ARR_BIN_TRI_END,           /* int32[num_bins] */
     FDZB_ARR_TRI_AABB,              /* float[8*T] (min xyz,1, max xyz,1) */
-    FDZB_ARR_WORK_COUNTERS,         /* uint64[6] occlusion work: pair tests, light rows, partial row
+    FDZB_ARR_WORK_COUNTERS,         /* uint64[7] occlusion work: pair tests, light rows, partial row
                                        masks, pairs reaching the AABB pre-cull, triangle chunks,
-                                       compute rounds (the last three: counted by the pair-compacting
-                                       occlusion kernel only) */
+                                       compute rounds (these three: counted by the pair-compacting
+                                       occlusion kernel only), pairs skipped by the open-box cull */
     FDZB_ARR_COUNT
 };
 int fdzb_ctx_export(fdzb_ctx *ctx, int what, void *dst, size_t bytes);
@@ -377,6 +377,15 @@ const char *fdzb_version(void);
  * stream. */
 int fdzb_ctx_set_graph(fdzb_ctx *ctx, int enable);
 
+/* Occlusion shape, no counterpart in the reference (its per-sample kernel runs
+ * one thread per sample, K/Step5_2_shadowCalPerSample.inl:236-260): chunk =
+ * triangles of a bin's list staged in shared memory per round (8, 16 or 32,
+ * default 32); item = samples of one bin per warp work item (32, 64 or 128,
+ * default 32; a warp takes an item's samples 32 at a time, so larger items
+ * put fewer warps on a bin).  Results are identical for every shape; the
+ * batch and server autotuners pick it per size class. */
+int fdzb_ctx_set_occlusion_shape(fdzb_ctx *ctx, int chunk, int item);
+
 /* Testing aids, no counterpart in the reference.  The sorts' decoupled
  * look-back tags its status words with the context's launch number (a device
  * word advanced by every launch; FS/api.cpp:402-582 has no look-back: Thrust's
@@ -454,11 +463,18 @@ int fdzb_batch_get_frame_stats(fdzb_batch *batch, int frame, fdzb_frame_stats *o
 int fdzb_batch_get_stats(fdzb_batch *batch, fdzb_batch_stats *out);
 /* Bins per side used for frame i of the last launch (>0), or an error code. */
 int fdzb_batch_frame_bins(fdzb_batch *batch, int frame);
+/* Bins per side and occlusion shape (see fdzb_ctx_set_occlusion_shape) used
+ * for frame i of the last launch. */
+int fdzb_batch_frame_shape(fdzb_batch *batch, int frame, int *bins, int *chunk, int *item);
+/* An occlusion shape for every frame of later launches (0, 0: each frame's
+ * tuned or default shape). */
+int fdzb_batch_set_occlusion_shape(fdzb_batch *batch, int chunk, int item);
 /* Autotuner: for every size class (ceil(log2 samples), ceil(log2 triangles), N)
  * of the frames with bins == 0 not tuned yet, times three bin grids around
- * ~128 samples per bin (each as a launch of up to 8 copies of the class's first
- * frame, so that the GPU is as full as inside a batch) and keeps the fastest
- * for later launches of this batch.  d_scratch: device float[scratch_floats],
+ * ~128 samples per bin, then at the best grid a staging chunk of 16 triangles,
+ * then items of 64 samples (each candidate a launch of up to 8 copies of the
+ * class's first frame, so that the GPU is as full as inside a batch) and keeps
+ * the fastest grid and occlusion shape for later launches of this batch.  d_scratch: device float[scratch_floats],
  * at least one frame's W*H (receives the copies' shadows). */
 int fdzb_batch_autotune(fdzb_batch *batch, const fdzb_frame_desc *frames, int n, float *d_scratch,
                         size_t scratch_floats);

@@ -151,3 +151,10 @@ def test_noalloc_sort_rejects_overlapping_buffers(fdzb):
     for a, b, c, d, st in bad:
         assert fn(a, b, c, d, n, 64, None, st) == -1
         assert b"overlap" in lib.fdzb_last_error()
+
+
+def test_occlusion_shape_arguments_are_checked(fdzb):
+    """Shapes outside {8, 16, 32} x {32, 64, 128} are refused before any GPU work."""
+    lib = fdzb.load()
+    assert lib.fdzb_ctx_set_occlusion_shape(None, 32, 32) == -3        # no context
+    assert lib.fdzb_batch_set_occlusion_shape(None, 16, 64) == -3

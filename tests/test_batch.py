@@ -179,3 +179,56 @@ def test_batch_reference_and_depth_order_same_masks(cuda_ok, fdzb, scenes):
     for i, t in enumerate(tens):
         assert np.array_equal(t["masks"].cpu().numpy(), depth[i]), i
     b.close()
+
+
+@pytest.mark.parametrize("chunk", [8, 16, 32])
+@pytest.mark.parametrize("item", [32, 64, 128])
+def test_every_occlusion_shape_gives_the_same_masks(cuda_ok, fdzb, scenes, chunk, item):
+    """Staging chunk and samples per warp item (the shapes the autotuner picks
+    from) change the schedule only: masks and shadows equal the default shape's
+    and the oracle's, in a batch and in a context."""
+    fr = _frames(scenes, 4, seed_base=5500)
+    tens = [_upload(fdzb, s) for s in fr]
+    d = [_desc(fdzb, s, t) for s, t in zip(fr, tens)]
+    b = fdzb.Batch()
+    b.launch(d)
+    base = [(t["shadow"].cpu().numpy().copy(), t["masks"].cpu().numpy().copy()) for t in tens]
+    for t in tens:
+        t["shadow"].fill_(-1.0)
+        t["masks"].zero_()
+    b.set_occlusion_shape(chunk, item)
+    b.launch(d)
+    for i, t in enumerate(tens):
+        assert b.frame_shape(i) == (fr[i].bins, chunk, item)
+        _check_same(t["shadow"].cpu().numpy(), base[i][0], f"frame {i} shadow, shape {chunk}x{item}")
+        _check_same(t["masks"].cpu().numpy().view(np.uint32), base[i][1].view(np.uint32), f"frame {i} masks")
+    b.close()
+    s = scenes.make_scene(300, 200, 4000, n=16, bins=32, seed=61, sigma=0.1)
+    ctx, t = fdzb.context_for_scene(s, masks=True)
+    ctx.set_occlusion_shape(chunk, item)
+    ctx.launch()
+    o = oracle.frame(s)
+    _check_same(t["shadow"].cpu().numpy(), o.arrays["shadow"].astype(np.float32), "context shadow vs oracle")
+    _check_same(t["masks"].cpu().numpy().view(np.uint32), o.arrays["masks"].astype(np.uint32), "context masks")
+    ctx.close()
+
+
+def test_autotuner_reports_a_shape_per_frame(cuda_ok, fdzb, scenes):
+    import torch
+    fr = _frames(scenes, 4, seed_base=5600)
+    tens = [_upload(fdzb, s) for s in fr]
+    d = [_desc(fdzb, s, t, bins=0) for s, t in zip(fr, tens)]
+    scratch = torch.empty(max(s.S for s in fr) * 8, dtype=torch.float32, device="cuda")
+    b = fdzb.Batch()
+    b.autotune(d, scratch)
+    b.launch(d)
+    for i, s in enumerate(fr):
+        g, chunk, item = b.frame_shape(i)
+        assert g == b.frame_bins(i) and chunk in fdzb.OCC_CHUNKS and item in fdzb.OCC_ITEMS
+        import dataclasses
+        ctx, t = fdzb.context_for_scene(dataclasses.replace(s, bins=g), masks=True)
+        ctx.launch()
+        _check_same(tens[i]["masks"].cpu().numpy().view(np.uint32), t["masks"].cpu().numpy().view(np.uint32),
+                    f"frame {i} masks, tuned shape {(g, chunk, item)}")
+        ctx.close()
+    b.close()
