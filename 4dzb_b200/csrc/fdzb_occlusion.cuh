@@ -38,6 +38,9 @@ namespace fdzb {
 #ifndef FDZB_OCC_REFINE
 #define FDZB_OCC_REFINE 1
 #endif
+#ifndef FDZB_OCC_UNION
+#define FDZB_OCC_UNION 0
+#endif
 
 constexpr int kOccWarps = 4;
 constexpr int kOccThreads = kOccWarps * 32;
@@ -190,19 +193,23 @@ __device__ __forceinline__ int highest_bit(R v)
     return (int)(8 * sizeof(R)) - 1 - (sizeof(R) == 8 ? __clzll((long long)v) : __clz((int)v));
 }
 
+// Returns false when the box is the whole grid: the test would then repeat the
+// reference's pre-cull and is not worth its instructions.
 template <class R>
-__device__ __forceinline__ void open_box(OpenBox &box, const LaneSample &s, const LightParams &L, int NR, int NC,
+__device__ __forceinline__ bool open_box(OpenBox &box, const LaneSample &s, const LightParams &L, int NR, int NC,
                                         R FR, R FC, R fullRows, R (*rows)[32], int lane)
 {
     const R orow = FR & ~fullRows;
     R ocol = 0;
     for (R m = orow; m; m &= m - R(1)) ocol |= ~rows[RowWord<R>::lowest(m)][lane];
     ocol &= FC;
+    const bool whole = orow == FR && ocol == FC;
+    if (whole && !FDZB_OCC_UNION) return false;
     if (!orow || !ocol) {
         // nothing open: every test fails (the walk ends at this chunk)
         box.u = make_float4(0.f, 0.f, -kF32Max, kF32Max);
         box.v = box.u;
-        return;
+        return true;
     }
     const float iwq = __frcp_rn(s.spZ);
     const int r0 = RowWord<R>::lowest(orow), r1 = highest_bit<R>(orow);
@@ -212,6 +219,41 @@ __device__ __forceinline__ void open_box(OpenBox &box, const LaneSample &s, cons
     const float mu = 1e-3f * L.RF[0] * iwq + 1e-5f, mv = 1e-3f * L.RF[1] * iwq + 1e-5f;
     box.u = make_float4(ku0, ku1, s.spx + ku0 * iwq + mu, s.spx + ku1 * iwq - mu);
     box.v = make_float4(kv0, kv1, s.spy + kv0 * iwq + mv, s.spy + kv1 * iwq - mv);
+    return !whole;
+}
+
+// The union over the warp's active lanes of their boxes: a triangle that one
+// lane's test passes passes the union's (smaller k and larger threshold on
+// the min side, the reverse on the max side, since 1/w > 0), so a triangle the
+// union test rejects is rejected by every lane's.
+__device__ __forceinline__ OpenBox union_box(const OpenBox &b, bool active)
+{
+    float a0 = active ? b.u.x : kF32Max, a1 = active ? b.u.y : -kF32Max;
+    float a2 = active ? b.u.z : -kF32Max, a3 = active ? b.u.w : kF32Max;
+    float c0 = active ? b.v.x : kF32Max, c1 = active ? b.v.y : -kF32Max;
+    float c2 = active ? b.v.z : -kF32Max, c3 = active ? b.v.w : kF32Max;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 = fminf(a0, __shfl_xor_sync(kFullWarp, a0, o));
+        a1 = fmaxf(a1, __shfl_xor_sync(kFullWarp, a1, o));
+        a2 = fmaxf(a2, __shfl_xor_sync(kFullWarp, a2, o));
+        a3 = fminf(a3, __shfl_xor_sync(kFullWarp, a3, o));
+        c0 = fminf(c0, __shfl_xor_sync(kFullWarp, c0, o));
+        c1 = fmaxf(c1, __shfl_xor_sync(kFullWarp, c1, o));
+        c2 = fmaxf(c2, __shfl_xor_sync(kFullWarp, c2, o));
+        c3 = fminf(c3, __shfl_xor_sync(kFullWarp, c3, o));
+    }
+    OpenBox u;
+    u.u = make_float4(a0, a1, a2, a3);
+    u.v = make_float4(c0, c1, c2, c3);
+    return u;
+}
+
+// The reference's pre-cull of a pair (K/Step5_2_shadowCalPerSample.inl:120-128).
+__device__ __forceinline__ bool precull_pass(const StagedTri &T, const LaneSample &s)
+{
+    const float4 p0 = T.p[0];
+    return p0.x <= s.spx && p0.y <= s.spy && s.spz <= p0.z && s.spw <= p0.w && T.p[1].x <= s.spZ;
 }
 
 // True if the triangle may set a bit inside the lane's open box.
@@ -598,6 +640,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
 
         LaneSample smp;
         OpenBox box;
+        bool boxOn = false;
         int local = 0;
         int remaining = 0;
         R fullRows = 0;
@@ -635,17 +678,36 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                 stage_triangle(tris[lane], rec, tri);
                 if (kRefine) stage_projection(prj[lane], fr.light.mat, rec, tri);
             }
-            if (kRefine && remaining > 0) open_box<R>(box, smp, fr.light, g.NR, g.NC, g.FR, g.FC, fullRows, rows, lane);
+            if (kRefine && remaining > 0)
+                boxOn = open_box<R>(box, smp, fr.light, g.NR, g.NC, g.FR, g.FC, fullRows, rows, lane);
             __syncwarp();
+#if FDZB_OCC_UNION
+            // triangles of the chunk that no active lane's box can use are
+            // skipped by the whole warp (each lane would skip them anyway);
+            // a lane's cycle covers the chunk's first rem0 triangles
+            unsigned keep = m >= 32 ? kFullWarp : ((1u << m) - 1u);
+            const int rem0 = remaining;
+            if (kRefine) {
+                const OpenBox ub = union_box(box, remaining > 0);
+                const bool k = lane < m && (tris[lane].p[1].x <= 0.0f || box_reach(prj[lane], ub));
+                keep &= __ballot_sync(kFullWarp, k);
+            }
+            for (unsigned km = keep; km; km &= km - 1u) {
+                const int t = __ffs(km) - 1;
+                if (!__any_sync(kFullWarp, remaining > 0 && t < rem0)) break;
+                if (remaining > 0 && t < rem0) {
+#else
             for (int t = 0; t < m; ++t) {
 #if FDZB_OCC_VOTE
                 if (!__any_sync(kFullWarp, remaining > 0)) break;
 #endif
                 if (remaining > 0) {
                     --remaining;
+#endif
                     if (RAYCAST) {
                         tested += raycast_pair<R>(tris[t], smp, ur, xd, yd, g, rows, lane, fullRows, nrows);
-                    } else if (kRefine && tris[t].p[1].x > 0.0f && !box_reach(prj[t], box)) {
+                    } else if (kRefine && boxOn && tris[t].p[1].x > 0.0f && precull_pass(tris[t], smp) &&
+                               !box_reach(prj[t], box)) {
                         ++boxSkips;
                     } else {
                         tested += pair_test<R, DEPTH>(tris[t], smp, xd, yd, ur, esp, g, rows, lane, fullRows,
@@ -654,6 +716,9 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                     if (fullRows == g.FR) remaining = 0;
                 }
             }
+#if FDZB_OCC_UNION
+            if (remaining > 0) remaining = rem0 > m ? rem0 - m : 0;
+#endif
             cur += m;
             if (cur >= nT) cur -= nT;
             // retire finished lanes, then refill them with the item's next samples

@@ -515,9 +515,12 @@ __global__ void k_tri_order(const FrameState *__restrict__ states, const int *__
 // Candidate bins of a triangle, swept by a warp 32 at a time in row-major
 // order; returns the number accepted and, with write != nullptr, writes the
 // accepted (bin, triangle) pairs from position `pos` on, in order.
+// With hist (the block's shared digit histograms of the pair sort), every
+// written key is also counted there, one histogram per radix pass.
 __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, const TriBins &c, int bb, int l2,
                                           int lane, uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals,
-                                          unsigned long long pos, int capacity, int g, bool write)
+                                          unsigned long long pos, int capacity, int g, bool write,
+                                          uint32_t *hist = nullptr, int histPasses = 0)
 {
     const int w = c.cex - c.cbx, h = c.cey - c.cby;
     if (w <= 0 || h <= 0) return 0;
@@ -535,11 +538,22 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
             ok = bin_accepts(binStat, gb, c);
         }
         const unsigned m = __ballot_sync(kFullWarp, ok);
+        bool stored = false;
         if (write && ok) {
             const unsigned long long p = pos + (unsigned long long)total + (unsigned)__popc(m & lanemask_lt());
             if (p < (unsigned long long)capacity) {
                 pkeys[p] = (uint32_t)gb;
                 pvals[p] = (uint32_t)g;
+                stored = true;
+            }
+        }
+        if (hist) {
+            // digits of the stored keys; lanes with equal digits add once
+            const unsigned sm_ = __ballot_sync(kFullWarp, stored);
+            for (int d = 0; d < histPasses; ++d) {
+                const uint32_t dig = ((uint32_t)gb >> (8 * d)) & 255u;
+                const unsigned peers = __match_any_sync(kFullWarp, stored ? dig : 256u + (unsigned)lane) & sm_;
+                if (stored && (peers & lanemask_lt()) == 0) atomicAdd(&hist[d * 256 + dig], (uint32_t)__popc(peers));
             }
         }
         total += __popc(m);
@@ -566,9 +580,12 @@ __global__ void __launch_bounds__(kTriThreads)
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
                 int32_t *__restrict__ triCount, unsigned long long *scanStatus, const uint32_t *epochWord,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
-                const uint32_t *__restrict__ order, Counters *ctr)
+                const uint32_t *__restrict__ order, Counters *ctr, uint32_t *pairHist, int histPasses)
 {
     constexpr int WARPS = kTriThreads / 32;
+    // digit histograms of the written pair keys for the pair sort's passes
+    // (its separate histogram pass over the keys is then not needed)
+    __shared__ uint32_t s_hist[2 * 256];
     __shared__ int s_tile;
     __shared__ int s_cnt[kTriThreads];
     __shared__ unsigned long long s_wsum[WARPS];
@@ -576,6 +593,9 @@ __global__ void __launch_bounds__(kTriThreads)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (totalTris + kTriThreads - 1) / kTriThreads;
     const uint32_t epoch = *epochWord;
+    if (histPasses > 2) histPasses = 2;
+    uint32_t *hist = (pairHist && histPasses > 0) ? s_hist : nullptr;
+    for (int i = tid; i < 2 * 256; i += kTriThreads) s_hist[i] = 0u;
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&ctr->triTileCounter, 1);
@@ -673,8 +693,13 @@ __global__ void __launch_bounds__(kTriThreads)
             const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
             if (!c.any) continue;
             sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals,
-                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true);
+                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true, hist, histPasses);
         }
+    }
+    if (hist) {
+        __syncthreads();
+        for (int i = tid; i < histPasses * 256; i += kTriThreads)
+            if (s_hist[i]) atomicAdd(&pairHist[i], s_hist[i]);
     }
 }
 
@@ -740,11 +765,12 @@ static int grid_for(long long n, int threads, int cap)
 // 16*launch + 4*slot + p.
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
-                     cudaStream_t s)
+                     cudaStream_t s, bool histDone = false)
 {
     uint32_t *hist = b.sortHist + slot * 4 * kRadix;
-    k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
-                                                                              cap, passes, hist);
+    if (!histDone)
+        k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
+                                                                                  cap, passes, hist);
     uint32_t *ki = kA, *vi = vA, *ko = kB, *vo = vB;
     const long long tiles = ((long long)cap + kSortTile - 1) / kSortTile;
     const int passGrid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
@@ -762,6 +788,10 @@ static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *v
         vo = t;
     }
 }
+
+#ifndef FDZB_PAIR_HIST_INLINE
+#define FDZB_PAIR_HIST_INLINE 1
+#endif
 
 static int g_smCount = 0;
 
@@ -811,7 +841,11 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
         (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
     nl += 2 + b.samplePasses;
-    // (a) triangle/bin pairs, in the coverage order when one is asked for
+    // (a) triangle/bin pairs, in the coverage order when one is asked for; the
+    // pair sort's digit histograms are built as the pairs are written when its
+    // keys (global bins) take at most two 8-bit passes (up to 65,536 bins in
+    // the launch); beyond that the sort's own histogram pass runs
+    const bool pairHistInline = FDZB_PAIR_HIST_INLINE && b.pairPasses <= 2;
     if (ev) cudaEventRecord(ev[STAGE_TRI_PAIRS], s);
     const uint32_t *order = nullptr;
     if (b.depthBits > 0 && b.totalTris > 0) {
@@ -830,7 +864,9 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 order, b.counters);
+                                                 order, b.counters, pairHistInline ? b.sortHist + 4 * kRadix
+                                                                                   : nullptr,
+                                                 pairHistInline ? b.pairPasses : 0);
         nl += 1;
     }
     if (b.dbgPKeys) {
@@ -840,13 +876,13 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     // (b) pair sort and segments
     if (ev) cudaEventRecord(ev[STAGE_PAIR_SORT], s);
     run_sort(b, 1, b.pkeysA, b.pvalsA, b.pkeysB, b.pvalsB, &b.counters->pairCount, 0, b.pairCapacity,
-             b.pairPasses, sm, s);
+             b.pairPasses, sm, s, pairHistInline);
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
     uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
         pk, &b.counters->pairCount, 0, b.pairCapacity, 0, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
-    nl += 2 + b.pairPasses;
+    nl += (pairHistInline ? 1 : 2) + b.pairPasses;
     // (c) + (d) occlusion and shading
     if (ev) cudaEventRecord(ev[STAGE_OCCLUSION], s);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(

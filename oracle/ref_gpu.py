@@ -51,7 +51,7 @@ class RefGpuOut(ctypes.Structure):
                 ("model_aabb", ctypes.c_float * 8), ("first_error", ctypes.c_char * 160),
                 ("surf_handle", ctypes.c_int64), ("pos_tex_handle", ctypes.c_int64), ("view_error", ctypes.c_int64),
                 ("masks", ctypes.POINTER(ctypes.c_uint32)), ("stage_ms", f32p), ("bins", ctypes.c_int32),
-                ("pad0", ctypes.c_int32)]
+                ("pad0", ctypes.c_int32), ("q2_events", ctypes.c_int64)]
 
 
 _libs: dict = {}

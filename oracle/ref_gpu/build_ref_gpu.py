@@ -32,12 +32,17 @@ the repository:
 * the kernel files K/*.inl are concatenated, in the order of K/FourD.cu:230-257,
   between harness_pre.cuh and harness_post.cuh into a temporary .cu under
   oracle/_ref/ that is deleted after compiling.  The concatenation changes
-  four things only, each checked to apply exactly once:
+  five things only, each checked to apply exactly once:
     - the nested includes of Step2_3 (already concatenated) are dropped and the
       backslash include path of moveModel.inl is normalised;
     - the unguarded per-frame pair dump `showBinTriPair(pairNum);`
       (K/Step4_RasterizeTriangleToBin.inl:218, a full device-to-host copy and
       an fprintf per pair into a Windows path) is removed from bindTriToBin;
+    - writeTriBinPair_kernel (:161-204) counts each pair it writes beyond the
+      count the counting kernel gave its triangle (REFGPU_Q2_MARK): the write
+      kernel tests the unclamped AABB and the counting kernel the clamped one
+      (:74-94 against :177-193), so a triangle can write into the next
+      triangle's slots, and which write lands there depends on scheduling;
     - in the per-sample kernel's row loop
       (K/Step5_2_shadowCalPerSample.inl:204-222) a row index >= N is counted
       and skipped instead of indexing past the sample's N rows of shared
@@ -87,6 +92,8 @@ HOST_SOURCES = [os.path.join(FS, "api.cpp"), os.path.join(FS, "util", "cudaBuffe
 EDITS = [
     ("Step4_RasterizeTriangleToBin.inl", "showBinTriPair(pairNum);",
      "/* per-frame pair dump removed by the harness */"),
+    ("Step4_RasterizeTriangleToBin.inl", "triPos[cnt] = tid;",
+     "triPos[cnt] = tid; REFGPU_Q2_MARK(cnt, tid)"),
     ("Step5_2_shadowCalPerSample.inl", "mask[rowID*32] |= M0 & M1 & M2;",
      "REFGPU_ROW_GUARD(rowID, lightResHeight) mask[rowID*32] |= M0 & M1 & M2;"),
     ("Step5_2_shadowCalPerSample.inl", "shadowResult[sampleID] = (float)result / (float)lightResNum;",

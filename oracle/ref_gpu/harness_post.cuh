@@ -230,6 +230,8 @@ struct RefGpuOut {
     float *stage_ms;
     int32_t bins;                    // the build's bins per side (FD_MAX_LP_GRID_SIZE)
     int32_t pad0;
+    int64_t q2_events;               // pairs written beyond their triangle's count (REFGPU_Q2_MARK),
+                                     // summed over all launches
 };
 
 static int refgpu_round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -301,6 +303,7 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     m_validSampleNum = 0;
     unsigned long long zero = 0;
     checkCudaErrors(cudaMemcpyToSymbol(refgpu_rows_beyond_n, &zero, sizeof(zero)));
+    checkCudaErrors(cudaMemcpyToSymbol(refgpu_q2_events, &zero, sizeof(zero)));
     // mask dump: N + 1 words per output slot of the reference's padded index
     const size_t dumpWords = (size_t)(in->lightRes + 1);
     const size_t dumpBytes = pitch * H * dumpWords * sizeof(uint32_t);
@@ -381,6 +384,9 @@ extern "C" int ref_gpu_frame(const RefGpuIn *in, RefGpuOut *out)
     unsigned long long rows = 0;
     checkCudaErrors(cudaMemcpyFromSymbol(&rows, refgpu_rows_beyond_n, sizeof(rows)));
     out->rows_beyond_n = (int64_t)rows;
+    unsigned long long q2 = 0;
+    checkCudaErrors(cudaMemcpyFromSymbol(&q2, refgpu_q2_events, sizeof(q2)));
+    out->q2_events = (int64_t)q2;
     out->pos_tex_handle = (int64_t)FDSample::positionTexObj;
 
     std::vector<float> pbo(pitch * H, 0.0f);

@@ -62,6 +62,14 @@ __device__ unsigned long long refgpu_rows_beyond_n;
         continue;                                         \
     }
 
+// Harness counter: pairs the write kernel puts beyond its triangle's counted
+// slots (reference quirk: count and write kernels test different AABBs, so the
+// extra pair overwrites the next triangle's first slot, racing with it).
+__device__ unsigned long long refgpu_q2_events;
+#define REFGPU_Q2_MARK(cnt, tid)                                                   \
+    if ((cnt) >= ((const int *)c_fdStaticParams.triBinNum)[(tid)])                \
+        atomicAdd(&refgpu_q2_events, 1ull);
+
 // Harness mask dump: after the per-sample kernel's shadow store
 // (K/Step5_2_shadowCalPerSample.inl:231) the sample's final light rows, when
 // the harness has set refgpu_mask_out: per sample (at the kernel's output

@@ -54,6 +54,8 @@ def _rows_of(words, n):
 def _check(fdzb, scene, ref, bins=ref_gpu.REF_BINS, tri_order=0):
     sh, mk, st = _product(fdzb, scene, bins, tri_order)
     assert ref["rows_beyond_n"] == 0
+    # no pair written past its triangle's count (else the reference's own lists race)
+    assert ref["q2_events"] == 0
     bad = np.flatnonzero(sh.view(np.uint32) != ref["shadow"].view(np.uint32))
     assert bad.size == 0, f"{bad.size} of {scene.S} shadows differ, first {bad[:5].tolist()}"
     # masks: the reference's per-sample kernel ran for every binned sample;
@@ -132,11 +134,29 @@ def test_small_frame_at_32_bins_equals_reference(cuda_ok, fdzb, scenes, cull, or
 
 @pytest.mark.parametrize("bins", [32, 128])
 def test_odd_sizes_at_other_bins_equal_reference(cuda_ok, fdzb, scenes, bins):
+    """Odd views at 32^2 and 128^2 bins.  Where the reference's write kernel
+    puts a pair past its triangle's counted slots (its count and write kernels
+    test different AABBs, K/Step4_RasterizeTriangleToBin.inl:74-94 vs :177-193;
+    it happens when a bin's only sample defines the light plane's edge, which
+    fine grids over small views make likely), the reference's lists depend on
+    which of two racing writes lands; the product uses the counting test for
+    both and must then equal the oracle, bit for bit."""
+    import oracle
     _needs(bins)
+    raced = 0
     for W, H, T, n, seed in ((301, 77, 700, 5, 11), (200, 150, 1500, 32, 12), (640, 360, 20000, 16, 13)):
         scene = scenes.make_scene(W, H, T, n=n, bins=bins, seed=seed, cull=False, sigma=0.1)
         ref = ref_gpu.run(scene, fmad=False, masks=True, bins=bins)
-        _check(fdzb, scene, ref, bins=bins, tri_order=1)
+        if ref["q2_events"] == 0:
+            _check(fdzb, scene, ref, bins=bins, tri_order=1)
+            continue
+        raced += 1
+        sh, mk, st = _product(fdzb, scene, bins, tri_order=1)
+        o = oracle.frame(scene)
+        assert np.array_equal(sh.view(np.uint32), o.arrays["shadow"].astype(np.float32).view(np.uint32))
+        assert np.array_equal(mk, o.arrays["masks"].reshape(scene.S, -1).astype(np.uint32))
+        assert st["num_pairs"] == ref["num_pairs"]
+    assert raced < 3
 
 
 def test_hd_frame_at_128_bins_equals_reference_every_mask(cuda_ok, fdzb, scenes):
