@@ -113,6 +113,7 @@ size_t layout(fdzb::DeviceBuffers &b, char *base, int nf, long long S, long long
     b.binSampleEnd = (int32_t *)take(4 * ((size_t)NB + 1));
     b.binStat = (uint32_t *)take(32 * (size_t)NB);
     b.triRec = (float4 *)take(64 * Ts);
+    b.triPrj = (float4 *)take(32 * Ts);
     b.triCount = (int32_t *)take(4 * Ts);
     b.triScanStatus = (unsigned long long *)take(8 * ((Ts + fdzb::kTriTileHost - 1) / fdzb::kTriTileHost));
     b.tkeysA = (uint32_t *)take(4 * Ts);

@@ -119,6 +119,7 @@ struct DeviceBuffers {
     uint32_t *binStat;                          // [8 * totalBins] ordered encodings: maxz, Rx, Ry, Rz, Rw, 3 pad
     // triangles
     float4 *triRec;                             // [4 * totalTris]
+    float4 *triPrj;                             // [2 * totalTris] vertex projections (open-box test)
     int32_t *triCount;                          // [totalTris]
     unsigned long long *triScanStatus;          // [triTiles] epoch-tagged look-back words
     // pairs

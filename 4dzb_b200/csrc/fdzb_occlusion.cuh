@@ -41,6 +41,11 @@ namespace fdzb {
 #ifndef FDZB_OCC_UNION
 #define FDZB_OCC_UNION 0
 #endif
+// The per-lane open-box test runs only while the box holds at most this share
+// of the light grid (a larger box culls too little to pay for the test).
+#ifndef FDZB_OCC_BOX_FRAC
+#define FDZB_OCC_BOX_FRAC 0.5f
+#endif
 
 constexpr int kOccWarps = 4;
 constexpr int kOccThreads = kOccWarps * 32;
@@ -167,18 +172,15 @@ struct StagedPrj {
     float c;       // 1/w2
 };
 
-__device__ __forceinline__ void stage_projection(StagedPrj &dst, const float *M, const float4 *__restrict__ rec,
-                                                 int tri)
+// The vertices' projections, written by the triangle setup (k_tri_setup):
+// prjRec holds (u0, v0, 1/w0, u1), (v1, 1/w1, u2, v2) and the record's third
+// float4 carries 1/w2 in w.
+__device__ __forceinline__ void stage_projection(StagedPrj &dst, const float4 *__restrict__ prjRec,
+                                                 const float4 *__restrict__ rec, int tri)
 {
-    const float4 q0 = __ldg(rec + 4 * (size_t)tri);
-    const float4 q1 = __ldg(rec + 4 * (size_t)tri + 1);
-    const float4 q2 = __ldg(rec + 4 * (size_t)tri + 2);
-    const f3 p0 = light_project(M, mk3(q0.x, q0.y, q0.z));
-    const f3 p1 = light_project(M, mk3(q1.x, q1.y, q1.z));
-    const f3 p2 = light_project(M, mk3(q2.x, q2.y, q2.z));
-    dst.a = make_float4(p0.x, p0.y, __frcp_rn(p0.z), p1.x);
-    dst.b = make_float4(p1.y, __frcp_rn(p1.z), p2.x, p2.y);
-    dst.c = __frcp_rn(p2.z);
+    dst.a = __ldg(prjRec + 2 * (size_t)tri);
+    dst.b = __ldg(prjRec + 2 * (size_t)tri + 1);
+    dst.c = __ldg(rec + 4 * (size_t)tri + 2).w;
 }
 
 // A lane's open box as thresholds: (k_r0, k_r1, u_Q + k_r0/w_Q + mu, u_Q + k_r1/w_Q - mu)
@@ -219,7 +221,7 @@ __device__ __forceinline__ bool open_box(OpenBox &box, const LaneSample &s, cons
     const float mu = 1e-3f * L.RF[0] * iwq + 1e-5f, mv = 1e-3f * L.RF[1] * iwq + 1e-5f;
     box.u = make_float4(ku0, ku1, s.spx + ku0 * iwq + mu, s.spx + ku1 * iwq - mu);
     box.v = make_float4(kv0, kv1, s.spy + kv0 * iwq + mv, s.spy + kv1 * iwq - mv);
-    return !whole;
+    return !whole && (float)((r1 - r0 + 1) * (c1 - c0 + 1)) <= FDZB_OCC_BOX_FRAC * (float)(NR * NC);
 }
 
 // The union over the warp's active lanes of their boxes: a triangle that one
@@ -585,7 +587,8 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                 const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
                 const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
                 const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
-                const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
+                const float4 *__restrict__ rec, const float4 *__restrict__ prjRec, int totalTris, int totalBins,
+                int nframes)
 {
     __shared__ StagedTri s_tri[RowWord<R>::kWarps][kOccChunk];
     __shared__ R s_rows[RowWord<R>::kWarps][RowWord<R>::kBits][32];
@@ -676,7 +679,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                     tri = 0;
                 }
                 stage_triangle(tris[lane], rec, tri);
-                if (kRefine) stage_projection(prj[lane], fr.light.mat, rec, tri);
+                if (kRefine) stage_projection(prj[lane], prjRec, rec, tri);
             }
             if (kRefine && remaining > 0)
                 boxOn = open_box<R>(box, smp, fr.light, g.NR, g.NC, g.FR, g.FC, fullRows, rows, lane);
@@ -876,7 +879,8 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
                       const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
                       const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
                       const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
-                      const float4 *__restrict__ rec, int totalTris, int totalBins, int nframes)
+                      const float4 *__restrict__ rec, const float4 *__restrict__ /* prjRec */, int totalTris,
+                      int totalBins, int nframes)
 {
     __shared__ StagedTri s_tri[kOccWarps][kOccChunk];
     __shared__ uint32_t s_rows[kOccWarps][kMaxLightN32][32];

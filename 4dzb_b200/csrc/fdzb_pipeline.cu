@@ -28,6 +28,7 @@
 #include <mutex>
 #include <string>
 
+
 namespace fdzb {
 
 // Vertex v of a frame's model: xyz from the caller's buffer, through the frame's
@@ -239,13 +240,15 @@ __global__ void k_plan(const FrameDesc *__restrict__ frames, FrameState *states,
 
 // ---------------------------------------------------------------------------
 // k_tri_setup: grid (x, frame).  Record layout (4 x float4 = 64 B):
-//   q0 = (v0, minz) q1 = (v1, maxz) q2 = (v2, 0) q3 = (aabb min x,y, aabb max x,y)
+//   q0 = (v0, minz) q1 = (v1, maxz) q2 = (v2, 1/w2) q3 = (aabb min x,y, aabb max x,y)
+// and the vertices' projections for the occlusion stage's open-box test
+// (2 x float4): (u0, v0, 1/w0, u1), (v1, 1/w1, u2, v2).
 // Culled triangles keep the inverted AABB of the reference's triAABB buffer, so
 // the pair counter's skip test rejects them exactly as K/Step4_*.inl:41 does.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     k_tri_setup(const FrameDesc *__restrict__ frames, FrameState *states, float4 *__restrict__ rec,
-                int *err)
+                float4 *__restrict__ prj, int *err)
 {
     const FrameDesc &fr = frames[blockIdx.y];
     FrameState &st = states[blockIdx.y];
@@ -266,6 +269,7 @@ __global__ void __launch_bounds__(256)
                       i2 = fr.idx[3 * (size_t)t + 2];
             float mnx = kF32Max, mny = kF32Max, mnz = kF32Max;
             float mxx = -kF32Max, mxy = -kF32Max, mxz = -kF32Max;
+            float pu[3] = {0.f, 0.f, 0.f}, pv[3] = {0.f, 0.f, 0.f}, pw[3] = {0.f, 0.f, 0.f};
             f3 v0 = mk3(0.f, 0.f, 0.f), v1 = v0, v2 = v0;
             const bool okIdx = i0 >= 0 && i0 < fr.V && i1 >= 0 && i1 < fr.V && i2 >= 0 && i2 < fr.V;
             if (!okIdx) {
@@ -287,6 +291,9 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const f3 r = light_project(M, vv[k]);
+                        pu[k] = r.x;
+                        pv[k] = r.y;
+                        pw[k] = __frcp_rn(r.z);
                         mnx = fminf(mnx, r.x);
                         mny = fminf(mny, r.y);
                         mnz = fminf(mnz, r.z);
@@ -300,8 +307,11 @@ __global__ void __launch_bounds__(256)
             float4 *o = rec + 4 * (size_t)(fr.triBase + t);
             o[0] = make_float4(v0.x, v0.y, v0.z, mnz);
             o[1] = make_float4(v1.x, v1.y, v1.z, mxz);
-            o[2] = make_float4(v2.x, v2.y, v2.z, 0.0f);
+            o[2] = make_float4(v2.x, v2.y, v2.z, pw[2]);
             o[3] = make_float4(mnx, mny, mxx, mxy);
+            float4 *pp = prj + 2 * (size_t)(fr.triBase + t);
+            pp[0] = make_float4(pu[0], pv[0], pw[0], pu[1]);
+            pp[1] = make_float4(pv[1], pw[1], pu[2], pv[2]);
         }
         const unsigned b = __ballot_sync(kFullWarp, inLP);
         if (lane == 0 && b) atomicAdd(&st.nValidTris, __popc(b));
@@ -515,12 +525,9 @@ __global__ void k_tri_order(const FrameState *__restrict__ states, const int *__
 // Candidate bins of a triangle, swept by a warp 32 at a time in row-major
 // order; returns the number accepted and, with write != nullptr, writes the
 // accepted (bin, triangle) pairs from position `pos` on, in order.
-// With hist (the block's shared digit histograms of the pair sort), every
-// written key is also counted there, one histogram per radix pass.
 __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, const TriBins &c, int bb, int l2,
                                           int lane, uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals,
-                                          unsigned long long pos, int capacity, int g, bool write,
-                                          uint32_t *hist = nullptr, int histPasses = 0)
+                                          unsigned long long pos, int capacity, int g, bool write)
 {
     const int w = c.cex - c.cbx, h = c.cey - c.cby;
     if (w <= 0 || h <= 0) return 0;
@@ -538,22 +545,11 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
             ok = bin_accepts(binStat, gb, c);
         }
         const unsigned m = __ballot_sync(kFullWarp, ok);
-        bool stored = false;
         if (write && ok) {
             const unsigned long long p = pos + (unsigned long long)total + (unsigned)__popc(m & lanemask_lt());
             if (p < (unsigned long long)capacity) {
                 pkeys[p] = (uint32_t)gb;
                 pvals[p] = (uint32_t)g;
-                stored = true;
-            }
-        }
-        if (hist) {
-            // digits of the stored keys; lanes with equal digits add once
-            const unsigned sm_ = __ballot_sync(kFullWarp, stored);
-            for (int d = 0; d < histPasses; ++d) {
-                const uint32_t dig = ((uint32_t)gb >> (8 * d)) & 255u;
-                const unsigned peers = __match_any_sync(kFullWarp, stored ? dig : 256u + (unsigned)lane) & sm_;
-                if (stored && (peers & lanemask_lt()) == 0) atomicAdd(&hist[d * 256 + dig], (uint32_t)__popc(peers));
             }
         }
         total += __popc(m);
@@ -580,12 +576,9 @@ __global__ void __launch_bounds__(kTriThreads)
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
                 int32_t *__restrict__ triCount, unsigned long long *scanStatus, const uint32_t *epochWord,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
-                const uint32_t *__restrict__ order, Counters *ctr, uint32_t *pairHist, int histPasses)
+                const uint32_t *__restrict__ order, Counters *ctr)
 {
     constexpr int WARPS = kTriThreads / 32;
-    // digit histograms of the written pair keys for the pair sort's passes
-    // (its separate histogram pass over the keys is then not needed)
-    __shared__ uint32_t s_hist[2 * 256];
     __shared__ int s_tile;
     __shared__ int s_cnt[kTriThreads];
     __shared__ unsigned long long s_wsum[WARPS];
@@ -593,9 +586,6 @@ __global__ void __launch_bounds__(kTriThreads)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (totalTris + kTriThreads - 1) / kTriThreads;
     const uint32_t epoch = *epochWord;
-    if (histPasses > 2) histPasses = 2;
-    uint32_t *hist = (pairHist && histPasses > 0) ? s_hist : nullptr;
-    for (int i = tid; i < 2 * 256; i += kTriThreads) s_hist[i] = 0u;
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&ctr->triTileCounter, 1);
@@ -693,13 +683,8 @@ __global__ void __launch_bounds__(kTriThreads)
             const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
             if (!c.any) continue;
             sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals,
-                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true, hist, histPasses);
+                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true);
         }
-    }
-    if (hist) {
-        __syncthreads();
-        for (int i = tid; i < histPasses * 256; i += kTriThreads)
-            if (s_hist[i]) atomicAdd(&pairHist[i], s_hist[i]);
     }
 }
 
@@ -765,12 +750,11 @@ static int grid_for(long long n, int threads, int cap)
 // 16*launch + 4*slot + p.
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
-                     cudaStream_t s, bool histDone = false)
+                     cudaStream_t s)
 {
     uint32_t *hist = b.sortHist + slot * 4 * kRadix;
-    if (!histDone)
-        k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
-                                                                                  cap, passes, hist);
+    k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
+                                                                              cap, passes, hist);
     uint32_t *ki = kA, *vi = vA, *ko = kB, *vo = vB;
     const long long tiles = ((long long)cap + kSortTile - 1) / kSortTile;
     const int passGrid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
@@ -789,9 +773,6 @@ static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *v
     }
 }
 
-#ifndef FDZB_PAIR_HIST_INLINE
-#define FDZB_PAIR_HIST_INLINE 1
-#endif
 
 static int g_smCount = 0;
 
@@ -823,7 +804,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     }
     k_plan<<<(nf + 63) / 64, 64, 0, s>>>(b.frames, b.states, nf);
     k_tri_setup<<<dim3(grid_for(maxT, 256, sm * 8), nf), 256, 0, s>>>(b.frames, b.states, b.triRec,
-                                                                      &b.counters->errorFlags);
+                                                                      b.triPrj, &b.counters->errorFlags);
     k_sample_keys<<<dim3(grid_for(maxS, 256, sm * 8), nf), 256, 0, s>>>(
         b.frames, b.states, b.keysA, b.valsA, b.binStat, b.totalBins);
     nl += 5;
@@ -841,11 +822,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
         (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
     nl += 2 + b.samplePasses;
-    // (a) triangle/bin pairs, in the coverage order when one is asked for; the
-    // pair sort's digit histograms are built as the pairs are written when its
-    // keys (global bins) take at most two 8-bit passes (up to 65,536 bins in
-    // the launch); beyond that the sort's own histogram pass runs
-    const bool pairHistInline = FDZB_PAIR_HIST_INLINE && b.pairPasses <= 2;
+    // (a) triangle/bin pairs, in the coverage order when one is asked for
     if (ev) cudaEventRecord(ev[STAGE_TRI_PAIRS], s);
     const uint32_t *order = nullptr;
     if (b.depthBits > 0 && b.totalTris > 0) {
@@ -864,9 +841,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 order, b.counters, pairHistInline ? b.sortHist + 4 * kRadix
-                                                                                   : nullptr,
-                                                 pairHistInline ? b.pairPasses : 0);
+                                                 order, b.counters);
         nl += 1;
     }
     if (b.dbgPKeys) {
@@ -876,13 +851,13 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     // (b) pair sort and segments
     if (ev) cudaEventRecord(ev[STAGE_PAIR_SORT], s);
     run_sort(b, 1, b.pkeysA, b.pvalsA, b.pkeysB, b.pvalsB, &b.counters->pairCount, 0, b.pairCapacity,
-             b.pairPasses, sm, s, pairHistInline);
+             b.pairPasses, sm, s);
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
     uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
         pk, &b.counters->pairCount, 0, b.pairCapacity, 0, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
-    nl += (pairHistInline ? 1 : 2) + b.pairPasses;
+    nl += 2 + b.pairPasses;
     // (c) + (d) occlusion and shading
     if (ev) cudaEventRecord(ev[STAGE_OCCLUSION], s);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(
@@ -895,7 +870,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     const int g32 = sm * FDZB_OCC_MINBLOCKS, g64 = sm * W64::kMinBlocks, t64 = W64::kWarps * 32;
 #define FDZB_OCC_ARGS                                                                                        \
     b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd, b.binTriStart, \
-        b.binTriEnd, pv, b.triRec, b.totalTris, b.totalBins, nf
+        b.binTriEnd, pv, b.triRec, b.triPrj, b.totalTris, b.totalBins, nf
     if (b.wide) {
         if (b.rayCast) k_occlusion<1, u64, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
         else if (b.depthPlane) k_occlusion<0, u64, 1><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);

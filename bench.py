@@ -952,8 +952,11 @@ def main():
                      "peak": alu_peak / 1e9, "unit": "Gop/s", "frac": achieved / alu_peak,
                      "traffic": profile_traffic("k_occlusion", args.config),
                      "ops_per_launch": ops, "launch_ms": occ_ms,
-                     "note": "algorithmic FP32/INT32 ops of the reference per-pair code / measured FP32 "
-                             "issue rate (lane ops/s) of this GPU"},
+                     "pairs_skipped_by_open_box": int(ctx.export("work_counters", 7)[6]),
+                     "note": "algorithmic FP32/INT32 ops of the reference per-pair code the kernel executes "
+                             "/ measured FP32 issue rate (lane ops/s) of this GPU; pairs the open-box cull "
+                             "proves useless (they pass the reference's pre-cull but cannot set an unset bit) "
+                             "are skipped and not counted"},
         "e2e": {"value": e2e_value, "unit": "frames/s",
                 "h2d_bytes_per_step": int(scene.pos.nbytes + scene.nrm.nbytes),
                 "d2h_bytes_per_step": int(scene.S * 4),
