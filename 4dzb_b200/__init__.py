@@ -66,7 +66,11 @@ EXPORTED = [
     "fdzb_serve_get_stats", "fdzb_serve_reset_stats", "fdzb_serve_last_worker_error",
     "fdzb_ctx_set_launch_epoch", "fdzb_ctx_get_launch_epoch",
     "fdzb_ctx_set_occlusion_shape", "fdzb_batch_frame_shape", "fdzb_batch_set_occlusion_shape",
+    "fdzb_ctx_set_open_box", "fdzb_batch_set_open_box",
 ]
+
+# Open-box cull modes (include/fdzb.h).
+OPEN_BOX_OFF, OPEN_BOX_ON, OPEN_BOX_AUTO = 0, 1, 2
 
 # Occlusion shapes (staged triangles per chunk, samples per warp item).
 OCC_CHUNKS = (8, 16, 32)
@@ -271,6 +275,7 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_set_occlusion_shape": ([vp, i32, i32], i32),
         "fdzb_batch_frame_shape": ([vp, i32, vp, vp, vp], i32),
         "fdzb_batch_set_occlusion_shape": ([vp, i32, i32], i32),
+        "fdzb_ctx_set_open_box": ([vp, i32], i32), "fdzb_batch_set_open_box": ([vp, i32], i32),
         "fdzb_ctx_set_pair_capacity_limit": ([vp, ctypes.c_int64], i32),
         "fdzb_ctx_set_model_transform": ([vp, P(ctypes.c_float)], i32),
         "fdzb_ctx_set_shadow_method": ([vp, i32], i32),
@@ -408,6 +413,10 @@ class Context:
         """Triangles staged per chunk (OCC_CHUNKS) and samples per warp item
         (OCC_ITEMS); results are identical for every shape."""
         _check(self._lib.fdzb_ctx_set_occlusion_shape(self._h, int(chunk), int(item)))
+
+    def set_open_box(self, mode: int) -> None:
+        """OPEN_BOX_OFF, OPEN_BOX_ON or OPEN_BOX_AUTO (default); results are identical."""
+        _check(self._lib.fdzb_ctx_set_open_box(self._h, int(mode)))
 
     def set_occlusion_schedule(self, schedule: int) -> None:
         """OCC_LANE_PER_SAMPLE (default) or OCC_LANE_PER_PAIR; results are identical."""
@@ -719,6 +728,10 @@ class Batch:
     def set_occlusion_shape(self, chunk: int = 0, item: int = 0) -> None:
         """One occlusion shape for every frame of later launches (0, 0: tuned or default)."""
         _check(self._lib.fdzb_batch_set_occlusion_shape(self._h, int(chunk), int(item)))
+
+    def set_open_box(self, mode: int) -> None:
+        """OPEN_BOX_OFF, OPEN_BOX_ON or OPEN_BOX_AUTO (default) for later launches."""
+        _check(self._lib.fdzb_batch_set_open_box(self._h, int(mode)))
 
     def frame_bins(self, i: int) -> int:
         rc = self._lib.fdzb_batch_frame_bins(self._h, i)

@@ -351,6 +351,17 @@ int engine_enqueue(Engine &e)
     b.depthPlane = e.depthPlane;
     b.rayCast = e.rayCast;
     b.occVariant = (e.occVariant == 1 && !wide && square && !e.depthPlane) ? 1 : 0;
+    {
+        const auto shape = std::make_tuple(nf, S, T, NB);
+        if (shape != e.openBoxShape) {
+            e.openBoxShape = shape;
+            e.openBoxAuto = true;     // a new shape: probe the cull again
+        }
+        const bool want = e.openBoxMode == FDZB_OPEN_BOX_ON ||
+                          (e.openBoxMode == FDZB_OPEN_BOX_AUTO && e.openBoxAuto);
+        b.openBox = (want && !e.rayCast && b.occVariant == 0) ? 1 : 0;
+        e.lastOpenBox = b.openBox != 0;
+    }
     // Triangle lists: the pairs are sorted by bin only (stable, so a bin lists
     // its triangles in the order the pairs were emitted,
     // K/Step4_RasterizeTriangleToBin.inl:220-223).  Reference order emits them by
@@ -417,7 +428,7 @@ int engine_enqueue(Engine &e)
         k.maxV = maxV;
         k.arena = e.arena;
         k.hFrames = e.hFrames;
-        k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane;
+        k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane + 128 * b.openBox;
         k.stream = e.stream;
         FDZB_CUDA(refresh_lookback(e));
         if (!e.graph || !(k == e.graphKey)) {
@@ -620,6 +631,11 @@ int engine_sync(Engine &e)
     FDZB_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
     e.lastMs = ms;
     e.passes = 1;
+    if (e.lastOpenBox && e.openBoxMode == FDZB_OPEN_BOX_AUTO) {
+        const fdzb::Counters &k = *e.hCounters;
+        const double rate = k.pairsExamined ? (double)k.boxSkips / (double)k.pairsExamined : 0.0;
+        if (rate < kOpenBoxKeep) e.openBoxAuto = false;
+    }
     return FDZB_OK;
 }
 
@@ -1087,6 +1103,28 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second)
 {
     if (!lane_ops_per_second) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
     FDZB_CUDA(fdzb::measure_alu_rate(lane_ops_per_second));
+    return FDZB_OK;
+}
+
+int fdzb_ctx_set_open_box(fdzb_ctx *c, int mode)
+{
+    if (int rc = ctx_check(c)) return rc;
+    if (mode != FDZB_OPEN_BOX_OFF && mode != FDZB_OPEN_BOX_ON && mode != FDZB_OPEN_BOX_AUTO)
+        return fail(FDZB_ERR_INVALID_ARG, "open-box mode: FDZB_OPEN_BOX_OFF, _ON or _AUTO");
+    if (int rc = ctx_sync(c)) return rc;
+    c->eng.openBoxMode = mode;
+    c->eng.openBoxAuto = true;
+    return FDZB_OK;
+}
+
+int fdzb_batch_set_open_box(fdzb_batch *b, int mode)
+{
+    if (int rc = batch_check(b)) return rc;
+    if (mode != FDZB_OPEN_BOX_OFF && mode != FDZB_OPEN_BOX_ON && mode != FDZB_OPEN_BOX_AUTO)
+        return fail(FDZB_ERR_INVALID_ARG, "open-box mode: FDZB_OPEN_BOX_OFF, _ON or _AUTO");
+    if (int rc = engine_sync(b->eng)) return rc;
+    b->eng.openBoxMode = mode;
+    b->eng.openBoxAuto = true;
     return FDZB_OK;
 }
 

@@ -106,7 +106,17 @@ struct Engine {
     // wraps round to the tag of a stale word.
     uint32_t epochCount = 0;
     std::tuple<const void *, size_t, const void *, int, const void *> statusLayout{};
+    // Open-box cull (FDZB_OPEN_BOX_*): in auto mode the first launch of a
+    // launch shape (frames, samples, triangles, bins) runs the cull's kernel
+    // and counts the staged pairs it skips; the shape keeps the cull only if
+    // it skipped at least kOpenBoxKeep of them.
+    int openBoxMode = FDZB_OPEN_BOX_AUTO;
+    bool openBoxAuto = true;
+    std::tuple<int, long long, long long, long long> openBoxShape{-1, 0, 0, 0};
+    bool lastOpenBox = false;
 };
+
+constexpr double kOpenBoxKeep = 0.25;
 
 // Launches between two clearings of the look-back words: the sort tags are
 // epoch * 16 + (4 x sort slot + pass) in 32 bits, so the epoch stays below 2^28.

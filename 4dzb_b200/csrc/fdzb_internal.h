@@ -93,10 +93,11 @@ struct Counters {
     int sortTileCounter[12]; // one ticket per radix pass (4 sample, 4 pair, 4 triangle)
     unsigned long long rowsEvaluated;   // light rows evaluated by pair tests
     unsigned long long partialMasks;    // row masks that needed the ceil(-D/B) threshold
-    unsigned long long pairsExamined;   // sample/triangle pairs reaching the AABB pre-cull
+    unsigned long long pairsExamined;   // sample/triangle pairs reaching the AABB pre-cull (the
+                                        // open-box kernel: staged triangles its lanes take up)
     unsigned long long chunks;          // staged triangle chunks (warp-level)
     unsigned long long rounds;          // compute rounds of 32 pair slots (k_occlusion_pairs)
-    unsigned long long boxSkips;        // pairs past the pre-cull skipped by the open-box cull
+    unsigned long long boxSkips;        // pairs the open-box cull skipped (warp union or the lane's box)
 };
 
 // Stage boundaries recorded when per-stage timing is on.
@@ -145,6 +146,7 @@ struct DeviceBuffers {
     int wide;                                   // 1: some frame's light grid exceeds 32 rows or
                                                 // columns: 64-bit row words
     int depthPlane;                             // 1: the frames test each triangle's own plane
+    int openBox;                                // 1: the occlusion kernel with the open-box cull
     uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
                                                 // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays

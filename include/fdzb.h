@@ -386,6 +386,21 @@ int fdzb_ctx_set_graph(fdzb_ctx *ctx, int enable);
  * batch and server autotuners pick it per size class. */
 int fdzb_ctx_set_occlusion_shape(fdzb_ctx *ctx, int chunk, int item);
 
+/* Open-box cull, no counterpart in the reference: once some of a sample's
+ * light rows or columns are full, a pair whose triangle cannot reach the box
+ * of its still-unset light samples (a test on the triangle's projected
+ * vertices, with a margin far above FP32 rounding) is skipped; masks and
+ * shadows are identical (the mask is the OR over the bin's triangles).  It
+ * runs in its own instantiation of the occlusion kernel, which is faster where
+ * samples end in umbra and slower where they stay in penumbra.  AUTO (the
+ * default): the first launch of each launch shape (frames, samples, triangles,
+ * bins) runs it and counts the staged pairs it skips; the shape keeps it only
+ * if that is at least a quarter of them.  Edge-function masks only. */
+#define FDZB_OPEN_BOX_OFF 0
+#define FDZB_OPEN_BOX_ON 1
+#define FDZB_OPEN_BOX_AUTO 2
+int fdzb_ctx_set_open_box(fdzb_ctx *ctx, int mode);
+
 /* Testing aids, no counterpart in the reference.  The sorts' decoupled
  * look-back tags its status words with the context's launch number (a device
  * word advanced by every launch; FS/api.cpp:402-582 has no look-back: Thrust's
@@ -469,6 +484,8 @@ int fdzb_batch_frame_shape(fdzb_batch *batch, int frame, int *bins, int *chunk, 
 /* An occlusion shape for every frame of later launches (0, 0: each frame's
  * tuned or default shape). */
 int fdzb_batch_set_occlusion_shape(fdzb_batch *batch, int chunk, int item);
+/* Open-box cull of the batch's launches (see fdzb_ctx_set_open_box). */
+int fdzb_batch_set_open_box(fdzb_batch *batch, int mode);
 /* Autotuner: for every size class (ceil(log2 samples), ceil(log2 triangles), N)
  * of the frames with bins == 0 not tuned yet, times three bin grids around
  * ~128 samples per bin, then at the best grid a staging chunk of 16 triangles,

@@ -158,3 +158,9 @@ def test_occlusion_shape_arguments_are_checked(fdzb):
     lib = fdzb.load()
     assert lib.fdzb_ctx_set_occlusion_shape(None, 32, 32) == -3        # no context
     assert lib.fdzb_batch_set_occlusion_shape(None, 16, 64) == -3
+
+
+def test_open_box_mode_arguments_are_checked(fdzb):
+    lib = fdzb.load()
+    assert lib.fdzb_ctx_set_open_box(None, fdzb.OPEN_BOX_AUTO) == -3
+    assert lib.fdzb_batch_set_open_box(None, fdzb.OPEN_BOX_ON) == -3

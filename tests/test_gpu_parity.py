@@ -106,3 +106,34 @@ def test_triangle_passes_match_oracle(cuda_ok, fdzb, scenes, masks, schedule):
     ctx.launch()
     assert np.array_equal(t["shadow"].cpu().numpy(), sh)
     ctx.close()
+
+
+@pytest.mark.parametrize("scene_args", [
+    ("small", None),
+    ("make", (640, 360, 20000, 16, 128, 31, 0.1)),     # penumbra-rich: the auto probe turns the cull off
+    ("make", (480, 270, 30000, 8, 64, 32, 0.1)),
+])
+def test_open_box_modes_give_the_oracle_masks(cuda_ok, fdzb, scenes, scene_args):
+    """The open-box cull skips only pairs that cannot set an unset bit: with it
+    forced off, forced on and in auto mode (whose first launch probes it and
+    may switch it off for the next), masks and shadows equal the oracle's."""
+    kind, a = scene_args
+    if kind == "small":
+        s = scenes.preset("small")
+    else:
+        W, H, T, n, bins, seed, sigma = a
+        s = scenes.make_scene(W, H, T, n=n, bins=bins, seed=seed, sigma=sigma)
+    orc = oracle.frame(s)
+    for mode in (fdzb.OPEN_BOX_OFF, fdzb.OPEN_BOX_ON, fdzb.OPEN_BOX_AUTO):
+        ctx, t = fdzb.context_for_scene(s, masks=True, tri_order=1)
+        ctx.set_open_box(mode)
+        for _ in range(2):
+            t["masks"].zero_()
+            t["shadow"].fill_(-1.0)
+            ctx.launch()
+            errs = parity.compare(s, gpu=parity.collect(ctx, t, s, tri_order=1, intermediates=False), orc=orc)
+            assert not errs, (mode, errs)
+        wc = ctx.export("work_counters", 7)
+        if mode == fdzb.OPEN_BOX_OFF:
+            assert wc[6] == 0           # no pair skipped by the cull
+        ctx.close()
