@@ -352,13 +352,10 @@ int engine_enqueue(Engine &e)
     b.rayCast = e.rayCast;
     b.occVariant = (e.occVariant == 1 && !wide && square && !e.depthPlane) ? 1 : 0;
     {
-        const auto shape = std::make_tuple(nf, S, T, NB);
-        if (shape != e.openBoxShape) {
-            e.openBoxShape = shape;
-            e.openBoxAuto = true;     // a new shape: probe the cull again
-        }
+        e.lastShape = std::make_tuple(nf, S, T, NB);
+        const auto known = e.openBoxKeep.find(e.lastShape);   // a shape not seen yet: probe the cull
         const bool want = e.openBoxMode == FDZB_OPEN_BOX_ON ||
-                          (e.openBoxMode == FDZB_OPEN_BOX_AUTO && e.openBoxAuto);
+                          (e.openBoxMode == FDZB_OPEN_BOX_AUTO && (known == e.openBoxKeep.end() || known->second));
         b.openBox = (want && !e.rayCast && b.occVariant == 0) ? 1 : 0;
         e.lastOpenBox = b.openBox != 0;
     }
@@ -631,10 +628,10 @@ int engine_sync(Engine &e)
     FDZB_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
     e.lastMs = ms;
     e.passes = 1;
-    if (e.lastOpenBox && e.openBoxMode == FDZB_OPEN_BOX_AUTO) {
+    if (e.lastOpenBox && e.openBoxMode == FDZB_OPEN_BOX_AUTO && !e.openBoxKeep.count(e.lastShape)) {
         const fdzb::Counters &k = *e.hCounters;
         const double rate = k.pairsExamined ? (double)k.boxSkips / (double)k.pairsExamined : 0.0;
-        if (rate < kOpenBoxKeep) e.openBoxAuto = false;
+        e.openBoxKeep[e.lastShape] = rate >= kOpenBoxKeep;
     }
     return FDZB_OK;
 }
@@ -1113,7 +1110,7 @@ int fdzb_ctx_set_open_box(fdzb_ctx *c, int mode)
         return fail(FDZB_ERR_INVALID_ARG, "open-box mode: FDZB_OPEN_BOX_OFF, _ON or _AUTO");
     if (int rc = ctx_sync(c)) return rc;
     c->eng.openBoxMode = mode;
-    c->eng.openBoxAuto = true;
+    c->eng.openBoxKeep.clear();
     return FDZB_OK;
 }
 
@@ -1124,7 +1121,7 @@ int fdzb_batch_set_open_box(fdzb_batch *b, int mode)
         return fail(FDZB_ERR_INVALID_ARG, "open-box mode: FDZB_OPEN_BOX_OFF, _ON or _AUTO");
     if (int rc = engine_sync(b->eng)) return rc;
     b->eng.openBoxMode = mode;
-    b->eng.openBoxAuto = true;
+    b->eng.openBoxKeep.clear();
     return FDZB_OK;
 }
 

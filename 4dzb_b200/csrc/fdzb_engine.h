@@ -109,10 +109,12 @@ struct Engine {
     // Open-box cull (FDZB_OPEN_BOX_*): in auto mode the first launch of a
     // launch shape (frames, samples, triangles, bins) runs the cull's kernel
     // and counts the staged pairs it skips; the shape keeps the cull only if
-    // it skipped at least kOpenBoxKeep of them.
+    // it skipped at least kOpenBoxKeep of them.  Decisions are kept per shape
+    // (an engine that alternates between shapes probes each once).
+    using BoxShape = std::tuple<int, long long, long long, long long>;
     int openBoxMode = FDZB_OPEN_BOX_AUTO;
-    bool openBoxAuto = true;
-    std::tuple<int, long long, long long, long long> openBoxShape{-1, 0, 0, 0};
+    std::map<BoxShape, bool> openBoxKeep;
+    BoxShape lastShape{-1, 0, 0, 0};
     bool lastOpenBox = false;
 };
 

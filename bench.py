@@ -909,6 +909,7 @@ def main():
            + pstats[-1]["partial_masks"] * OPS_PER_PARTIAL)
     alu_peak = fdzb.measure_alu_rate()
     achieved = ops / (occ_ms * 1e-3)
+    work = [int(x) for x in ctx.export("work_counters", 7)]
 
     # end to end through the public API with host buffers: every frame uploads
     # its G-buffer (positions + normals) from pinned host memory and reads its
@@ -952,7 +953,7 @@ def main():
                      "peak": alu_peak / 1e9, "unit": "Gop/s", "frac": achieved / alu_peak,
                      "traffic": profile_traffic("k_occlusion", args.config),
                      "ops_per_launch": ops, "launch_ms": occ_ms,
-                     "pairs_skipped_by_open_box": int(ctx.export("work_counters", 7)[6]),
+                     "open_box": {"staged_pairs": work[3], "skipped": work[6]},
                      "note": "algorithmic FP32/INT32 ops of the reference per-pair code the kernel executes "
                              "/ measured FP32 issue rate (lane ops/s) of this GPU; pairs the open-box cull "
                              "proves useless (they pass the reference's pre-cull but cannot set an unset bit) "
