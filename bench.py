@@ -260,7 +260,8 @@ def _ref_gpu_timing(ref_gpu, scene, args, fmad: bool, bins: int) -> dict:
     for j, name in enumerate(ref_gpu.STAGES):
         col = [float(v) for v in st[:, j] if v >= 0]
         if col:
-            stages[name] = {"median_ms": statistics.median(col), "mean_ms": statistics.mean(col)}
+            stages[name] = {"median_ms": statistics.median(col), "mean_ms": statistics.mean(col),
+                            "max_ms": max(col)}
     med = statistics.median(t)
     return {"value": 1e3 / med, "unit": "frames/s", "median_ms": med, "mean_ms": statistics.mean(t),
             "min_ms": min(t), "max_ms": max(t), "frames": len(t), "bins": bins,
@@ -910,6 +911,14 @@ def main():
     alu_peak = fdzb.measure_alu_rate()
     achieved = ops / (occ_ms * 1e-3)
     work = [int(x) for x in ctx.export("work_counters", 7)]
+    # the same frame's work without the open-box cull (one untimed launch of the
+    # other kernel instantiation): the reference-equivalent operation count
+    ctx.set_open_box(fdzb.OPEN_BOX_OFF)
+    ctx.launch()
+    so = ctx.stats()
+    ops_off = (so["pair_tests"] * OPS_PER_PAIR + so["rows_evaluated"] * OPS_PER_ROW
+               + so["partial_masks"] * OPS_PER_PARTIAL)
+    ctx.set_open_box(fdzb.OPEN_BOX_AUTO)
 
     # end to end through the public API with host buffers: every frame uploads
     # its G-buffer (positions + normals) from pinned host memory and reads its
@@ -954,6 +963,11 @@ def main():
                      "traffic": profile_traffic("k_occlusion", args.config),
                      "ops_per_launch": ops, "launch_ms": occ_ms,
                      "open_box": {"staged_pairs": work[3], "skipped": work[6]},
+                     "equivalent": {"ops_per_launch": ops_off, "frac": ops_off / (occ_ms * 1e-3) / alu_peak,
+                                    "pair_tests": so["pair_tests"],
+                                    "note": "the reference per-pair operations of the same frame without the "
+                                            "open-box cull (one untimed launch of the other kernel), over this "
+                                            "kernel's time: the rate of reference-equivalent work"},
                      "note": "algorithmic FP32/INT32 ops of the reference per-pair code the kernel executes "
                              "/ measured FP32 issue rate (lane ops/s) of this GPU; pairs the open-box cull "
                              "proves useless (they pass the reference's pre-cull but cannot set an unset bit) "
