@@ -136,55 +136,6 @@ __device__ __forceinline__ void st_volatile_u64(unsigned long long *p, unsigned 
     asm volatile("st.volatile.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Look-back status words: [63:32] tag, [31:30] flag (1 aggregate, 2 inclusive
-// prefix, 0 not published under this tag), [29:0] count.
-constexpr unsigned long long kLbAgg = 1ull << 30;
-constexpr unsigned long long kLbPrefix = 2ull << 30;
-constexpr unsigned long long kLbMask = (1ull << 30) - 1ull;
-
-// Warp-wide decoupled look-back: the calling warp (all 32 lanes) sums the
-// counts of the tiles before `tile` back to the nearest inclusive prefix,
-// reading 32 predecessors' status words (status[i * stride]) per round, so a
-// chain of n aggregates costs n / 32 dependent loads instead of n.  Every lane
-// returns the exclusive sum.  A round that finds the next word unpublished
-// retries it; after kSpinLimit such rounds it gives up and sets *timedOut.
-__device__ __forceinline__ unsigned long long warp_lookback(const unsigned long long *status, size_t stride,
-                                                            int tile, uint32_t tag, bool *timedOut)
-{
-    const int lane = threadIdx.x & 31;
-    unsigned long long excl = 0;
-    int t = tile - 1;
-    unsigned spins = 0;
-    while (t >= 0) {
-        const int idx = t - lane;
-        unsigned long long s = 0;
-        unsigned flag = 2u;                 // before tile 0: a prefix of 0
-        if (idx >= 0) {
-            s = ld_volatile_u64(status + (size_t)idx * stride);
-            flag = ((uint32_t)(s >> 32) == tag) ? (unsigned)((s >> 30) & 3u) : 0u;
-        }
-        const unsigned unpub = __ballot_sync(kFullWarp, flag == 0u);
-        const unsigned pre = __ballot_sync(kFullWarp, flag == 2u);
-        const int firstPre = pre ? __ffs(pre) - 1 : 32;
-        const int firstUnp = unpub ? __ffs(unpub) - 1 : 32;
-        // consume the published words before the first unpublished one, up to
-        // and including the nearest prefix
-        const bool done = firstPre < firstUnp;
-        const int n = done ? firstPre + 1 : firstUnp;
-        unsigned long long v = (lane < n && idx >= 0) ? (s & kLbMask) : 0ull;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullWarp, v, o);
-        excl += v;
-        if (done) break;
-        if (n == 0 && ++spins > kSpinLimit) {
-            *timedOut = true;
-            break;
-        }
-        t -= n;
-    }
-    return excl;
-}
-
 // Index of the frame owning global index g, given ascending bases[0..n).
 __device__ __forceinline__ int frame_of(const int *bases, int n, int g)
 {

@@ -632,31 +632,39 @@ __global__ void __launch_bounds__(kTriThreads)
         const unsigned long long mine_excl = wbase + x - (unsigned long long)cnt;
         __syncthreads();
         s_cnt[tid] = (int)min(mine_excl, (unsigned long long)0x7fffffff);   // now: exclusive offset in the tile
-        if (warp == 0) {
-            // warp 0: publish the tile's aggregate, look back 32 tiles a round
+        if (tid == 0) {
             unsigned long long excl = 0;
             unsigned long long *my = scanStatus + tile;
             const unsigned long long ep = (unsigned long long)epoch << 32;
             const unsigned long long tot = total > kScanMask ? kScanMask : total;
             if (tile == 0) {
-                if (lane == 0) st_volatile_u64(my, ep | kScanPrefix | tot);
+                st_volatile_u64(my, ep | kScanPrefix | tot);
             } else {
-                if (lane == 0) st_volatile_u64(my, ep | kScanAgg | tot);
-                bool timedOut = false;
-                excl = warp_lookback(scanStatus, 1, tile, epoch, &timedOut);
-                if (lane == 0) {
-                    if (timedOut) atomicOr(&ctr->errorFlags, (int)ERR_LOOKBACK_TIMEOUT);
-                    const unsigned long long inc = excl + total > kScanMask ? kScanMask : excl + total;
-                    st_volatile_u64(my, ep | kScanPrefix | inc);
+                st_volatile_u64(my, ep | kScanAgg | tot);
+                int t = tile - 1;
+                unsigned spins = 0;
+                while (t >= 0) {
+                    const unsigned long long s = ld_volatile_u64(scanStatus + t);
+                    const unsigned long long flag = ((s >> 32) == epoch) ? (s & 0xC0000000ull) : 0ull;
+                    if (flag == 0) {
+                        if (++spins > kSpinLimit) {
+                            atomicOr(&ctr->errorFlags, (int)ERR_LOOKBACK_TIMEOUT);
+                            break;
+                        }
+                        continue;
+                    }
+                    excl += s & kScanMask;
+                    if (flag == kScanPrefix) break;
+                    --t;
                 }
+                const unsigned long long inc = excl + total > kScanMask ? kScanMask : excl + total;
+                st_volatile_u64(my, ep | kScanPrefix | inc);
             }
-            if (lane == 0) {
-                s_excl = excl;
-                if (tile == ntiles - 1) {
-                    const unsigned long long all = excl + total;
-                    ctr->pairCount = (int)(all > 0x7fffffffull ? 0x7fffffffull : all);
-                    if (all > (unsigned long long)capacity) ctr->pairOverflow = 1;
-                }
+            s_excl = excl;
+            if (tile == ntiles - 1) {
+                const unsigned long long all = excl + total;
+                ctr->pairCount = (int)(all > 0x7fffffffull ? 0x7fffffffull : all);
+                if (all > (unsigned long long)capacity) ctr->pairOverflow = 1;
             }
         }
         __syncthreads();

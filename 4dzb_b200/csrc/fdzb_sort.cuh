@@ -21,9 +21,6 @@ namespace fdzb {
 #ifndef FDZB_SORT_MINBLOCKS
 #define FDZB_SORT_MINBLOCKS 3
 #endif
-#ifndef FDZB_SORT_LOOKAHEAD
-#define FDZB_SORT_LOOKAHEAD 4
-#endif
 constexpr int kSortThreads = 256;                      // = kRadix: thread d handles digit d
 constexpr int kSortItems = FDZB_SORT_ITEMS;
 constexpr int kSortTile = kSortThreads * kSortItems;   // keys per tile
@@ -161,32 +158,21 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
             st_volatile_u64(my, ep | kStatPrefix | run);
         } else {
             st_volatile_u64(my, ep | kStatAgg | run);
-            // look back kLookAhead predecessors per round (independent loads)
-            constexpr int kLookAhead = FDZB_SORT_LOOKAHEAD;
             int t = tile - 1;
             unsigned spins = 0;
             while (t >= 0) {
-                unsigned long long s[kLookAhead];
-#pragma unroll
-                for (int j = 0; j < kLookAhead; ++j)
-                    s[j] = t - j >= 0 ? ld_volatile_u64(status + (size_t)(t - j) * kRadix + tid) : 0ull;
-                int used = 0;
-                bool done = false;
-#pragma unroll
-                for (int j = 0; j < kLookAhead; ++j) {
-                    if (done || used < j) break;                  // stopped at an unpublished word
-                    const unsigned long long flag = ((s[j] >> 32) == epoch) ? (s[j] & 0xC0000000ull) : 0ull;
-                    if (flag == 0) break;
-                    excl += (uint32_t)(s[j] & kStatMask);
-                    ++used;
-                    if (flag == kStatPrefix || t - j == 0) done = true;
+                const unsigned long long s = ld_volatile_u64(status + (size_t)t * kRadix + tid);
+                const unsigned long long flag = ((s >> 32) == epoch) ? (s & 0xC0000000ull) : 0ull;
+                if (flag == 0) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, (int)ERR_LOOKBACK_TIMEOUT);
+                        break;
+                    }
+                    continue;
                 }
-                if (done) break;
-                if (used == 0 && ++spins > kSpinLimit) {
-                    atomicOr(err, (int)ERR_LOOKBACK_TIMEOUT);
-                    break;
-                }
-                t -= used;
+                excl += (uint32_t)(s & kStatMask);
+                if (flag == kStatPrefix) break;
+                --t;
             }
             st_volatile_u64(my, ep | kStatPrefix | (excl + run));
         }
