@@ -593,22 +593,54 @@ __global__ void __launch_bounds__(kTriThreads)
         const int tile = s_tile;
         if (tile >= ntiles) break;
         const int t0 = tile * kTriThreads;
-        // count pass: warp per triangle
-        for (int k = warp; k < kTriThreads; k += WARPS) {
-            const int i = t0 + k;
+        // Each lane prepares one of the warp's 32 triangles of the tile
+        // (k = warp + 8 lane): order, record and candidate bins are loaded for
+        // all 32 at once, and the sweeps take them from the owning lane.
+        TriBins myC;
+        myC.any = false;
+        myC.cbx = myC.cby = myC.cex = myC.cey = 0;
+        myC.bx = myC.by = myC.bz = myC.ex = myC.ey = 0.0f;
+        int myG = -1, myBB = 0, myL2 = 0;
+        {
+            const int i = t0 + warp + WARPS * lane;
             const int g = (order && i < totalTris) ? (int)order[i] : i;
-            int cnt = 0;
             if (i < totalTris && (unsigned)g < (unsigned)totalTris) {
+                myG = g;
                 const int fi = frame_of(triBases, nframes, g);
                 const FrameState &st = states[fi];
                 if (st.state == 2 && st.nValidTris > 0) {
                     const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
                                  q3 = __ldg(rec + 4 * (size_t)g + 3);
-                    const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
-                    if (c.any)
-                        cnt = sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals, 0,
-                                         capacity, g, false);
+                    myC = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
+                    myBB = frames[fi].binBase;
+                    myL2 = frames[fi].log2Wb;
                 }
+            }
+        }
+        auto take = [&](int j, TriBins &c, int &g, int &bb, int &l2) {
+            c.cbx = __shfl_sync(kFullWarp, myC.cbx, j);
+            c.cby = __shfl_sync(kFullWarp, myC.cby, j);
+            c.cex = __shfl_sync(kFullWarp, myC.cex, j);
+            c.cey = __shfl_sync(kFullWarp, myC.cey, j);
+            c.bx = __shfl_sync(kFullWarp, myC.bx, j);
+            c.by = __shfl_sync(kFullWarp, myC.by, j);
+            c.bz = __shfl_sync(kFullWarp, myC.bz, j);
+            c.ex = __shfl_sync(kFullWarp, myC.ex, j);
+            c.ey = __shfl_sync(kFullWarp, myC.ey, j);
+            c.any = __shfl_sync(kFullWarp, (int)myC.any, j) != 0;
+            g = __shfl_sync(kFullWarp, myG, j);
+            bb = __shfl_sync(kFullWarp, myBB, j);
+            l2 = __shfl_sync(kFullWarp, myL2, j);
+        };
+        // count pass: warp per triangle
+        for (int j = 0; j < 32; ++j) {
+            const int k = warp + WARPS * j;
+            TriBins c;
+            int g, bb, l2;
+            take(j, c, g, bb, l2);
+            int cnt = 0;
+            if (g >= 0) {
+                if (c.any) cnt = sweep_bins(binStat, c, bb, l2, lane, pkeys, pvals, 0, capacity, g, false);
                 if (lane == 0) triCount[g] = cnt;
             }
             if (lane == 0) s_cnt[k] = cnt;
@@ -670,20 +702,14 @@ __global__ void __launch_bounds__(kTriThreads)
         __syncthreads();
         // write pass, same order
         const unsigned long long tileBase = s_excl;
-        for (int k = warp; k < kTriThreads; k += WARPS) {
-            const int i = t0 + k;
-            if (i >= totalTris) continue;
-            const int g = order ? (int)order[i] : i;
-            if ((unsigned)g >= (unsigned)totalTris) continue;
-            const int fi = frame_of(triBases, nframes, g);
-            const FrameState &st = states[fi];
-            if (!(st.state == 2 && st.nValidTris > 0)) continue;
-            const float4 q0 = __ldg(rec + 4 * (size_t)g), q1 = __ldg(rec + 4 * (size_t)g + 1),
-                         q3 = __ldg(rec + 4 * (size_t)g + 3);
-            const TriBins c = tri_candidates(q0, q1, q3, st, frames[fi].Wb);
-            if (!c.any) continue;
-            sweep_bins(binStat, c, frames[fi].binBase, frames[fi].log2Wb, lane, pkeys, pvals,
-                       tileBase + (unsigned long long)s_cnt[k], capacity, g, true);
+        for (int j = 0; j < 32; ++j) {
+            const int k = warp + WARPS * j;
+            TriBins c;
+            int g, bb, l2;
+            take(j, c, g, bb, l2);
+            if (g < 0 || !c.any) continue;
+            sweep_bins(binStat, c, bb, l2, lane, pkeys, pvals, tileBase + (unsigned long long)s_cnt[k], capacity, g,
+                       true);
         }
     }
 }
