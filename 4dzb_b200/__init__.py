@@ -51,7 +51,7 @@ EXPORTED = [
     "fdzb_ctx_set_scene_params", "fdzb_ctx_set_area_light", "fdzb_ctx_move_model",
     "fdzb_ctx_launch", "fdzb_ctx_launch_async", "fdzb_ctx_sync", "fdzb_ctx_get_stats",
     "fdzb_ctx_export", "fdzb_ctx_set_debug", "fdzb_ctx_set_tri_order", "fdzb_light_setup",
-    "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate", "fdzb_sort_pairs_noalloc",
+    "fdzb_version", "fdzb_ctx_set_profiling", "fdzb_measure_alu_rate", "fdzb_check_division", "fdzb_sort_pairs_noalloc",
     "fdzb_ctx_set_graph", "fdzb_batch_create", "fdzb_batch_destroy", "fdzb_batch_set_stream",
     "fdzb_batch_set_graph", "fdzb_batch_set_profiling", "fdzb_batch_set_tri_order",
     "fdzb_batch_launch_async", "fdzb_batch_sync", "fdzb_batch_launch", "fdzb_batch_get_frame_stats",
@@ -265,6 +265,7 @@ def load() -> ctypes.CDLL:
         "fdzb_ctx_export": ([vp, i32, vp, sz], i32), "fdzb_ctx_set_debug": ([vp, i32], i32),
         "fdzb_ctx_set_tri_order": ([vp, i32], i32), "fdzb_ctx_set_profiling": ([vp, i32], i32),
         "fdzb_measure_alu_rate": ([P(ctypes.c_double)], i32),
+        "fdzb_check_division": ([ctypes.c_uint64, ctypes.c_uint64, P(ctypes.c_uint64), P(ctypes.c_uint64)], i32),
         "fdzb_light_setup": ([P(AreaLightDesc), P(ctypes.c_float), P(ctypes.c_float),
                               P(ctypes.c_float), P(ctypes.c_float)], i32),
         "fdzb_version": ([], ctypes.c_char_p),
@@ -341,6 +342,14 @@ def light_setup(light) -> dict:
     return dict(mat=np.array(mat, dtype=np.float32), RF=np.array(rf, dtype=np.float32),
                 corners=np.array(corners, dtype=np.float32).reshape(4, 3),
                 deltas=np.array(deltas, dtype=np.float32).reshape(2, 3))
+
+
+def check_division(trials: int, seed: int = 1) -> tuple:
+    """(mismatches, checked): the device self-check of the occlusion rows'
+    quotient against the IEEE division (fdzb_check_division)."""
+    m, n = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(load().fdzb_check_division(trials, seed, ctypes.byref(m), ctypes.byref(n)))
+    return int(m.value), int(n.value)
 
 
 def measure_alu_rate() -> float:

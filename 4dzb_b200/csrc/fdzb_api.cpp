@@ -1103,6 +1103,16 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second)
     return FDZB_OK;
 }
 
+int fdzb_check_division(uint64_t trials, uint64_t seed, uint64_t *mismatches, uint64_t *checked)
+{
+    if (!mismatches || !checked) return fail(FDZB_ERR_INVALID_ARG, "out is NULL");
+    unsigned long long m = 0, n = 0;
+    FDZB_CUDA(fdzb::check_division(trials, seed, &m, &n));
+    *mismatches = m;
+    *checked = n;
+    return FDZB_OK;
+}
+
 int fdzb_ctx_set_open_box(fdzb_ctx *c, int mode)
 {
     if (int rc = ctx_check(c)) return rc;

@@ -166,6 +166,8 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
                          cudaEvent_t *stageEvents, int *launches);
 // Issue-rate probe: lane FP32 adds per second of a kernel with independent chains.
 cudaError_t measure_alu_rate(double *laneOpsPerSecond);
+cudaError_t check_division(unsigned long long trials, unsigned long long seed, unsigned long long *mismatches,
+                           unsigned long long *checked);
 
 // Records `msg` as this thread's fdzb_last_error() and returns `code`.
 int set_error(int code, const std::string &msg);

@@ -15,6 +15,7 @@
 // exactly one full cycle.  The final mask is the OR over the tested triangles,
 // so it is independent of the order and of where in the cycle a lane starts.
 #pragma once
+#include <type_traits>
 #include "fdzb_device.cuh"
 
 namespace fdzb {
@@ -67,24 +68,24 @@ template <> struct RowWord<unsigned long long> {
 typedef unsigned long long u64;
 
 // K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(count-1) precomputed (the
-// same product) and the result limited to the grid's bits.  The shift has the
-// PTX shl semantics of the reference's device code: amounts >= the word width
-// (or negative) give 0.  -1*D is the exact negation -D, and the reference's
-// truncating conversion of ceilf(q) is the round-up conversion of q (both
-// saturate out of range and map NaN to 0).  The quotient is formed whether or
-// not the row is partial and the full and empty cases are selected after it:
-// within a warp some lane nearly always needs it, and the branch around it
-// cost more than the division (measured: HD frame occlusion 7.23 -> 7.09 ms,
-// 20k-triangle frame 8.07 -> 7.56 ms).  A zero slope makes the quotient
-// infinite or NaN, but then D and D + slope*(count-1) have the same sign and
-// the selection never takes it.
+// same product) and the result limited to the grid's bits; q is the quotient
+// -D / slope, rounded to nearest as the reference's division rounds it.  The
+// shift has the PTX shl semantics of the reference's device code: amounts >=
+// the word width (or negative) give 0.  -1*D is the exact negation -D, and the
+// reference's truncating conversion of ceilf(q) is the round-up conversion of
+// q (both saturate out of range and map NaN to 0).  The quotient is formed
+// whether or not the row is partial and the full and empty cases are selected
+// after it: within a warp some lane nearly always needs it, and the branch
+// around it cost more than the division (measured: HD frame occlusion 7.23 ->
+// 7.09 ms, 20k-triangle frame 8.07 -> 7.56 ms).  A zero slope makes the
+// quotient infinite or NaN, but then D and D + slope*(count-1) have the same
+// sign and the selection never takes it.
 template <class R>
-__device__ __forceinline__ R row_mask(float D, float slopeNm1, float slope, R full, uint32_t &npart)
+__device__ __forceinline__ R row_mask(float D, float slopeNm1, float q, R full, uint32_t &npart)
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
     npart += (f1 != f2);
-    const float q = __fdiv_rn(-D, slope);
     const int k = __float2int_ru(q);
     R m = ((unsigned)k >= (unsigned)RowWord<R>::kBits) ? R(0) : (R(1) << k);
     m -= R(1);
@@ -92,6 +93,28 @@ __device__ __forceinline__ R row_mask(float D, float slopeNm1, float slope, R fu
     m &= full;
     return (f1 == f2) ? (f1 ? full : R(0)) : m;
 }
+
+// a / b rounded to nearest, from y = RN(1/b): two correction steps of
+// Markstein's method (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990, with the
+// theorem as restated in Muller et al., Handbook of Floating-Point
+// Arithmetic, sec. 4.7).  With a, b, y free of underflow and overflow:
+// q0 = RN(a y) lies within two ulps of a/b, so each residual a - b q is exact
+// (an FMA); the first step brings q within one ulp (in fact within half an
+// ulp plus a term of order 2^-46), and the second, by Markstein's theorem (y
+// within half an ulp of 1/b, q within one ulp of a/b), returns RN(a/b).  The
+// pair test hoists y out of its row loop, one reciprocal per edge, so that a
+// row's quotient costs five FP32 operations instead of a division; a device
+// self-check (fdzb_check_division) compares it with the IEEE division.
+__device__ __forceinline__ float div_by_rcp(float a, float b, float y)
+{
+    const float q0 = __fmul_rn(a, y);
+    const float r0 = __fmaf_rn(-b, q0, a);
+    const float q1 = __fmaf_rn(r0, y, q0);
+    const float r1 = __fmaf_rn(-b, q1, a);
+    return __fmaf_rn(r1, y, q1);
+}
+
 // The same mask with the full and empty cases returned before the division:
 // the per-pair row filter's masks are mostly full or empty across the warp,
 // so there the branch pays (measured: HD frame occlusion 6.88 -> 6.82 ms,
@@ -389,20 +412,66 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
     // occlusion 7.09 -> 6.91 ms) and the early stop in the other (20k-triangle
     // frame 7.54 vs 7.62 ms); the unconditional write-back pays in the second
     // only when combined with the early stop.
-    while (vr) {
-        const int r = RowWord<R>::lowest(vr);
-        vr &= vr - R(1);
-        ++nrows;
-        const float fr = (float)r;
-        const R have = rows[r][lane];
-        R m = row_mask<R>(__fadd_rn(__fmul_rn(A0, fr), C0), Bn0, B0, g.FC, npart);
-        if (FLAT || (m & ~have)) m &= row_mask<R>(__fadd_rn(__fmul_rn(A1, fr), C1), Bn1, B1, g.FC, npart);
-        if (FLAT || (m & ~have)) m &= row_mask<R>(__fadd_rn(__fmul_rn(A2, fr), C2), Bn2, B2, g.FC, npart);
-        if (dp && (m & ~have)) m &= row_mask<R>(__fadd_rn(__fmul_rn(A3, fr), C3), Bn3, B3, g.FC, npart);
-        const R nv = have | m;
-        rows[r][lane] = nv;
-        if (nv == g.FC) fullRows |= R(1) << r;
-    }
+    // The rows' quotients -D / B_k by div_by_rcp with y_k = RN(1/B_k).  Its
+    // preconditions hold when every A_k and C_k lies in [2^-38, 2^40] and every
+    // B_k in [2^-100, 2^39] (magnitudes): then D = RN(RN(A_k r) + C_k) is a
+    // multiple of 2^-61 (each term is a multiple of its operand's ulp), so a
+    // nonzero D has |D| >= 2^-61 and |D| <= 2^47; a partial row (D and
+    // D + B_k (count-1) of opposite signs) has |D / B_k| < 64, and with
+    // |B_k| <= 2^39 a nonzero quotient is at least 2^-100 -- no quantity of
+    // the method underflows or overflows.  A zero D gives a zero quotient of
+    // the division's sign either way.  Where the full and empty cases
+    // discard the quotient, its value does not matter.  A pair outside these
+    // ranges (a zero coefficient included) takes the IEEE division.
+    // Measured: HD frame occlusion 6.82 -> 6.39 ms, 20k-triangle frame 7.46 ->
+    // 6.85 ms, identical masks.
+    const float lo = fminf(fminf(fminf(fabsf(A0), fabsf(A1)), fminf(fabsf(A2), fabsf(C0))),
+                           fminf(fabsf(C1), fabsf(C2)));
+    const float hi = fmaxf(fmaxf(fmaxf(fabsf(A0), fabsf(A1)), fmaxf(fabsf(A2), fabsf(C0))),
+                           fmaxf(fabsf(C1), fabsf(C2)));
+    const float bl = fminf(fminf(fabsf(B0), fabsf(B1)), fabsf(B2));
+    const float bh = fmaxf(fmaxf(fabsf(B0), fabsf(B1)), fabsf(B2));
+    const bool viaRcp = lo >= 0x1p-38f && hi <= 0x1p40f && bl >= 0x1p-100f && bh <= 0x1p39f;
+    const float y0 = __frcp_rn(B0), y1 = __frcp_rn(B1), y2 = __frcp_rn(B2);
+    // rows (:204-222).  The row's mask is the AND of the edges' masks, so it only
+    // loses bits as edges are added: once it holds no bit the row lacks, the
+    // remaining edges cannot change the row.  Without FLAT they are then not
+    // evaluated; with it every edge is (no divergent branch per edge).  The
+    // row is written back either way (OR-ing nothing new leaves it as it is).
+    // Measured, the flat form pays in the open-box instantiation (HD frame
+    // occlusion 7.09 -> 6.91 ms) and the early stop in the other (20k-triangle
+    // frame 7.54 vs 7.62 ms); the unconditional write-back pays in the second
+    // only when combined with the early stop.
+    auto row_loop = [&](auto rcp) {
+        constexpr bool kRcp = decltype(rcp)::value;
+        auto quot = [&](float D, float B, float y) { return kRcp ? div_by_rcp(-D, B, y) : __fdiv_rn(-D, B); };
+        while (vr) {
+            const int r = RowWord<R>::lowest(vr);
+            vr &= vr - R(1);
+            ++nrows;
+            const float fr = (float)r;
+            const R have = rows[r][lane];
+            const float D0 = __fadd_rn(__fmul_rn(A0, fr), C0);
+            R m = row_mask<R>(D0, Bn0, quot(D0, B0, y0), g.FC, npart);
+            if (FLAT || (m & ~have)) {
+                const float D1 = __fadd_rn(__fmul_rn(A1, fr), C1);
+                m &= row_mask<R>(D1, Bn1, quot(D1, B1, y1), g.FC, npart);
+            }
+            if (FLAT || (m & ~have)) {
+                const float D2 = __fadd_rn(__fmul_rn(A2, fr), C2);
+                m &= row_mask<R>(D2, Bn2, quot(D2, B2, y2), g.FC, npart);
+            }
+            if (dp && (m & ~have)) {
+                const float D3 = __fadd_rn(__fmul_rn(A3, fr), C3);
+                m &= row_mask<R>(D3, Bn3, __fdiv_rn(-D3, B3), g.FC, npart);
+            }
+            const R nv = have | m;
+            rows[r][lane] = nv;
+            if (nv == g.FC) fullRows |= R(1) << r;
+        }
+    };
+    if (viaRcp) row_loop(std::true_type{});
+    else row_loop(std::false_type{});
     return 1;
 }
 

@@ -967,6 +967,111 @@ cudaError_t measure_alu_rate(double *rate)
     return e;
 }
 
+// ---------------------------------------------------------------------------
+// Self-check of div_by_rcp (the occlusion rows' quotient) against the IEEE
+// division __fdiv_rn, over the operand ranges the pair test admits to it.
+// Trial t draws (from a counter hash of seed and t) three cases: a and b with
+// random significands and signs, |a| in [2^-61, 2^47] and |b| in
+// [2^-100, 2^39] (quotients outside [2^-100, 2^100] are skipped); a quotient
+// within two ulps of the midpoint above a random float in [2^-8, 64] (the
+// hardest case for rounding); and b a random float with a = b * k for a small
+// integer k (quotients at integers, where the rows' round-up conversion
+// turns).  Counts the trials whose results differ in any bit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t check_hash(unsigned long long x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+
+// random float with biased exponent 127 + [lo, hi], random significand and sign
+__device__ __forceinline__ float check_float(unsigned long long s, int lo, int hi)
+{
+    const uint32_t h = check_hash(s), g = check_hash(s * 0x9E3779B97F4A7C15ull + 7u);
+    const int e = lo + (int)(g % (uint32_t)(hi - lo + 1));
+    return __uint_as_float(((uint32_t)(e + 127) << 23) | (h & 0x807FFFFFu));
+}
+
+__global__ void k_check_division(unsigned long long trials, unsigned long long seed,
+                                 unsigned long long *mismatches, unsigned long long *checked)
+{
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    unsigned long long bad = 0, n = 0;
+    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < trials;
+         t += stride) {
+        const unsigned long long s = (seed << 40) ^ (t * 4u);
+        // 1. random operands
+        {
+            const float a = check_float(s, -61, 46), b = check_float(s + 1u, -100, 38);
+            const float q = __fdiv_rn(a, b);
+            const float aq = fabsf(q);
+            if (aq >= 0x1p-100f && aq <= 0x1p100f) {
+                ++n;
+                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+            }
+        }
+        // 2. quotients next to a rounding midpoint
+        {
+            const float m = fabsf(check_float(s + 2u, -8, 5));
+            const float b = check_float(s + 3u, -60, 38);
+            const double mid = 0.5 * ((double)m + (double)__uint_as_float(__float_as_uint(m) + 1u));
+            float a = (float)(mid * (double)b);
+            const int k = (int)(check_hash(s + 5u) % 5u) - 2;
+            a = __uint_as_float(__float_as_uint(a) + (uint32_t)k);
+            const float q = __fdiv_rn(a, b);
+            const float aq = fabsf(q);
+            if (aq >= 0x1p-100f && aq <= 0x1p100f && fabsf(a) <= 0x1p47f && fabsf(a) >= 0x1p-61f) {
+                ++n;
+                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+            }
+        }
+        // 3. quotients at and next to small integers
+        {
+            const float b = check_float(s + 6u, -40, 38);
+            const int k = (int)(check_hash(s + 7u) % 130u) - 65;
+            float a = __fmul_rn(b, (float)k);
+            const int d = (int)(check_hash(s + 8u) % 3u) - 1;
+            if (a != 0.0f) a = __uint_as_float(__float_as_uint(a) + (uint32_t)d);
+            const float q = __fdiv_rn(a, b);
+            const float aq = fabsf(q);
+            if ((aq >= 0x1p-100f || q == 0.0f) && aq <= 0x1p100f && fabsf(a) <= 0x1p47f &&
+                (fabsf(a) >= 0x1p-61f || a == 0.0f)) {
+                ++n;
+                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bad += __shfl_xor_sync(kFullWarp, bad, o);
+        n += __shfl_xor_sync(kFullWarp, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicAdd(mismatches, bad);
+        atomicAdd(checked, n);
+    }
+}
+
+cudaError_t check_division(unsigned long long trials, unsigned long long seed, unsigned long long *mismatches,
+                           unsigned long long *checked)
+{
+    unsigned long long *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+    cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+    k_check_division<<<sm_count() * 8, 256>>>(trials, seed, d, d + 1);
+    e = cudaGetLastError();
+    unsigned long long h[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    *mismatches = h[0];
+    *checked = h[1];
+    return e;
+}
+
 }  // namespace fdzb
 
 // ---------------------------------------------------------------------------

@@ -271,6 +271,16 @@ int fdzb_ctx_set_profiling(fdzb_ctx *ctx, int enable);
  * occlusion kernel's operation rate is reported.  No counterpart in the reference. */
 int fdzb_measure_alu_rate(double *lane_ops_per_second);
 
+/* Device self-check of the occlusion kernel's row quotient: -D / B from a
+ * hoisted reciprocal RN(1/B) by two Markstein correction steps, which the pair
+ * test uses in place of the IEEE division where its operands are in range.
+ * Runs `trials` trials of three cases each (random operands over the admitted
+ * ranges, quotients next to rounding midpoints, quotients at small integers)
+ * and returns the number of compared cases and of results that differ from
+ * __fdiv_rn in any bit (expected: 0).  No counterpart in the reference, whose
+ * rows divide directly (K/Step5_2_shadowCalPerSample.inl:20). */
+int fdzb_check_division(uint64_t trials, uint64_t seed, uint64_t *mismatches, uint64_t *checked);
+
 /* Host-side light setup only (FS/api.cpp:303-400): fills the 16-float
  * column-major light projection, RectangleFactor and the four light corners
  * (upRight, upLeft, downLeft, downRight), x_delt and y_delt. */
