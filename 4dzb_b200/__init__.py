@@ -352,6 +352,16 @@ def check_division(trials: int, seed: int = 1) -> tuple:
     return int(m.value), int(n.value)
 
 
+PROFILE_OFF, PROFILE_ALL, PROFILE_STAGES = 0, 1, 2
+
+
+def _profile_mode(enable) -> int:
+    """True/False or one of the PROFILE_* modes."""
+    if isinstance(enable, bool):
+        return PROFILE_ALL if enable else PROFILE_OFF
+    return int(enable)
+
+
 def measure_alu_rate() -> float:
     """FP32 lane operations per second of the current device (issue-rate probe)."""
     v = ctypes.c_double()
@@ -396,9 +406,11 @@ class Context:
         """flags bit 0: keep pre-sort copies of the key arrays for export()."""
         _check(self._lib.fdzb_ctx_set_debug(self._h, int(flags)))
 
-    def set_profiling(self, enable: bool) -> None:
-        """Per-stage CUDA-event timing, reported in stats()['stage_ms']."""
-        _check(self._lib.fdzb_ctx_set_profiling(self._h, int(bool(enable))))
+    def set_profiling(self, enable) -> None:
+        """Per-stage CUDA-event timing, reported in stats()['stage_ms'], and the
+        occlusion kernel's work counters (True or PROFILE_ALL); PROFILE_STAGES:
+        the timing alone, with the unprofiled kernels."""
+        _check(self._lib.fdzb_ctx_set_profiling(self._h, _profile_mode(enable)))
 
     def set_tri_order(self, order: int) -> None:
         """TRI_ORDER_REFERENCE (the reference's per-bin order) or TRI_ORDER_COVERAGE."""
@@ -682,8 +694,9 @@ class Batch:
     def set_graph(self, enable: bool) -> None:
         _check(self._lib.fdzb_batch_set_graph(self._h, int(bool(enable))))
 
-    def set_profiling(self, enable: bool) -> None:
-        _check(self._lib.fdzb_batch_set_profiling(self._h, int(bool(enable))))
+    def set_profiling(self, enable) -> None:
+        """As Context.set_profiling."""
+        _check(self._lib.fdzb_batch_set_profiling(self._h, _profile_mode(enable)))
 
     def set_tri_order(self, order: int) -> None:
         _check(self._lib.fdzb_batch_set_tri_order(self._h, int(order)))

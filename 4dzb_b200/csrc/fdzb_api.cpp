@@ -357,6 +357,7 @@ int engine_enqueue(Engine &e)
         const bool want = e.openBoxMode == FDZB_OPEN_BOX_ON ||
                           (e.openBoxMode == FDZB_OPEN_BOX_AUTO && (known == e.openBoxKeep.end() || known->second));
         b.openBox = (want && !e.rayCast && b.occVariant == 0) ? 1 : 0;
+        b.countWork = (e.profile && e.countWork) ? 1 : 0;
         e.lastOpenBox = b.openBox != 0;
     }
     // Triangle lists: the pairs are sorted by bin only (stable, so a bin lists
@@ -1061,7 +1062,9 @@ int fdzb_ctx_set_debug(fdzb_ctx *c, int flags)
 int fdzb_ctx_set_profiling(fdzb_ctx *c, int enable)
 {
     if (int rc = ctx_check(c)) return rc;
+    if (enable < 0 || enable > FDZB_PROFILE_STAGES) return fail(FDZB_ERR_INVALID_ARG, "profiling mode must be 0, 1 or 2");
     c->eng.profile = enable != 0;
+    c->eng.countWork = enable == FDZB_PROFILE_ALL;
     return FDZB_OK;
 }
 
@@ -1511,7 +1514,9 @@ int fdzb_batch_set_graph(fdzb_batch *b, int enable)
 int fdzb_batch_set_profiling(fdzb_batch *b, int enable)
 {
     if (int rc = batch_check(b)) return rc;
+    if (enable < 0 || enable > FDZB_PROFILE_STAGES) return fail(FDZB_ERR_INVALID_ARG, "profiling mode must be 0, 1 or 2");
     b->eng.profile = enable != 0;
+    b->eng.countWork = enable == FDZB_PROFILE_ALL;
     return FDZB_OK;
 }
 

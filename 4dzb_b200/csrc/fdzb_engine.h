@@ -62,6 +62,7 @@ struct Engine {
     int debug = 0;  // keep pre-sort copies for export
     int triOrder = FDZB_TRI_ORDER_COVERAGE;
     bool profile = false;  // record events at the stage boundaries
+    bool countWork = false;  // with profile: the occlusion kernel form that counts its work
     bool useGraph = true;
     int occVariant = 0;    // occlusion kernel (DeviceBuffers::occVariant)
     int rayCast = 0;       // ray-cast cross-check instead of edge masks (DeviceBuffers::rayCast)

@@ -67,31 +67,48 @@ template <> struct RowWord<unsigned long long> {
 };
 typedef unsigned long long u64;
 
-// K/Step5_2_shadowCalPerSample.inl:14-33 with slope*(count-1) precomputed (the
-// same product) and the result limited to the grid's bits; q is the quotient
-// -D / slope, rounded to nearest as the reference's division rounds it.  The
-// shift has the PTX shl semantics of the reference's device code: amounts >=
-// the word width (or negative) give 0.  -1*D is the exact negation -D, and the
-// reference's truncating conversion of ceilf(q) is the round-up conversion of
-// q (both saturate out of range and map NaN to 0).  The quotient is formed
-// whether or not the row is partial and the full and empty cases are selected
-// after it: within a warp some lane nearly always needs it, and the branch
-// around it cost more than the division (measured: HD frame occlusion 7.23 ->
-// 7.09 ms, 20k-triangle frame 8.07 -> 7.56 ms).  A zero slope makes the
-// quotient infinite or NaN, but then D and D + slope*(count-1) have the same
-// sign and the selection never takes it.
-template <class R>
-__device__ __forceinline__ R row_mask(float D, float slopeNm1, float q, R full, uint32_t &npart)
+// K/Step5_2_shadowCalPerSample.inl:14-33, as the range of set columns.  With
+// f1 = D >= 0, f2 = D + slope*(count-1) >= 0 and k = the round-up conversion
+// of q (q = -D / slope rounded to nearest, as the reference divides; its
+// truncating conversion of ceilf(q) is the same integer) the reference's mask
+// is: all columns when f1 and f2, none when neither, else (1 << k) - 1 (PTX
+// shl: amounts >= the word width give 0), complemented when !f1, limited to
+// the grid.  In the partial cases 0 <= k <= count: D and D + slope*(count-1)
+// have opposite signs, so |q| <= (count-1)(1 + 2^-24) and the quotient's sign
+// is that of D / (D - (D + Bn)), i.e. q >= 0.  So the mask is the column range
+// [lo, hi) with lo = f1 ? 0 : k and hi = f2 ? count : k -- [0, count) when
+// both hold, [0, k) or [k, count) when one does, and [k, k) = nothing when
+// neither (whatever k is then).  A row's mask, the AND of its edges' masks,
+// is the intersection of their ranges: [max lo, min hi).  This replaces
+// per-edge shifts, complements and selections by two min/max and one
+// two-shift difference per row (measured: HD frame occlusion 6.48 -> 5.94
+// ms, large frame 1457 -> 1290 ms).  npart counts the partial cases (COUNT).
+template <int COUNT>
+__device__ __forceinline__ void col_range(float D, float slopeNm1, float q, int count, int &lo, int &hi,
+                                          uint32_t &npart)
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
-    npart += (f1 != f2);
+    if (COUNT) npart += (f1 != f2);
     const int k = __float2int_ru(q);
-    R m = ((unsigned)k >= (unsigned)RowWord<R>::kBits) ? R(0) : (R(1) << k);
-    m -= R(1);
-    if (!f1) m = ~m;
-    m &= full;
-    return (f1 == f2) ? (f1 ? full : R(0)) : m;
+    lo = f1 ? 0 : k;
+    hi = f2 ? count : k;
+}
+
+// 1 << s with the PTX shl semantics (0 for s >= the word width; s < 0 read as
+// unsigned, so 0 as well), and the bits [lo, hi) (none when hi <= lo).
+template <class R> __device__ __forceinline__ R bit_at(int s);
+template <> __device__ __forceinline__ uint32_t bit_at<uint32_t>(int s)
+{
+    return __funnelshift_lc(0u, 1u, (unsigned)s);   // high word of (1:0) << min(s, 32)
+}
+template <> __device__ __forceinline__ unsigned long long bit_at<unsigned long long>(int s)
+{
+    return (unsigned)s >= 64u ? 0ull : (1ull << s);
+}
+template <class R> __device__ __forceinline__ R range_bits(int lo, int hi)
+{
+    return bit_at<R>(max(hi, lo)) - bit_at<R>(lo);
 }
 
 // a / b rounded to nearest, from y = RN(1/b): two correction steps of
@@ -115,18 +132,19 @@ __device__ __forceinline__ float div_by_rcp(float a, float b, float y)
     return __fmaf_rn(r1, y, q1);
 }
 
-// The same mask with the full and empty cases returned before the division:
-// the per-pair row filter's masks are mostly full or empty across the warp,
-// so there the branch pays (measured: HD frame occlusion 6.88 -> 6.82 ms,
-// 20k-triangle frame 7.52 -> 7.44 ms against row_mask).
-template <class R>
+// The same mask, over the light rows (the row filter, :176-191), with the
+// full and empty cases returned before the division: the per-pair row
+// filter's masks are mostly full or empty across the warp, so there the
+// branch pays (measured: HD frame occlusion 6.88 -> 6.82 ms, 20k-triangle
+// frame 7.52 -> 7.44 ms against a branch-free form).
+template <class R, int COUNT>
 __device__ __forceinline__ R row_filter_mask(float D, float slopeNm1, float slope, R full, uint32_t &npart)
 {
     const bool f1 = D >= 0.0f;
     const bool f2 = __fadd_rn(slopeNm1, D) >= 0.0f;
     if (f1 && f2) return full;
     if (!f1 && !f2) return R(0);
-    ++npart;
+    if (COUNT) ++npart;
     const float q = __fdiv_rn(-D, slope);
     const int k = __float2int_ru(q);
     R m = ((unsigned)k >= (unsigned)RowWord<R>::kBits) ? R(0) : (R(1) << k);
@@ -357,7 +375,7 @@ template <class R> __device__ __forceinline__ GridC<R> grid_of(const FrameDesc &
 // between them needs no such test.  Returns 1 if the pair passed the AABB
 // pre-cull.  FLAT = 1 evaluates all three edges of every open row instead of
 // stopping once the row mask holds nothing new (see the row loop).
-template <class R, int DEPTH, int FLAT>
+template <class R, int DEPTH, int FLAT, int COUNT>
 __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s, f3 xd, f3 yd, f3 ur,
                                          float esp, const GridC<R> &g, R (*rows)[32], int lane, R &fullRows,
                                          uint32_t &nrows, uint32_t &npart)
@@ -387,9 +405,9 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
     const float An0 = __fmul_rn(A0, g.nrm1), An1 = __fmul_rn(A1, g.nrm1), An2 = __fmul_rn(A2, g.nrm1);
     const float Bn0 = __fmul_rn(B0, g.ncm1), Bn1 = __fmul_rn(B1, g.ncm1), Bn2 = __fmul_rn(B2, g.ncm1);
     // row filter (:176-191)
-    const R N0 = row_filter_mask<R>(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, g.FR, npart);
-    const R N1 = row_filter_mask<R>(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, g.FR, npart);
-    const R N2 = row_filter_mask<R>(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, g.FR, npart);
+    const R N0 = row_filter_mask<R, COUNT>(__fadd_rn(B0 > 0.0f ? Bn0 : 0.0f, C0), An0, A0, g.FR, npart);
+    const R N1 = row_filter_mask<R, COUNT>(__fadd_rn(B1 > 0.0f ? Bn1 : 0.0f, C1), An1, A1, g.FR, npart);
+    const R N2 = row_filter_mask<R, COUNT>(__fadd_rn(B2 > 0.0f ? Bn2 : 0.0f, C2), An2, A2, g.FR, npart);
     R vr = N0 & N1 & N2 & ~fullRows;
     const bool dp = DEPTH && (p1.x <= 0.0f || p6.z >= s.spZ);
     float A3 = 0.0f, B3 = 0.0f, C3 = 0.0f, Bn3 = 0.0f;
@@ -401,17 +419,8 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
         B3 = dot3(m, t1);
         C3 = dot3(m, lv);
         Bn3 = __fmul_rn(B3, g.ncm1);
-        vr &= row_filter_mask<R>(__fadd_rn(B3 > 0.0f ? Bn3 : 0.0f, C3), __fmul_rn(A3, g.nrm1), A3, g.FR, npart);
+        vr &= row_filter_mask<R, COUNT>(__fadd_rn(B3 > 0.0f ? Bn3 : 0.0f, C3), __fmul_rn(A3, g.nrm1), A3, g.FR, npart);
     }
-    // rows (:204-222).  The row's mask is the AND of the edges' masks, so it only
-    // loses bits as edges are added: once it holds no bit the row lacks, the
-    // remaining edges cannot change the row.  Without FLAT they are then not
-    // evaluated; with it every edge is (no divergent branch per edge).  The
-    // row is written back either way (OR-ing nothing new leaves it as it is).
-    // Measured, the flat form pays in the open-box instantiation (HD frame
-    // occlusion 7.09 -> 6.91 ms) and the early stop in the other (20k-triangle
-    // frame 7.54 vs 7.62 ms); the unconditional write-back pays in the second
-    // only when combined with the early stop.
     // The rows' quotients -D / B_k by div_by_rcp with y_k = RN(1/B_k).  Its
     // preconditions hold when every A_k and C_k lies in [2^-38, 2^40] and every
     // B_k in [2^-100, 2^39] (magnitudes): then D = RN(RN(A_k r) + C_k) is a
@@ -448,22 +457,46 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
         while (vr) {
             const int r = RowWord<R>::lowest(vr);
             vr &= vr - R(1);
-            ++nrows;
+            if (COUNT) ++nrows;
             const float fr = (float)r;
             const R have = rows[r][lane];
             const float D0 = __fadd_rn(__fmul_rn(A0, fr), C0);
-            R m = row_mask<R>(D0, Bn0, quot(D0, B0, y0), g.FC, npart);
-            if (FLAT || (m & ~have)) {
+            int lo, hi;
+            col_range<COUNT>(D0, Bn0, quot(D0, B0, y0), g.NC, lo, hi, npart);
+            R m;
+            if (FLAT) {
                 const float D1 = __fadd_rn(__fmul_rn(A1, fr), C1);
-                m &= row_mask<R>(D1, Bn1, quot(D1, B1, y1), g.FC, npart);
-            }
-            if (FLAT || (m & ~have)) {
                 const float D2 = __fadd_rn(__fmul_rn(A2, fr), C2);
-                m &= row_mask<R>(D2, Bn2, quot(D2, B2, y2), g.FC, npart);
+                int lo1, hi1, lo2, hi2;
+                col_range<COUNT>(D1, Bn1, quot(D1, B1, y1), g.NC, lo1, hi1, npart);
+                col_range<COUNT>(D2, Bn2, quot(D2, B2, y2), g.NC, lo2, hi2, npart);
+                lo = max(lo, max(lo1, lo2));
+                hi = min(hi, min(hi1, hi2));
+                m = range_bits<R>(lo, hi);
+            } else {
+                m = range_bits<R>(lo, hi);
+                if (m & ~have) {
+                    const float D1 = __fadd_rn(__fmul_rn(A1, fr), C1);
+                    int lo1, hi1;
+                    col_range<COUNT>(D1, Bn1, quot(D1, B1, y1), g.NC, lo1, hi1, npart);
+                    lo = max(lo, lo1);
+                    hi = min(hi, hi1);
+                    m = range_bits<R>(lo, hi);
+                }
+                if (m & ~have) {
+                    const float D2 = __fadd_rn(__fmul_rn(A2, fr), C2);
+                    int lo2, hi2;
+                    col_range<COUNT>(D2, Bn2, quot(D2, B2, y2), g.NC, lo2, hi2, npart);
+                    lo = max(lo, lo2);
+                    hi = min(hi, hi2);
+                    m = range_bits<R>(lo, hi);
+                }
             }
             if (dp && (m & ~have)) {
                 const float D3 = __fadd_rn(__fmul_rn(A3, fr), C3);
-                m &= row_mask<R>(D3, Bn3, __fdiv_rn(-D3, B3), g.FC, npart);
+                int lo3, hi3;
+                col_range<COUNT>(D3, Bn3, __fdiv_rn(-D3, B3), g.NC, lo3, hi3, npart);
+                m = range_bits<R>(max(lo, lo3), min(hi, hi3));
             }
             const R nv = have | m;
             rows[r][lane] = nv;
@@ -486,7 +519,7 @@ __device__ __forceinline__ int pair_test(const StagedTri &T, const LaneSample &s
 // masks compare bit for bit.  Same pre-cull as the reference's checker: the
 // sample's rectangle inside the triangle's AABB and minz - 1e-3 (in double, as
 // the reference's double literal makes it) not above the sample's depth.
-template <class R>
+template <class R, int COUNT>
 __device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample &s, f3 ur, f3 xd, f3 yd,
                                             const GridC<R> &g, R (*rows)[32], int lane, R &fullRows,
                                             uint32_t &nrows)
@@ -505,7 +538,7 @@ __device__ __forceinline__ int raycast_pair(const StagedTri &T, const LaneSample
     for (int r = 0; r < g.NR; ++r) {
         const R have = rows[r][lane];
         if (have == g.FC) continue;
-        ++nrows;
+        if (COUNT) ++nrows;
         const f3 lr = add3(ur, mul3(xd, (float)r));   // upRight + x_delt * j
         R add = 0;
         for (int c = 0; c < g.NC; ++c) {
@@ -675,7 +708,11 @@ __global__ void k_items(const FrameDesc *__restrict__ frames, const int32_t *__r
 // 64-bit form runs 2 warps per block to keep its rows in shared memory).
 // DEPTH = 1: the edge-function masks also test the triangle's own plane.
 // BOX = 1: the open-box cull (edge-function masks only).
-template <int RAYCAST, class R, int DEPTH, int BOX>
+// COUNT = 1: the work counters (pair tests, light rows, partial row masks) are
+// accumulated; the engine runs this form when profiling is on.  Counting costs
+// an add per row and per edge, 4-6 % of the kernel (measured); the open-box
+// cull's own counters (skipped and examined pairs) are kept in both forms.
+template <int RAYCAST, class R, int DEPTH, int BOX, int COUNT>
 __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlocks)
     k_occlusion(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
@@ -782,13 +819,15 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
             // staged triangle t against the lane's sample
             auto test_one = [&](int t) {
                 if (RAYCAST) {
-                    tested += raycast_pair<R>(tris[t], smp, ur, xd, yd, g, rows, lane, fullRows, nrows);
+                    const int ts = raycast_pair<R, COUNT>(tris[t], smp, ur, xd, yd, g, rows, lane, fullRows, nrows);
+                    if (COUNT) tested += ts;
                 } else if (kRefine && boxOn && tris[t].p[1].x > 0.0f && precull_pass(tris[t], smp) &&
                            !box_reach(prj[t], box)) {
                     ++boxSkips;
                 } else {
-                    tested += pair_test<R, DEPTH, kRefine>(tris[t], smp, xd, yd, ur, esp, g, rows, lane, fullRows, nrows,
-                                                  npart);
+                    const int ts = pair_test<R, DEPTH, kRefine, COUNT>(tris[t], smp, xd, yd, ur, esp, g, rows, lane,
+                                                                       fullRows, nrows, npart);
+                    if (COUNT) tested += ts;
                 }
                 if (fullRows == g.FR) remaining = 0;
             };
@@ -869,7 +908,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
         tb += __shfl_xor_sync(kFullWarp, tb, o);
         te += __shfl_xor_sync(kFullWarp, te, o);
     }
-    if (lane == 0 && t) {
+    if (COUNT && lane == 0 && t) {
         atomicAdd(&ctr->pairTests, t);
         atomicAdd(&ctr->rowsEvaluated, tr);
         atomicAdd(&ctr->partialMasks, tp);
@@ -926,8 +965,9 @@ __device__ __forceinline__ int nth_set_bit(uint32_t m, int k)
     return pos;
 }
 
-// row_mask without branches: the threshold is computed whatever the case and
-// selected away when the row is full or empty (same result as row_mask).
+// The reference's row mask without branches: the threshold is computed
+// whatever the case and selected away when the row is full or empty (the same
+// mask as col_range's column range).
 __device__ __forceinline__ uint32_t row_mask_sel(float D, float slopeNm1, float slope, uint32_t full,
                                                  uint32_t &npart)
 {

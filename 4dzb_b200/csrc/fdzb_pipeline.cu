@@ -897,25 +897,32 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
 #define FDZB_OCC_ARGS                                                                                        \
     b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd, b.binTriStart, \
         b.binTriEnd, pv, b.triRec, b.triPrj, b.totalTris, b.totalBins, nf
-    // b.openBox: the open-box cull's instantiation (edge-function masks only)
+    // b.openBox: the open-box cull's instantiation (edge-function masks only);
+    // b.countWork: the instantiation that accumulates the work counters
+#define FDZB_OCC(RC, RT, DP, BX, G, T)                                                                        \
+    do {                                                                                                   \
+        if (b.countWork) k_occlusion<RC, RT, DP, BX, 1><<<G, T, 0, s>>>(FDZB_OCC_ARGS);                     \
+        else k_occlusion<RC, RT, DP, BX, 0><<<G, T, 0, s>>>(FDZB_OCC_ARGS);                                 \
+    } while (0)
     if (b.wide) {
-        if (b.rayCast) k_occlusion<1, u64, 0, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
-        else if (b.depthPlane && b.openBox) k_occlusion<0, u64, 1, 1><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
-        else if (b.depthPlane) k_occlusion<0, u64, 1, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
-        else if (b.openBox) k_occlusion<0, u64, 0, 1><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
-        else k_occlusion<0, u64, 0, 0><<<g64, t64, 0, s>>>(FDZB_OCC_ARGS);
+        if (b.rayCast) FDZB_OCC(1, u64, 0, 0, g64, t64);
+        else if (b.depthPlane && b.openBox) FDZB_OCC(0, u64, 1, 1, g64, t64);
+        else if (b.depthPlane) FDZB_OCC(0, u64, 1, 0, g64, t64);
+        else if (b.openBox) FDZB_OCC(0, u64, 0, 1, g64, t64);
+        else FDZB_OCC(0, u64, 0, 0, g64, t64);
     } else if (b.rayCast) {
-        k_occlusion<1, uint32_t, 0, 0><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+        FDZB_OCC(1, uint32_t, 0, 0, g32, kOccThreads);
     } else if (b.occVariant == 1) {
         k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
     } else if (b.depthPlane) {
-        if (b.openBox) k_occlusion<0, uint32_t, 1, 1><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
-        else k_occlusion<0, uint32_t, 1, 0><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+        if (b.openBox) FDZB_OCC(0, uint32_t, 1, 1, g32, kOccThreads);
+        else FDZB_OCC(0, uint32_t, 1, 0, g32, kOccThreads);
     } else if (b.openBox) {
-        k_occlusion<0, uint32_t, 0, 1><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+        FDZB_OCC(0, uint32_t, 0, 1, g32, kOccThreads);
     } else {
-        k_occlusion<0, uint32_t, 0, 0><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
+        FDZB_OCC(0, uint32_t, 0, 0, g32, kOccThreads);
     }
+#undef FDZB_OCC
 #undef FDZB_OCC_ARGS
     nl += 2;
     if (ev) cudaEventRecord(ev[STAGE_COUNT], s);

@@ -382,14 +382,11 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
     for i in range(nframes):                 # warm-up: grows the arena to the largest frame
         plain_launch(i)
     plain_ms = []
-    pair_tests = 0
     for _ in range(max(2, steps // 2)):
         a, b = ev(), ev()
         a.record(stream)
-        pair_tests = 0
         for i in range(nframes):
             plain_launch(i)
-            pair_tests += plain.frame_stats(0)["pair_tests"]
         b.record(stream)
         stream.synchronize()
         plain_ms.append(a.elapsed_time(b))
@@ -402,18 +399,28 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
     # small frames, but it runs the same pair tests; if everything but its own
     # occlusion stage took no time, it would run plain_ms / batch_occlusion_ms
     # times faster than the plain loop -- the cap on its speed-up.
-    plain.set_profiling(True)
+    # (Stage times with the unprofiled kernels; the work counters -- pair
+    # tests -- from one more pass of each form with the counting kernel.)
+    plain.set_profiling(fdzb.PROFILE_STAGES)
     p_occ = p_all = 0.0
     for i in range(nframes):
         plain_launch(i)
         st = plain.frame_stats(0)["stage_ms"]
         p_occ += st[4]
         p_all += sum(st)
-    plain.set_profiling(False)
-    bat.set_profiling(True)
+    plain.set_profiling(fdzb.PROFILE_ALL)
+    pair_tests = 0
+    for i in range(nframes):
+        plain_launch(i)
+        pair_tests += plain.frame_stats(0)["pair_tests"]
+    plain.set_profiling(fdzb.PROFILE_OFF)
+    bat.set_profiling(fdzb.PROFILE_STAGES)
     bat.launch(d_batch)
     b_stage = bat.stats()["totals"]["stage_ms"]
-    bat.set_profiling(False)
+    bat.set_profiling(fdzb.PROFILE_ALL)
+    bat.launch(d_batch)
+    bpst = bat.stats()
+    bat.set_profiling(fdzb.PROFILE_OFF)
     bat.launch(d_batch)
     amdahl = {"plain_stage_ms": p_all, "plain_occlusion_ms": p_occ,
               "plain_occlusion_share": p_occ / ms_p, "batch_stage_ms": [round(x, 3) for x in b_stage],
@@ -435,9 +442,9 @@ def batched_workload(fdzb, torch, stream, nframes: int = 64, steps: int = 5) -> 
         "frames_per_s": nframes * 1e3 / ms_b, "ms_per_batch": ms_b,
         "plain_frames_per_s": nframes * 1e3 / ms_p, "plain_ms_per_loop": ms_p,
         "speedup_vs_plain": ms_p / ms_b,
-        "pair_tests_per_s": bst["totals"]["pair_tests"] * 1e3 / ms_b,
+        "pair_tests_per_s": bpst["totals"]["pair_tests"] * 1e3 / ms_b,
         "effective_gpairs_per_s": sxt * 1e3 / ms_b / 1e9,
-        "plain_pair_tests": pair_tests, "batch_pair_tests": bst["totals"]["pair_tests"],
+        "plain_pair_tests": pair_tests, "batch_pair_tests": bpst["totals"]["pair_tests"],
         "masks_identical": bool(same), "graph": bool(bst["from_graph"]),
         "graph_replays": bst["graph_replays"], "kernel_launches_per_batch": bst["totals"]["kernel_launches"],
         "amdahl": amdahl,
@@ -686,6 +693,8 @@ def next_rows_workload(fdzb, torch, stream, reps: int = 3) -> dict:
         if setup:
             setup(ctx)
         ms = _device_ms(torch, stream, lambda: (ctx.launch_async(), ctx.sync()), reps, flush)
+        ctx.set_profiling(True)              # one more launch that counts the work
+        ctx.launch()
         st = ctx.stats()
         ctx.close()
         return ms, st
@@ -872,7 +881,7 @@ def main():
         ctx.launch()
 
     # device-timed frames, inputs resident, L2 flushed before each frame
-    def timed(profile: bool):
+    def timed(profile):
         ctx.set_profiling(profile)
         evs = []
         stats = []
@@ -902,10 +911,16 @@ def main():
     st = stats[-1]
     assert all(s["replans"] == 0 for s in stats), "pair buffer regrown inside the timed region"
 
-    # per-stage times (separate pass with stage events) for the roofline
-    prof_ms, pstats = timed(True)
-    stage = [statistics.mean(s["stage_ms"][i] for s in pstats) for i in range(5)]
+    # per-stage times (separate pass with stage events, the same kernels) for
+    # the roofline; the work counters from one launch of the counting form of
+    # the occlusion kernel (the work is deterministic: the same pair tests,
+    # rows and partial masks every launch)
+    prof_ms, sstats = timed(fdzb.PROFILE_STAGES)
+    stage = [statistics.mean(s["stage_ms"][i] for s in sstats) for i in range(5)]
     occ_ms = stage[4]
+    ctx.set_profiling(fdzb.PROFILE_ALL)
+    ctx.launch()
+    pstats = [ctx.stats()]
     ops = (pstats[-1]["pair_tests"] * OPS_PER_PAIR + pstats[-1]["rows_evaluated"] * OPS_PER_ROW
            + pstats[-1]["partial_masks"] * OPS_PER_PARTIAL)
     alu_peak = fdzb.measure_alu_rate()
@@ -919,6 +934,8 @@ def main():
     ops_off = (so["pair_tests"] * OPS_PER_PAIR + so["rows_evaluated"] * OPS_PER_ROW
                + so["partial_masks"] * OPS_PER_PARTIAL)
     ctx.set_open_box(fdzb.OPEN_BOX_AUTO)
+    ctx.set_profiling(False)
+    pst = pstats[-1]                          # the work counters of a profiled launch
 
     # end to end through the public API with host buffers: every frame uploads
     # its G-buffer (positions + normals) from pinned host memory and reads its
@@ -955,7 +972,7 @@ def main():
                    "W": scene.W, "H": scene.H, "triangles": scene.T, "light_grid": scene.light.n,
                    "bins": scene.bins, "tri_order": "coverage" if args.tri_order else "reference",
                    "l2": "flushed (256 MB write) before every timed frame", "parallelism": f"replicas{args.gpus}"},
-        "pair_tests_per_s": st["pair_tests"] * 1e3 / ms_step * args.gpus,
+        "pair_tests_per_s": pst["pair_tests"] * 1e3 / ms_step * args.gpus,
         "effective_gpairs_per_s": scene.S * scene.T * 1e3 / ms_step * args.gpus / 1e9,
         "stage_ms": dict(zip(fdzb.STAGES, stage)),
         "roofline": {"kernel": "k_occlusion", "bound": "alu", "achieved": achieved / 1e9,
@@ -980,8 +997,8 @@ def main():
         "gpu_launches": st["kernel_launches"] * args.steps,
         "clocks": clocks,
         "frame_stats": {"valid_samples": st["valid_samples"], "pairs": st["num_pairs"],
-                        "pair_tests": st["pair_tests"], "rows_evaluated": st["rows_evaluated"],
-                        "partial_masks": st["partial_masks"]},
+                        "pair_tests": pst["pair_tests"], "rows_evaluated": pst["rows_evaluated"],
+                        "partial_masks": pst["partial_masks"]},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }
     if cpu:

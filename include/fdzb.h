@@ -123,7 +123,8 @@ typedef struct fdzb_frame_stats {
     int32_t num_pairs;         /* triangle/bin pairs */
     int32_t num_bins;
     int32_t pair_capacity;
-    int64_t pair_tests;        /* sample/triangle pairs past the AABB pre-cull */
+    int64_t pair_tests;        /* sample/triangle pairs past the AABB pre-cull (counted with
+                                  profiling on, fdzb_ctx_set_profiling; 0 otherwise) */
     float f;                   /* far plane */
     float sub[2];
     float lp_begin[3], lp_end[3], lp_factor[2];
@@ -133,8 +134,8 @@ typedef struct fdzb_frame_stats {
     int32_t kernel_launches;   /* kernels enqueued by the frame */
     int32_t triangle_passes;   /* 1, or the passes over triangle ranges of a frame whose pairs
                                   exceeded the pair-capacity limit */
-    int64_t rows_evaluated;    /* light-grid rows evaluated by pair tests */
-    int64_t partial_masks;     /* row masks that needed the ceil(-D/B) threshold */
+    int64_t rows_evaluated;    /* light-grid rows evaluated by pair tests (profiling on) */
+    int64_t partial_masks;     /* row masks that needed the ceil(-D/B) threshold (profiling on) */
     float stage_ms[5];         /* with profiling on: setup, sample sort, triangle pairs,
                                   pair sort, occlusion+shading (CUDA events) */
     float pad1;
@@ -216,7 +217,8 @@ enum fdzb_array_id {
     FDZB_ARR_BIN_TRI_END,           /* int32[num_bins] */
     FDZB_ARR_TRI_AABB,              /* float[8*T] (min xyz,1, max xyz,1) */
     FDZB_ARR_WORK_COUNTERS,         /* uint64[7] occlusion work: pair tests, light rows, partial row
-                                       masks, pairs reaching the AABB pre-cull, triangle chunks,
+                                       masks (these three with profiling on), pairs reaching the
+                                       AABB pre-cull, triangle chunks,
                                        compute rounds (these three: counted by the pair-compacting
                                        occlusion kernel only), pairs skipped by the open-box cull */
     FDZB_ARR_COUNT
@@ -261,9 +263,17 @@ int fdzb_ctx_set_occlusion_schedule(fdzb_ctx *ctx, int schedule);
  * for the passes. */
 int fdzb_ctx_set_pair_capacity_limit(fdzb_ctx *ctx, int64_t pairs);
 
-/* Per-stage GPU timing (CUDA events between stages, read back in
- * fdzb_frame_stats.stage_ms); off by default.  The reference times only the whole
- * frame (FS/api.cpp:405-409,574-581). */
+/* Profiling modes.  FDZB_PROFILE_ALL: per-stage GPU timing (CUDA events
+ * between stages, read back in fdzb_frame_stats.stage_ms) and the occlusion
+ * kernel's work counters (pair_tests, rows_evaluated, partial_masks: counted
+ * only in this mode, by a form of the kernel that accumulates them, a few per
+ * cent slower).  FDZB_PROFILE_STAGES: the stage timing alone, with the kernels
+ * that run unprofiled.  Off by default; profiled launches are not replayed
+ * from a CUDA graph.  The reference times only the whole frame
+ * (FS/api.cpp:405-409,574-581). */
+#define FDZB_PROFILE_OFF 0
+#define FDZB_PROFILE_ALL 1
+#define FDZB_PROFILE_STAGES 2
 int fdzb_ctx_set_profiling(fdzb_ctx *ctx, int enable);
 
 /* Measures the FP32 issue rate of the current device (lane operations per second
@@ -470,6 +480,7 @@ int fdzb_batch_destroy(fdzb_batch *batch);
 /* stream: a cudaStream_t; NULL = the batch's own stream. */
 int fdzb_batch_set_stream(fdzb_batch *batch, void *stream);
 int fdzb_batch_set_graph(fdzb_batch *batch, int enable);
+/* Profiling modes as fdzb_ctx_set_profiling (FDZB_PROFILE_*). */
 int fdzb_batch_set_profiling(fdzb_batch *batch, int enable);
 int fdzb_batch_set_tri_order(fdzb_batch *batch, int order);
 int fdzb_batch_set_occlusion_schedule(fdzb_batch *batch, int schedule);
