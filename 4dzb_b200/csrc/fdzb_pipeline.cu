@@ -975,8 +975,11 @@ cudaError_t measure_alu_rate(double *rate)
 }
 
 // ---------------------------------------------------------------------------
-// Self-check of div_by_rcp (the occlusion rows' quotient) against the IEEE
-// division __fdiv_rn, over the operand ranges the pair test admits to it.
+// Self-check of the occlusion rows' quotient.  k_check_reciprocal enumerates
+// every float b with |b| in [2^-100, 2^40) (both signs) and compares
+// rcp_nearest(b) with __frcp_rn(b).  k_check_division compares
+// div_by_rcp(a, b, rcp_nearest(b)) with the IEEE division __fdiv_rn, over
+// the operand ranges the pair test admits to it.
 // Trial t draws (from a counter hash of seed and t) three cases: a and b with
 // random significands and signs, |a| in [2^-61, 2^47] and |b| in
 // [2^-100, 2^39] (quotients outside [2^-100, 2^100] are skipped); a quotient
@@ -1018,7 +1021,7 @@ __global__ void k_check_division(unsigned long long trials, unsigned long long s
             const float aq = fabsf(q);
             if (aq >= 0x1p-100f && aq <= 0x1p100f) {
                 ++n;
-                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+                if (__float_as_uint(div_by_rcp(a, b, rcp_nearest(b))) != __float_as_uint(q)) ++bad;
             }
         }
         // 2. quotients next to a rounding midpoint
@@ -1033,7 +1036,7 @@ __global__ void k_check_division(unsigned long long trials, unsigned long long s
             const float aq = fabsf(q);
             if (aq >= 0x1p-100f && aq <= 0x1p100f && fabsf(a) <= 0x1p47f && fabsf(a) >= 0x1p-61f) {
                 ++n;
-                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+                if (__float_as_uint(div_by_rcp(a, b, rcp_nearest(b))) != __float_as_uint(q)) ++bad;
             }
         }
         // 3. quotients at and next to small integers
@@ -1048,9 +1051,31 @@ __global__ void k_check_division(unsigned long long trials, unsigned long long s
             if ((aq >= 0x1p-100f || q == 0.0f) && aq <= 0x1p100f && fabsf(a) <= 0x1p47f &&
                 (fabsf(a) >= 0x1p-61f || a == 0.0f)) {
                 ++n;
-                if (__float_as_uint(div_by_rcp(a, b, __frcp_rn(b))) != __float_as_uint(q)) ++bad;
+                if (__float_as_uint(div_by_rcp(a, b, rcp_nearest(b))) != __float_as_uint(q)) ++bad;
             }
         }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bad += __shfl_xor_sync(kFullWarp, bad, o);
+        n += __shfl_xor_sync(kFullWarp, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicAdd(mismatches, bad);
+        atomicAdd(checked, n);
+    }
+}
+
+__global__ void k_check_reciprocal(unsigned long long *mismatches, unsigned long long *checked)
+{
+    constexpr unsigned long long kValues = 140ull << 23;   // biased exponents 27 .. 166
+    unsigned long long bad = 0, n = 0;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < kValues;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t bits = ((uint32_t)(27u + (i >> 23)) << 23) | (uint32_t)(i & 0x7FFFFFu);
+        const float b = __uint_as_float(bits), nb = __uint_as_float(bits | 0x80000000u);
+        bad += __float_as_uint(rcp_nearest(b)) != __float_as_uint(__frcp_rn(b));
+        bad += __float_as_uint(rcp_nearest(nb)) != __float_as_uint(__frcp_rn(nb));
+        n += 2;
     }
     for (int o = 16; o > 0; o >>= 1) {
         bad += __shfl_xor_sync(kFullWarp, bad, o);
@@ -1069,6 +1094,7 @@ cudaError_t check_division(unsigned long long trials, unsigned long long seed, u
     cudaError_t e = cudaMalloc(&d, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) return e;
     cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+    k_check_reciprocal<<<sm_count() * 8, 256>>>(d, d + 1);
     k_check_division<<<sm_count() * 8, 256>>>(trials, seed, d, d + 1);
     e = cudaGetLastError();
     unsigned long long h[2] = {0, 0};

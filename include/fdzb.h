@@ -283,12 +283,15 @@ int fdzb_measure_alu_rate(double *lane_ops_per_second);
 
 /* Device self-check of the occlusion kernel's row quotient: -D / B from a
  * hoisted reciprocal RN(1/B) by two Markstein correction steps, which the pair
- * test uses in place of the IEEE division where its operands are in range.
- * Runs `trials` trials of three cases each (random operands over the admitted
+ * test uses in place of the IEEE division where its operands are in range,
+ * the reciprocal itself from the hardware approximation and one
+ * Newton-Raphson step.  Compares that reciprocal with __frcp_rn for every
+ * float of the admitted range (|B| in [2^-100, 2^40), 2.35e9 values), then
+ * runs `trials` trials of three cases each (random operands over the admitted
  * ranges, quotients next to rounding midpoints, quotients at small integers)
- * and returns the number of compared cases and of results that differ from
- * __fdiv_rn in any bit (expected: 0).  No counterpart in the reference, whose
- * rows divide directly (K/Step5_2_shadowCalPerSample.inl:20). */
+ * against __fdiv_rn; returns the number of compared values and of results
+ * that differ in any bit (expected: 0).  No counterpart in the reference,
+ * whose rows divide directly (K/Step5_2_shadowCalPerSample.inl:20). */
 int fdzb_check_division(uint64_t trials, uint64_t seed, uint64_t *mismatches, uint64_t *checked);
 
 /* Host-side light setup only (FS/api.cpp:303-400): fills the 16-float
