@@ -403,7 +403,9 @@ class Context:
         _check(self._lib.fdzb_ctx_set_backface_cull(self._h, int(bool(enable))))
 
     def set_debug(self, flags: int) -> None:
-        """flags bit 0: keep pre-sort copies of the key arrays for export()."""
+        """flags bit 0 (DEBUG_COPIES): keep pre-sort copies of the key arrays for
+        export(); bit 1 (DEBUG_SEPARATE_PAIRS): triangle/bin pairs as separate
+        key and value arrays even where one word would hold a pair."""
         _check(self._lib.fdzb_ctx_set_debug(self._h, int(flags)))
 
     def set_profiling(self, enable) -> None:
@@ -612,8 +614,11 @@ def upload_scene(scene, device: str = "cuda"):
     return pos, nrm, vtx, idx
 
 
+DEBUG_COPIES, DEBUG_SEPARATE_PAIRS = 1, 2
+
+
 def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bool = False,
-                      tri_order: Optional[int] = None):
+                      tri_order: Optional[int] = None, separate_pairs: bool = False):
     """A Context with the scene's buffers uploaded and outputs allocated.
     Returns (ctx, tensors dict)."""
     import torch
@@ -622,8 +627,8 @@ def context_for_scene(scene, device: str = "cuda", masks: bool = True, debug: bo
     mk = (torch.empty(scene.S * mask_words(scene.light.n, scene.light.cols), dtype=torch.int32, device=device)
           if masks else None)
     ctx = Context()
-    if debug:
-        ctx.set_debug(1)
+    if debug or separate_pairs:
+        ctx.set_debug((DEBUG_COPIES if debug else 0) | (DEBUG_SEPARATE_PAIRS if separate_pairs else 0))
     if tri_order is not None:
         ctx.set_tri_order(tri_order)
     ctx.set_view(scene.W, scene.H)

@@ -369,6 +369,19 @@ int engine_enqueue(Engine &e)
     b.depthBits = e.triOrder == FDZB_TRI_ORDER_COVERAGE ? kCoverageBucketBits : 0;
     b.triPasses = b.depthBits ? fdzb::sort_passes_for(1ll << b.depthBits) : 0;
     b.pairPasses = fdzb::sort_passes_for(NB);
+    // A pair is one word, bin << triBits | triangle, when the bin and triangle
+    // numbers fit 32 bits together (the HD frame: 14 + 18): the pair sort then
+    // moves keys alone, half the bytes and instructions of a key/value sort,
+    // on the same digits (bits triBits and up), and keeps the same order.
+    {
+        auto bitsFor = [](long long n) {
+            int k = 1;
+            while (k < 32 && (1ll << k) < n) ++k;
+            return k;
+        };
+        const int binBits = bitsFor((long long)NB), triBits = bitsFor((long long)T);
+        b.pairTriBits = (!e.separatePairs && binBits + triBits <= 32) ? triBits : 0;
+    }
     int sb = 0, tb = 0, bb = 0;
     for (int i = 0; i < nf; ++i) {
         const FrameSpec &s = e.frames[i];
@@ -419,7 +432,7 @@ int engine_enqueue(Engine &e)
         k.NB = (int)NB;
         k.P = (int)e.pairCapacity;
         k.sp = b.samplePasses;
-        k.pp = b.pairPasses;
+        k.pp = b.pairPasses + 16 * b.pairTriBits;
         k.db = b.depthBits;
         k.maxS = maxS;
         k.maxT = maxT;
@@ -1056,6 +1069,7 @@ int fdzb_ctx_set_debug(fdzb_ctx *c, int flags)
 {
     if (int rc = ctx_check(c)) return rc;
     c->eng.debug = flags & 1;
+    c->eng.separatePairs = (flags & 2) != 0;
     return FDZB_OK;
 }
 
@@ -1385,18 +1399,28 @@ int fdzb_ctx_export(fdzb_ctx *c, int what, void *dst, size_t bytes)
     }
     case FDZB_ARR_TRI_COUNT: src = b.triCount; avail = 4 * T; break;
     case FDZB_ARR_PAIR_BIN:
-    case FDZB_ARR_SORTED_PAIR_BIN: {
-        // pair keys are the global bins
-        const uint32_t *s2 = what == FDZB_ARR_PAIR_BIN ? b.dbgPKeys : (pOdd ? b.pkeysB : b.pkeysA);
+    case FDZB_ARR_SORTED_PAIR_BIN:
+    case FDZB_ARR_PAIR_TRI:
+    case FDZB_ARR_SORTED_PAIR_TRI: {
+        // pair keys are the global bins, values the triangles -- or one word
+        // bin << pairTriBits | triangle each
+        const bool pre = what == FDZB_ARR_PAIR_BIN || what == FDZB_ARR_PAIR_TRI;
+        const bool wantBin = what == FDZB_ARR_PAIR_BIN || what == FDZB_ARR_SORTED_PAIR_BIN;
+        const int tb = b.pairTriBits;
+        const uint32_t *s2 = nullptr;
+        if (tb || wantBin) s2 = pre ? b.dbgPKeys : (pOdd ? b.pkeysB : b.pkeysA);
+        else s2 = pre ? b.dbgPVals : (pOdd ? b.pvalsB : b.pvalsA);
         if (!s2) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
         if (bytes > 4 * P) return fail(FDZB_ERR_INVALID_ARG, "export size exceeds the array");
-        if (bytes) FDZB_CUDA(cudaMemcpy(dst, s2, bytes, cudaMemcpyDeviceToHost));
+        if (!bytes) return FDZB_OK;
+        FDZB_CUDA(cudaMemcpy(dst, s2, bytes, cudaMemcpyDeviceToHost));
+        if (tb) {
+            uint32_t *o = (uint32_t *)dst;
+            const uint32_t mask = (1u << tb) - 1u;
+            for (size_t i = 0; i < bytes / 4; ++i) o[i] = wantBin ? (o[i] >> tb) : (o[i] & mask);
+        }
         return FDZB_OK;
     }
-    case FDZB_ARR_PAIR_TRI:
-        if (!b.dbgPVals) return fail(FDZB_ERR_NOT_READY, "pre-sort arrays need fdzb_ctx_set_debug(ctx, 1)");
-        src = b.dbgPVals; avail = 4 * P; break;
-    case FDZB_ARR_SORTED_PAIR_TRI: src = pOdd ? b.pvalsB : b.pvalsA; avail = 4 * P; break;
     case FDZB_ARR_BIN_TRI_START: src = b.binTriStart; avail = 4 * NB; break;
     case FDZB_ARR_BIN_TRI_END: src = b.binTriEnd; avail = 4 * NB; break;
     case FDZB_ARR_TRI_AABB: {

@@ -60,6 +60,7 @@ struct Engine {
     DeviceBuffers buf{};
     long long pairCapacity = 0;
     int debug = 0;  // keep pre-sort copies for export
+    bool separatePairs = false;  // pairs as key/value arrays even where one word would hold them
     int triOrder = FDZB_TRI_ORDER_COVERAGE;
     bool profile = false;  // record events at the stage boundaries
     bool countWork = false;  // with profile: the occlusion kernel form that counts its work

@@ -139,6 +139,7 @@ struct DeviceBuffers {
     int itemCapacity;
     // sorted data lands in the A buffers after an even number of passes, B after odd
     int samplePasses, pairPasses, triPasses;
+    int pairTriBits;                            // > 0: pairs are words bin << pairTriBits | triangle
     int depthBits;                              // coverage-bucket bits of the triangle order (0:
                                                 // the reference's order, no triangle sort)
     int occVariant;                             // 0: k_occlusion (lane per sample), 1: k_occlusion_pairs

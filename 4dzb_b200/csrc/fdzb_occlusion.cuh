@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
                 const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
                 const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
                 const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
-                const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
+                const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri, uint32_t triMask,
                 const float4 *__restrict__ rec, const float4 *__restrict__ prjRec, int totalTris, int totalBins,
                 int nframes)
 {
@@ -820,7 +820,7 @@ __global__ void __launch_bounds__(RowWord<R>::kWarps * 32, RowWord<R>::kMinBlock
             if (lane < m) {
                 int off = cur + lane;
                 if (off >= nT) off -= nT;
-                int tri = (int)pairTri[tS + off];
+                int tri = (int)(pairTri[tS + off] & triMask);
                 if ((unsigned)tri >= (unsigned)totalTris) {
                     atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
                     tri = 0;
@@ -1039,7 +1039,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
                       const int4 *__restrict__ items, int itemCapacity, Counters *ctr,
                       const uint32_t *__restrict__ sortedVals, const int32_t *__restrict__ bss,
                       const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
-                      const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri,
+                      const int32_t *__restrict__ bte, const uint32_t *__restrict__ pairTri, uint32_t triMask,
                       const float4 *__restrict__ rec, const float4 *__restrict__ /* prjRec */, int totalTris,
                       int totalBins, int nframes)
 {
@@ -1121,7 +1121,7 @@ __global__ void __launch_bounds__(kOccThreads, FDZB_OCC2_MINBLOCKS)
             const int m = min(kOccChunk, nT - base);
             __syncwarp();
             if (lane < m) {
-                int tri = (int)pairTri[tS + base + lane];
+                int tri = (int)(pairTri[tS + base + lane] & triMask);
                 if ((unsigned)tri >= (unsigned)totalTris) {
                     atomicOr(&ctr->errorFlags, (int)ERR_INTERNAL);
                     tri = 0;

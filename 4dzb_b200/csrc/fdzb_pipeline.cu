@@ -523,11 +523,13 @@ __global__ void k_tri_order(const FrameState *__restrict__ states, const int *__
 }
 
 // Candidate bins of a triangle, swept by a warp 32 at a time in row-major
-// order; returns the number accepted and, with write != nullptr, writes the
-// accepted (bin, triangle) pairs from position `pos` on, in order.
+// order; returns the number accepted and, with write, writes the accepted
+// (bin, triangle) pairs from position `pos` on, in order: as (key = bin,
+// value = triangle), or, with triBits > 0, as the one word
+// bin << triBits | triangle.
 __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, const TriBins &c, int bb, int l2,
                                           int lane, uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals,
-                                          unsigned long long pos, int capacity, int g, bool write)
+                                          unsigned long long pos, int capacity, int g, bool write, int triBits)
 {
     const int w = c.cex - c.cbx, h = c.cey - c.cby;
     if (w <= 0 || h <= 0) return 0;
@@ -548,8 +550,12 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
         if (write && ok) {
             const unsigned long long p = pos + (unsigned long long)total + (unsigned)__popc(m & lanemask_lt());
             if (p < (unsigned long long)capacity) {
-                pkeys[p] = (uint32_t)gb;
-                pvals[p] = (uint32_t)g;
+                if (triBits) {
+                    pkeys[p] = ((uint32_t)gb << triBits) | (uint32_t)g;
+                } else {
+                    pkeys[p] = (uint32_t)gb;
+                    pvals[p] = (uint32_t)g;
+                }
             }
         }
         total += __popc(m);
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(kTriThreads)
                 const float4 *__restrict__ rec, const uint32_t *__restrict__ binStat,
                 int32_t *__restrict__ triCount, unsigned long long *scanStatus, const uint32_t *epochWord,
                 uint32_t *__restrict__ pkeys, uint32_t *__restrict__ pvals, int capacity,
-                const uint32_t *__restrict__ order, Counters *ctr)
+                const uint32_t *__restrict__ order, int triBits, Counters *ctr)
 {
     constexpr int WARPS = kTriThreads / 32;
     __shared__ int s_tile;
@@ -640,7 +646,7 @@ __global__ void __launch_bounds__(kTriThreads)
             take(j, c, g, bb, l2);
             int cnt = 0;
             if (g >= 0) {
-                if (c.any) cnt = sweep_bins(binStat, c, bb, l2, lane, pkeys, pvals, 0, capacity, g, false);
+                if (c.any) cnt = sweep_bins(binStat, c, bb, l2, lane, pkeys, pvals, 0, capacity, g, false, triBits);
                 if (lane == 0) triCount[g] = cnt;
             }
             if (lane == 0) s_cnt[k] = cnt;
@@ -709,7 +715,7 @@ __global__ void __launch_bounds__(kTriThreads)
             take(j, c, g, bb, l2);
             if (g < 0 || !c.any) continue;
             sweep_bins(binStat, c, bb, l2, lane, pkeys, pvals, tileBase + (unsigned long long)s_cnt[k], capacity, g,
-                       true);
+                       true, triBits);
         }
     }
 }
@@ -771,25 +777,46 @@ static int grid_for(long long n, int threads, int cap)
     return (int)g;
 }
 
+// Keys-only passes (packed pairs): 64 registers, so 4 blocks of 256 threads
+// per SM (pair sort at HD 0.353 -> 0.343 ms; 5 blocks spill, 6144-key tiles
+// spill and gain nothing).
+#ifndef FDZB_SORTK_ITEMS
+#define FDZB_SORTK_ITEMS 16
+#endif
+#ifndef FDZB_SORTK_MINBLOCKS
+#define FDZB_SORTK_MINBLOCKS 4
+#endif
+constexpr int kKeysItems = FDZB_SORTK_ITEMS, kKeysMinBlocks = FDZB_SORTK_MINBLOCKS;
+constexpr int kKeysTile = kSortThreads * kKeysItems;
+static_assert(kKeysTile >= kSortTile, "the look-back status array is sized for tiles of kSortTile keys");
+
 // Sorts (kA, vA) with kB/vB as ping-pong buffers; `slot` selects the histogram
 // and ticket block (0 samples, 1 pairs, 2 triangles).  Pass p uses tag
-// 16*launch + 4*slot + p.
+// 16*launch + 4*slot + p and the key's bits [shift0 + 8p, shift0 + 8p + 8).
+// vA == nullptr: keys alone.
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
-                     cudaStream_t s)
+                     cudaStream_t s, int shift0 = 0)
 {
     uint32_t *hist = b.sortHist + slot * 4 * kRadix;
     k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
-                                                                              cap, passes, hist);
+                                                                              cap, passes, shift0, hist);
     uint32_t *ki = kA, *vi = vA, *ko = kB, *vo = vB;
     const long long tiles = ((long long)cap + kSortTile - 1) / kSortTile;
     const int passGrid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
+    const long long keysTiles = ((long long)cap + kKeysTile - 1) / kKeysTile;
+    const int keysGrid = grid_for(keysTiles * kSortThreads, kSortThreads, sm * kKeysMinBlocks);
     for (int p = 0; p < passes; ++p) {
-        k_radix_pass<<<passGrid, kSortThreads, 0, s>>>(ki, vi, ko, vo, n_dev, n_static, cap, 8 * p,
-                                                       hist + p * kRadix, b.sortStatus, b.epochWord,
-                                                       (uint32_t)(slot * 4 + p),
-                                                       b.counters->sortTileCounter + slot * 4 + p,
-                                                       &b.counters->errorFlags);
+        if (vA)
+            k_radix_pass<true><<<passGrid, kSortThreads, 0, s>>>(
+                ki, vi, ko, vo, n_dev, n_static, cap, shift0 + 8 * p, hist + p * kRadix, b.sortStatus,
+                b.epochWord, (uint32_t)(slot * 4 + p), b.counters->sortTileCounter + slot * 4 + p,
+                &b.counters->errorFlags);
+        else
+            k_radix_pass<false, kKeysItems, kKeysMinBlocks><<<keysGrid, kSortThreads, 0, s>>>(
+                ki, nullptr, ko, nullptr, n_dev, n_static, cap, shift0 + 8 * p, hist + p * kRadix, b.sortStatus,
+                b.epochWord, (uint32_t)(slot * 4 + p), b.counters->sortTileCounter + slot * 4 + p,
+                &b.counters->errorFlags);
         uint32_t *t = ki;
         ki = ko;
         ko = t;
@@ -867,21 +894,26 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
                                                  b.triRec, b.binStat, b.triCount, b.triScanStatus,
                                                  b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 order, b.counters);
+                                                 order, b.pairTriBits, b.counters);
         nl += 1;
     }
     if (b.dbgPKeys) {
         cudaMemcpyAsync(b.dbgPKeys, b.pkeysA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(b.dbgPVals, b.pvalsA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
+        if (!b.pairTriBits)
+            cudaMemcpyAsync(b.dbgPVals, b.pvalsA, 4ull * b.pairCapacity, cudaMemcpyDeviceToDevice, s);
     }
     // (b) pair sort and segments
     if (ev) cudaEventRecord(ev[STAGE_PAIR_SORT], s);
-    run_sort(b, 1, b.pkeysA, b.pvalsA, b.pkeysB, b.pvalsB, &b.counters->pairCount, 0, b.pairCapacity,
-             b.pairPasses, sm, s);
+    // packed pairs (pairTriBits > 0): the keys alone are sorted on their bin
+    // bits, and the sorted keys are the triangle lists
+    const bool packed = b.pairTriBits > 0;
+    run_sort(b, 1, b.pkeysA, packed ? nullptr : b.pvalsA, b.pkeysB, packed ? nullptr : b.pvalsB,
+             &b.counters->pairCount, 0, b.pairCapacity, b.pairPasses, sm, s, b.pairTriBits);
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
-    uint32_t *pv = (b.pairPasses & 1) ? b.pvalsB : b.pvalsA;
+    uint32_t *pv = packed ? pk : ((b.pairPasses & 1) ? b.pvalsB : b.pvalsA);
+    const uint32_t triMask = packed ? (1u << b.pairTriBits) - 1u : 0xFFFFFFFFu;
     k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
-        pk, &b.counters->pairCount, 0, b.pairCapacity, 0, b.binTriStart, b.binTriEnd,
+        pk, &b.counters->pairCount, 0, b.pairCapacity, b.pairTriBits, b.binTriStart, b.binTriEnd,
         (uint32_t)b.totalBins, &b.counters->errorFlags);
     nl += 2 + b.pairPasses;
     // (c) + (d) occlusion and shading
@@ -896,7 +928,7 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     const int g32 = sm * FDZB_OCC_MINBLOCKS, g64 = sm * W64::kMinBlocks, t64 = W64::kWarps * 32;
 #define FDZB_OCC_ARGS                                                                                        \
     b.frames, b.states, b.items, b.itemCapacity, b.counters, sv, b.binSampleStart, b.binSampleEnd, b.binTriStart, \
-        b.binTriEnd, pv, b.triRec, b.triPrj, b.totalTris, b.totalBins, nf
+        b.binTriEnd, pv, triMask, b.triRec, b.triPrj, b.totalTris, b.totalBins, nf
     // b.openBox: the open-box cull's instantiation (edge-function masks only);
     // b.countWork: the instantiation that accumulates the work counters
 #define FDZB_OCC(RC, RT, DP, BX, G, T)                                                                        \
@@ -1219,7 +1251,7 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
     if (n > 0) {
         const int sm = sm_count();
         k_radix_hist<<<grid_for(n, kSortThreads, sm * 4), kSortThreads, 0, s>>>(d_keys_in, nullptr, n, n,
-                                                                                  passes, hist);
+                                                                                  passes, 0, hist);
         // destinations alternate so that the last pass lands in the outputs
         const int grid = grid_for(tiles * kSortThreads, kSortThreads, sm * 4);
         const uint32_t *ki = d_keys_in, *vi = d_vals_in;
@@ -1229,7 +1261,7 @@ extern "C" int fdzb_sort_pairs_noalloc(const uint32_t *d_keys_in, const uint32_t
             uint32_t *vo = toOut ? d_vals_out : tmpV;
             // tag p + 1: the cleared words (tag 0) and the words of this call's
             // earlier passes both read as unpublished
-            k_radix_pass<<<grid, kSortThreads, 0, s>>>(ki, vi, ko, vo, nullptr, n, n, 8 * p,
+            k_radix_pass<true><<<grid, kSortThreads, 0, s>>>(ki, vi, ko, vo, nullptr, n, n, 8 * p,
                                                        hist + p * kRadix, status, nullptr, (uint32_t)p + 1u,
                                                        tickets + p, err);
             ki = ko;

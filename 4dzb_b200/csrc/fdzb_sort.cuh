@@ -38,10 +38,11 @@ __device__ __forceinline__ int sort_count(const int *n_dev, int n_static, int ca
     return n < cap ? n : cap;
 }
 
-// hist[p * 256 + digit] += count, for passes p < passes.
+// hist[p * 256 + digit] += count, for passes p < passes; pass p's digit is
+// bits [shift0 + 8p, shift0 + 8p + 8) of the key.
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_hist(const uint32_t *__restrict__ keys, const int *n_dev, int n_static, int cap,
-                 int passes, uint32_t *__restrict__ hist)
+                 int passes, int shift0, uint32_t *__restrict__ hist)
 {
     __shared__ uint32_t s_hist[4 * kRadix];
     const int n = sort_count(n_dev, n_static, cap);
@@ -49,7 +50,7 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t k = keys[i];
-        for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p * kRadix + ((k >> (8 * p)) & 255u)], 1u);
+        for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p * kRadix + ((k >> (shift0 + 8 * p)) & 255u)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x)
@@ -57,7 +58,10 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 // One digit pass.  status: [tiles * 256] zeroed before the pass; ticket zeroed.
-__global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
+// KV = false sorts keys alone (vin and vout unused): the pairs' keys can carry
+// their value in the bits below the digits.
+template <bool KV, int ITEMS = kSortItems, int MINB = FDZB_SORT_MINBLOCKS>
+__global__ void __launch_bounds__(kSortThreads, MINB)
     k_radix_pass(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                  uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, const int *n_dev,
                  int n_static, int cap, int shift, const uint32_t *__restrict__ hist,
@@ -65,13 +69,14 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
                  int *err)
 {
     constexpr int WARPS = kSortThreads / 32;
+    constexpr int TILE = kSortThreads * ITEMS;
     __shared__ uint32_t s_start[kRadix];
     __shared__ uint32_t s_whist[WARPS][kRadix];
     __shared__ uint32_t s_base[kRadix];
     __shared__ uint32_t s_tstart[kRadix];
     __shared__ uint32_t s_scan[WARPS];
-    __shared__ uint32_t s_k[kSortTile];
-    __shared__ uint32_t s_v[kSortTile];
+    __shared__ uint32_t s_k[TILE];
+    __shared__ uint32_t s_v[KV ? TILE : 1];
     __shared__ int s_tile;
 
     const int n = sort_count(n_dev, n_static, cap);
@@ -102,20 +107,20 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
         for (int i = tid; i < WARPS * kRadix; i += kSortThreads) (&s_whist[0][0])[i] = 0;
         __syncthreads();
         const int tile = s_tile;
-        if ((long long)tile * kSortTile >= n) break;
-        const int tileN = min(kSortTile, n - tile * kSortTile);
+        if ((long long)tile * TILE >= n) break;
+        const int tileN = min(TILE, n - tile * TILE);
 
-        const int base = tile * kSortTile + warp * (kSortItems * 32);
-        uint32_t k[kSortItems], v[kSortItems], rk[kSortItems];
+        const int base = tile * TILE + warp * (ITEMS * 32);
+        uint32_t k[ITEMS], v[ITEMS], rk[ITEMS];
 #pragma unroll
-        for (int i = 0; i < kSortItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             const int idx = base + i * 32 + lane;
             const bool ok = idx < n;
             k[i] = ok ? kin[idx] : 0u;
-            v[i] = ok ? vin[idx] : 0u;
+            v[i] = (KV && ok) ? vin[idx] : 0u;
         }
 #pragma unroll
-        for (int i = 0; i < kSortItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             const int idx = base + i * 32 + lane;
             const bool ok = idx < n;
             const uint32_t d = ok ? ((k[i] >> shift) & 255u) : 256u;
@@ -182,13 +187,13 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
 
         // reorder the tile by digit in shared memory (stable)
 #pragma unroll
-        for (int i = 0; i < kSortItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             const int idx = base + i * 32 + lane;
             if (idx < n) {
                 const uint32_t d = (k[i] >> shift) & 255u;
                 const uint32_t lp = s_tstart[d] + s_whist[warp][d] + rk[i];
                 s_k[lp] = k[i];
-                s_v[lp] = v[i];
+                if (KV) s_v[lp] = v[i];
             }
         }
         __syncthreads();
@@ -199,7 +204,7 @@ __global__ void __launch_bounds__(kSortThreads, FDZB_SORT_MINBLOCKS)
             const uint32_t dst = s_base[d] + ((uint32_t)j - s_tstart[d]);
             if (dst < (uint32_t)cap) {
                 kout[dst] = kk;
-                vout[dst] = s_v[j];
+                if (KV) vout[dst] = s_v[j];
             }
         }
     }

@@ -226,7 +226,10 @@ enum fdzb_array_id {
 int fdzb_ctx_export(fdzb_ctx *ctx, int what, void *dst, size_t bytes);
 /* flags bit 0: keep copies of the pre-sort key/value arrays (FDZB_ARR_SAMPLE_KEYS,
  * FDZB_ARR_PAIR_BIN, FDZB_ARR_PAIR_TRI) at the cost of two extra device copies per
- * sort.  Off by default. */
+ * sort.  Bit 1: keep triangle/bin pairs as separate key and value arrays even
+ * where one 32-bit word (bin << b | triangle) would hold a pair -- the packed
+ * form sorts keys alone; both give the same lists (this switch exists to test
+ * both).  Off by default. */
 int fdzb_ctx_set_debug(fdzb_ctx *ctx, int flags);
 
 /* Order of each bin's triangle list (no counterpart in the reference, whose

@@ -11,13 +11,15 @@ import numpy as np
 import oracle
 
 
-def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0):
+def run_gpu(scene, masks: bool = True, tri_order: int = 0, schedule: int = 0, separate_pairs: bool = False):
     """One frame through the library's public Context API; returns
     (outputs dict, stats dict, exported intermediates dict).  tri_order 0 is the
     reference's per-bin triangle order, 1 the coverage order; schedule selects the
-    occlusion kernel's warp schedule."""
+    occlusion kernel's warp schedule; separate_pairs keeps the triangle/bin
+    pairs as key and value arrays where one word would hold them."""
     fdzb = importlib.import_module("4dzb_b200")
-    ctx, t = fdzb.context_for_scene(scene, masks=masks, debug=True, tri_order=tri_order)
+    ctx, t = fdzb.context_for_scene(scene, masks=masks, debug=True, tri_order=tri_order,
+                                    separate_pairs=separate_pairs)
     ctx.set_occlusion_schedule(schedule)
     ms = ctx.launch()
     res = collect(ctx, t, scene, ms=ms, tri_order=tri_order)

@@ -19,9 +19,10 @@ pytestmark = pytest.mark.gpu
 ORDERS = [0, 1]
 
 
-def _check(scene, tri_order=0, occ_stride=1, schedule=0):
+def _check(scene, tri_order=0, occ_stride=1, schedule=0, separate_pairs=False):
     orc = oracle.frame(scene, occ_stride=occ_stride)
-    errs = parity.compare(scene, gpu=parity.run_gpu(scene, tri_order=tri_order, schedule=schedule), orc=orc)
+    errs = parity.compare(scene, gpu=parity.run_gpu(scene, tri_order=tri_order, schedule=schedule,
+                                                    separate_pairs=separate_pairs), orc=orc)
     assert not errs, "\n".join(errs)
 
 
@@ -29,6 +30,14 @@ def _check(scene, tri_order=0, occ_stride=1, schedule=0):
 @pytest.mark.parametrize("order", ORDERS)
 def test_small_preset(cuda_ok, scenes, cull, order):
     _check(scenes.preset("small", cull=cull), order)
+
+
+# Pairs as one word (bin << triangle bits | triangle, where they fit 32 bits:
+# every scene above) and as separate key and value arrays: the same lists.
+@pytest.mark.parametrize("order", ORDERS)
+def test_separate_pair_arrays(cuda_ok, scenes, order):
+    _check(scenes.preset("small"), order, separate_pairs=True)
+    _check(scenes.make_scene(300, 170, 2000, n=16, bins=64, seed=11, sigma=0.1), order, separate_pairs=True)
 
 
 @pytest.mark.parametrize("n,bins", [(8, 16), (16, 32), (32, 64), (4, 8), (12, 32), (1, 16), (2, 1)])
