@@ -366,8 +366,10 @@ __global__ void __launch_bounds__(256)
                     ey0 = __fsub_rn(__fadd_rn(r.y, __fdiv_rn(RFy, r.z)), suby);
                     w = r.z;
                     if (!((bx0 > ex0 || by0 > ey0) || (bx0 < Bx || by0 < By || ex0 > Ex || ey0 > Ey))) {
-                        const float cx = __fdiv_rn(__fadd_rn(ex0, bx0), 2.0f);
-                        const float cy = __fdiv_rn(__fadd_rn(ey0, by0), 2.0f);
+                        // (e + b) / 2 of the reference: halving is exact, so the
+                        // product by 0.5 is the same correctly rounded value
+                        const float cx = __fmul_rn(__fadd_rn(ex0, bx0), 0.5f);
+                        const float cy = __fmul_rn(__fadd_rn(ey0, by0), 0.5f);
                         const int bxi = __float2int_rz(floorf(__fmul_rn(__fsub_rn(cx, Bx), fx)));
                         const int byi = __float2int_rz(floorf(__fmul_rn(__fsub_rn(cy, By), fy)));
                         if (bxi >= 0 && bxi < fr.Wb && byi >= 0 && byi < fr.Wb) {
