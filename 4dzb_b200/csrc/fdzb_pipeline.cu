@@ -442,6 +442,7 @@ __global__ void __launch_bounds__(256)
 // (:184-202) with the counting predicate used for both passes.
 // ---------------------------------------------------------------------------
 constexpr int kTriThreads = 256;
+constexpr int kTriTile = 64;   // triangles per pair-scan tile
 // Look-back status word of a triangle tile: [63:32] launch epoch, [31:30] flag,
 // [29:0] pair count (the pair capacity stays below 2^30).
 constexpr unsigned long long kScanAgg = 1ull << 30;
@@ -571,13 +572,14 @@ __device__ __forceinline__ int sweep_bins(const uint32_t *__restrict__ binStat, 
     return total;
 }
 
-// k_tri_pairs: persistent tiles of kTriThreads triangles; a warp takes the
+// k_tri_pairs: persistent tiles of TILE triangles; a warp takes the
 // tile's triangles in turn (warp w: triangles w, w + 8, ...) and sweeps each
 // one's candidate bins with its 32 lanes.  Count pass, block scan of the
 // per-triangle counts, decoupled look-back over tiles for the tile's global
 // offset, then the write pass in the same order: pairs come out in triangle
 // order, bins row-major -- the reference's layout.  With `order` (the coverage
 // order) the i-th triangle processed is order[i] instead of i.
+template <int TILE>
 __global__ void __launch_bounds__(kTriThreads)
     k_tri_pairs(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ states,
                 const int *__restrict__ triBases, int nframes, int totalTris,
@@ -587,12 +589,14 @@ __global__ void __launch_bounds__(kTriThreads)
                 const uint32_t *__restrict__ order, int triBits, Counters *ctr)
 {
     constexpr int WARPS = kTriThreads / 32;
+    constexpr int TPW = TILE / WARPS;   // triangles per warp and tile
+    static_assert(TILE % WARPS == 0 && TPW <= 32 && TILE <= kTriThreads, "tile of 8..256 triangles");
     __shared__ int s_tile;
-    __shared__ int s_cnt[kTriThreads];
+    __shared__ int s_cnt[TILE];
     __shared__ unsigned long long s_wsum[WARPS];
     __shared__ unsigned long long s_excl;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ntiles = (totalTris + kTriThreads - 1) / kTriThreads;
+    const int ntiles = (totalTris + TILE - 1) / TILE;
     const uint32_t epoch = *epochWord;
     for (;;) {
         __syncthreads();
@@ -600,16 +604,16 @@ __global__ void __launch_bounds__(kTriThreads)
         __syncthreads();
         const int tile = s_tile;
         if (tile >= ntiles) break;
-        const int t0 = tile * kTriThreads;
-        // Each lane prepares one of the warp's 32 triangles of the tile
-        // (k = warp + 8 lane): order, record and candidate bins are loaded for
-        // all 32 at once, and the sweeps take them from the owning lane.
+        const int t0 = tile * TILE;
+        // Each of the first TPW lanes prepares one of the warp's triangles of
+        // the tile (k = warp + 8 lane): order, record and candidate bins are
+        // loaded for all at once, and the sweeps take them from the owning lane.
         TriBins myC;
         myC.any = false;
         myC.cbx = myC.cby = myC.cex = myC.cey = 0;
         myC.bx = myC.by = myC.bz = myC.ex = myC.ey = 0.0f;
         int myG = -1, myBB = 0, myL2 = 0;
-        {
+        if (lane < TPW) {
             const int i = t0 + warp + WARPS * lane;
             const int g = (order && i < totalTris) ? (int)order[i] : i;
             if (i < totalTris && (unsigned)g < (unsigned)totalTris) {
@@ -641,7 +645,7 @@ __global__ void __launch_bounds__(kTriThreads)
             l2 = __shfl_sync(kFullWarp, myL2, j);
         };
         // count pass: warp per triangle
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < TPW; ++j) {
             const int k = warp + WARPS * j;
             TriBins c;
             int g, bb, l2;
@@ -655,7 +659,7 @@ __global__ void __launch_bounds__(kTriThreads)
         }
         __syncthreads();
         // block inclusive scan of the per-triangle counts (thread tid holds triangle tid)
-        const int cnt = s_cnt[tid];
+        const int cnt = tid < TILE ? s_cnt[tid] : 0;
         unsigned long long x = (unsigned long long)cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -671,7 +675,8 @@ __global__ void __launch_bounds__(kTriThreads)
         }
         const unsigned long long mine_excl = wbase + x - (unsigned long long)cnt;
         __syncthreads();
-        s_cnt[tid] = (int)min(mine_excl, (unsigned long long)0x7fffffff);   // now: exclusive offset in the tile
+        if (tid < TILE)
+            s_cnt[tid] = (int)min(mine_excl, (unsigned long long)0x7fffffff);   // now: exclusive offset in the tile
         if (tid == 0) {
             unsigned long long excl = 0;
             unsigned long long *my = scanStatus + tile;
@@ -710,7 +715,7 @@ __global__ void __launch_bounds__(kTriThreads)
         __syncthreads();
         // write pass, same order
         const unsigned long long tileBase = s_excl;
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < TPW; ++j) {
             const int k = warp + WARPS * j;
             TriBins c;
             int g, bb, l2;
@@ -761,7 +766,7 @@ cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cu
 // Host driver.
 // ---------------------------------------------------------------------------
 static_assert(kSortTileHost == kSortTile, "sort tile mismatch");
-static_assert(kTriTileHost == kTriThreads, "triangle tile mismatch");
+static_assert(kTriTileHost == kTriTile, "pair-scan tile mismatch");
 
 int sort_passes_for(long long keyRangeExclusive)
 {
@@ -889,14 +894,17 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         nl += 2 + b.triPasses;
     }
     {
-        const int tiles = (b.totalTris + kTriThreads - 1) / kTriThreads;
-        // up to 8 blocks per SM: the sweeps wait on bin-statistics loads, so
-        // more resident warps hide more of that latency (40 registers: 6 fit)
+        // tiles of 64 triangles, 8 a warp: a frame of few triangles still
+        // spreads over the SMs (2k triangles: pairs 0.159 -> 0.074 ms against
+        // tiles of 256; HD: 0.305 -> 0.283 ms); up to 8 blocks per SM (the
+        // sweeps wait on bin-statistics loads, so more resident warps hide more
+        // of that latency)
+        const int tiles = (b.totalTris + kTriTile - 1) / kTriTile;
         const int grid = tiles < sm * 8 ? (tiles > 0 ? tiles : 1) : sm * 8;
-        k_tri_pairs<<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
-                                                 b.triRec, b.binStat, b.triCount, b.triScanStatus,
-                                                 b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                 order, b.pairTriBits, b.counters);
+        k_tri_pairs<kTriTile><<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
+                                                           b.triRec, b.binStat, b.triCount, b.triScanStatus,
+                                                           b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
+                                                           order, b.pairTriBits, b.counters);
         nl += 1;
     }
     if (b.dbgPKeys) {
