@@ -179,7 +179,7 @@ cudaError_t run_move_model(float *vtx, int vstride, int V, const float m[16], cu
 #define FDZB_SORT_ITEMS 16
 #endif
 constexpr int kSortTileHost = 256 * FDZB_SORT_ITEMS;   // keys per radix-sort tile (fdzb_sort.cuh)
-constexpr int kTriTileHost = 64;      // triangles per pair-scan tile
+constexpr int kTriTileHost = 64;      // triangles per pair-scan tile (the smaller of the two sizes)
 constexpr int kSortSlots = 3;        // radix sorts per launch: samples, pairs, triangles
 
 }  // namespace fdzb

@@ -442,7 +442,8 @@ __global__ void __launch_bounds__(256)
 // (:184-202) with the counting predicate used for both passes.
 // ---------------------------------------------------------------------------
 constexpr int kTriThreads = 256;
-constexpr int kTriTile = 64;   // triangles per pair-scan tile
+constexpr int kTriTile = 64;   // triangles per pair-scan tile (launches of up to kTriSmallLaunch triangles)
+constexpr int kTriSmallLaunch = 1 << 20;
 // Look-back status word of a triangle tile: [63:32] launch epoch, [31:30] flag,
 // [29:0] pair count (the pair capacity stays below 2^30).
 constexpr unsigned long long kScanAgg = 1ull << 30;
@@ -894,17 +895,26 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         nl += 2 + b.triPasses;
     }
     {
-        // tiles of 64 triangles, 8 a warp: a frame of few triangles still
-        // spreads over the SMs (2k triangles: pairs 0.159 -> 0.074 ms against
-        // tiles of 256; HD: 0.305 -> 0.283 ms); up to 8 blocks per SM (the
-        // sweeps wait on bin-statistics loads, so more resident warps hide more
-        // of that latency)
-        const int tiles = (b.totalTris + kTriTile - 1) / kTriTile;
+        // tiles of 64 triangles, 8 a warp, up to a million triangles: a frame
+        // of few triangles still spreads over the SMs (2k triangles: pairs
+        // 0.159 -> 0.074 ms against tiles of 256; HD: 0.305 -> 0.277 ms);
+        // above, tiles of 256 (64 frames, 8.9M triangles: 7.1 ms against 8.4
+        // ms with tiles of 64).  Up to 8 blocks per SM: the sweeps wait on
+        // bin-statistics loads, so more resident warps hide more of that latency.
+        const bool small = b.totalTris <= kTriSmallLaunch;
+        const int tile = small ? kTriTile : 256;
+        const int tiles = (b.totalTris + tile - 1) / tile;
         const int grid = tiles < sm * 8 ? (tiles > 0 ? tiles : 1) : sm * 8;
-        k_tri_pairs<kTriTile><<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
-                                                           b.triRec, b.binStat, b.triCount, b.triScanStatus,
-                                                           b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
-                                                           order, b.pairTriBits, b.counters);
+        if (small)
+            k_tri_pairs<kTriTile><<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
+                                                               b.triRec, b.binStat, b.triCount, b.triScanStatus,
+                                                               b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
+                                                               order, b.pairTriBits, b.counters);
+        else
+            k_tri_pairs<256><<<grid, kTriThreads, 0, s>>>(b.frames, b.states, b.triBases, nf, b.totalTris,
+                                                          b.triRec, b.binStat, b.triCount, b.triScanStatus,
+                                                          b.epochWord, b.pkeysA, b.pvalsA, b.pairCapacity,
+                                                          order, b.pairTriBits, b.counters);
         nl += 1;
     }
     if (b.dbgPKeys) {
