@@ -342,12 +342,14 @@ int engine_enqueue(Engine &e)
     // 64-bit row words when some frame's grid exceeds 32 rows or columns; the
     // lane-per-pair schedule covers square 32-bit grids without the depth
     // plane, other launches use lane per sample
-    bool wide = false, square = true;
+    bool wide = false, square = true, rows16 = true;
     for (const FrameSpec &f : e.frames) {
         wide = wide || f.light.N > fdzb::kMaxLightN32 || f.light.NC > fdzb::kMaxLightN32;
         square = square && f.light.N == f.light.NC;
+        rows16 = rows16 && f.light.N <= 16;
     }
     b.wide = wide ? 1 : 0;
+    b.rows16 = rows16 ? 1 : 0;
     b.depthPlane = e.depthPlane;
     b.rayCast = e.rayCast;
     b.occVariant = (e.occVariant == 1 && !wide && square && !e.depthPlane) ? 1 : 0;
@@ -439,7 +441,7 @@ int engine_enqueue(Engine &e)
         k.maxV = maxV;
         k.arena = e.arena;
         k.hFrames = e.hFrames;
-        k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane + 128 * b.openBox;
+        k.ov = b.occVariant + 16 * b.rayCast + 32 * b.wide + 64 * e.depthPlane + 128 * b.openBox + 256 * b.rows16;
         k.stream = e.stream;
         FDZB_CUDA(refresh_lookback(e));
         if (!e.graph || !(k == e.graphKey)) {

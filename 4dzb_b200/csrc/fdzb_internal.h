@@ -149,6 +149,7 @@ struct DeviceBuffers {
     int depthPlane;                             // 1: the frames test each triangle's own plane
     int openBox;                                // 1: the occlusion kernel with the open-box cull
     int countWork;                              // 1: the occlusion kernel that accumulates the work counters
+    int rows16;                                 // 1: every grid of the launch has at most 16 rows
     uint32_t *epochWord;                        // launch sequence number (look-back tags), advanced
                                                 // on the device by k_init so graph replays stay fresh
     // debug capture (nullptr unless enabled): pre-sort copies of the key/value arrays

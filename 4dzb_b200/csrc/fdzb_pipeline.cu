@@ -956,6 +956,12 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
         if (b.countWork) k_occlusion<RC, RT, DP, BX, 1><<<G, T, 0, s>>>(FDZB_OCC_ARGS);                     \
         else k_occlusion<RC, RT, DP, BX, 0><<<G, T, 0, s>>>(FDZB_OCC_ARGS);                                 \
     } while (0)
+    // grids of at most 16 rows: the lanes' masks in 16-row shared arrays
+#define FDZB_OCC16(DP, BX)                                                                                    \
+    do {                                                                                                   \
+        if (b.countWork) k_occlusion<0, uint32_t, DP, BX, 1, 16><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS); \
+        else k_occlusion<0, uint32_t, DP, BX, 0, 16><<<g32, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);             \
+    } while (0)
     if (b.wide) {
         if (b.rayCast) FDZB_OCC(1, u64, 0, 0, g64, t64);
         else if (b.depthPlane && b.openBox) FDZB_OCC(0, u64, 1, 1, g64, t64);
@@ -967,14 +973,19 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     } else if (b.occVariant == 1) {
         k_occlusion_pairs<<<sm * FDZB_OCC2_MINBLOCKS, kOccThreads, 0, s>>>(FDZB_OCC_ARGS);
     } else if (b.depthPlane) {
-        if (b.openBox) FDZB_OCC(0, uint32_t, 1, 1, g32, kOccThreads);
+        if (b.openBox && b.rows16) FDZB_OCC16(1, 1);
+        else if (b.openBox) FDZB_OCC(0, uint32_t, 1, 1, g32, kOccThreads);
+        else if (b.rows16) FDZB_OCC16(1, 0);
         else FDZB_OCC(0, uint32_t, 1, 0, g32, kOccThreads);
     } else if (b.openBox) {
-        FDZB_OCC(0, uint32_t, 0, 1, g32, kOccThreads);
+        if (b.rows16) FDZB_OCC16(0, 1);
+        else FDZB_OCC(0, uint32_t, 0, 1, g32, kOccThreads);
     } else {
-        FDZB_OCC(0, uint32_t, 0, 0, g32, kOccThreads);
+        if (b.rows16) FDZB_OCC16(0, 0);
+        else FDZB_OCC(0, uint32_t, 0, 0, g32, kOccThreads);
     }
 #undef FDZB_OCC
+#undef FDZB_OCC16
 #undef FDZB_OCC_ARGS
     nl += 2;
     if (ev) cudaEventRecord(ev[STAGE_COUNT], s);
