@@ -104,6 +104,10 @@ struct Counters {
 enum StageId { STAGE_SETUP = 0, STAGE_SAMPLE_SORT, STAGE_TRI_PAIRS, STAGE_PAIR_SORT, STAGE_OCCLUSION,
                STAGE_COUNT };
 
+// Start of a segment no element reached (the bins' sample and triangle
+// segments are built by atomic minima and maxima from this value and 0).
+constexpr int kSegAbsent = 0x7FFFFFFF;
+
 enum ErrorBits { ERR_LOOKBACK_TIMEOUT = 1, ERR_MBAR_TIMEOUT = 2, ERR_BAD_INPUT = 4, ERR_INTERNAL = 8 };
 
 // Device buffers of one launch (carved from one arena).

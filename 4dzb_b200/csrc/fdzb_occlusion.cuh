@@ -684,17 +684,23 @@ __device__ __forceinline__ int chunk_of(const FrameDesc &fr)
 // k_items: one thread per bin; a bin with n samples yields ceil(n / item) items
 // (bin, first sample offset, frame, triangle count), item = the frame's samples
 // per work item.
-__global__ void k_items(const FrameDesc *__restrict__ frames, const int32_t *__restrict__ bss,
-                        const int32_t *__restrict__ bse, const int32_t *__restrict__ bts,
-                        const int32_t *__restrict__ bte, const int *__restrict__ binBases, int nframes,
+__global__ void k_items(const FrameDesc *__restrict__ frames, int32_t *__restrict__ bss,
+                        int32_t *__restrict__ bse, int32_t *__restrict__ bts,
+                        int32_t *__restrict__ bte, const int *__restrict__ binBases, int nframes,
                         int totalBins, int4 *__restrict__ items, int capacity, Counters *ctr)
 {
     const int lane = threadIdx.x & 31;
+    // segments no element reached hold (kSegAbsent, 0): (0, 0), as the
+    // reference's pre-zeroed arrays (the samples' array has the extra slot of
+    // the unbinned samples)
+    if (blockIdx.x == 0 && threadIdx.x == 0 && bss[totalBins] == kSegAbsent) bss[totalBins] = bse[totalBins] = 0;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < totalBins;
          base += gridDim.x * blockDim.x) {
         const int b = base + lane;
         int n = 0, f = 0, isz = kItemSamples;
         if (b < totalBins) {
+            if (bss[b] == kSegAbsent) bss[b] = bse[b] = 0;
+            if (bts[b] == kSegAbsent) bts[b] = bte[b] = 0;
             const int cnt = bse[b] - bss[b];
             if (cnt > 0) {
                 f = frame_of(binBases, nframes, b);

@@ -56,11 +56,11 @@ __global__ void k_init(FrameState *states, int nframes, uint32_t *binStat, int32
         uint4 s1 = make_uint4(pos, 0u, 0u, 0u);
         reinterpret_cast<uint4 *>(binStat)[2 * b] = s0;
         reinterpret_cast<uint4 *>(binStat)[2 * b + 1] = s1;
-        bts[b] = 0;
+        bts[b] = kSegAbsent;   // segment bounds: lowered / raised by the sorts' last passes
         bte[b] = 0;
     }
     for (int b = gid; b <= totalBins; b += stride) {
-        bss[b] = 0;
+        bss[b] = kSegAbsent;
         bse[b] = 0;
     }
     for (int f = gid; f < nframes; f += stride) {
@@ -801,10 +801,12 @@ static_assert(kKeysTile >= kSortTile, "the look-back status array is sized for t
 // Sorts (kA, vA) with kB/vB as ping-pong buffers; `slot` selects the histogram
 // and ticket block (0 samples, 1 pairs, 2 triangles).  Pass p uses tag
 // 16*launch + 4*slot + p and the key's bits [shift0 + 8p, shift0 + 8p + 8).
-// vA == nullptr: keys alone.
+// vA == nullptr: keys alone.  With segStart/segEnd the last pass also writes
+// the bounds of the segments key >> segShift (nslots of them; K/binRaster.inl:5-33).
 static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *vA, uint32_t *kB,
                      uint32_t *vB, const int *n_dev, int n_static, int cap, int passes, int sm,
-                     cudaStream_t s, int shift0 = 0)
+                     cudaStream_t s, int shift0 = 0, int32_t *segStart = nullptr, int32_t *segEnd = nullptr,
+                     int segShift = 0, uint32_t nslots = 0)
 {
     uint32_t *hist = b.sortHist + slot * 4 * kRadix;
     k_radix_hist<<<grid_for(cap, kSortThreads, sm * 4), kSortThreads, 0, s>>>(kA, n_dev, n_static,
@@ -815,16 +817,22 @@ static void run_sort(const DeviceBuffers &b, int slot, uint32_t *kA, uint32_t *v
     const long long keysTiles = ((long long)cap + kKeysTile - 1) / kKeysTile;
     const int keysGrid = grid_for(keysTiles * kSortThreads, kSortThreads, sm * kKeysMinBlocks);
     for (int p = 0; p < passes; ++p) {
-        if (vA)
-            k_radix_pass<true><<<passGrid, kSortThreads, 0, s>>>(
-                ki, vi, ko, vo, n_dev, n_static, cap, shift0 + 8 * p, hist + p * kRadix, b.sortStatus,
-                b.epochWord, (uint32_t)(slot * 4 + p), b.counters->sortTileCounter + slot * 4 + p,
-                &b.counters->errorFlags);
+        const bool seg = segStart && p == passes - 1;
+#define FDZB_PASS_ARGS(VI, VO)                                                                               \
+    ki, VI, ko, VO, n_dev, n_static, cap, shift0 + 8 * p, hist + p * kRadix, b.sortStatus, b.epochWord,      \
+        (uint32_t)(slot * 4 + p), b.counters->sortTileCounter + slot * 4 + p, &b.counters->errorFlags
+        if (vA && seg)
+            k_radix_pass<true, kSortItems, FDZB_SORT_MINBLOCKS, true><<<passGrid, kSortThreads, 0, s>>>(
+                FDZB_PASS_ARGS(vi, vo), segStart, segEnd, segShift, nslots);
+        else if (vA)
+            k_radix_pass<true><<<passGrid, kSortThreads, 0, s>>>(FDZB_PASS_ARGS(vi, vo));
+        else if (seg)
+            k_radix_pass<false, kKeysItems, kKeysMinBlocks, true><<<keysGrid, kSortThreads, 0, s>>>(
+                FDZB_PASS_ARGS(nullptr, nullptr), segStart, segEnd, segShift, nslots);
         else
             k_radix_pass<false, kKeysItems, kKeysMinBlocks><<<keysGrid, kSortThreads, 0, s>>>(
-                ki, nullptr, ko, nullptr, n_dev, n_static, cap, shift0 + 8 * p, hist + p * kRadix, b.sortStatus,
-                b.epochWord, (uint32_t)(slot * 4 + p), b.counters->sortTileCounter + slot * 4 + p,
-                &b.counters->errorFlags);
+                FDZB_PASS_ARGS(nullptr, nullptr));
+#undef FDZB_PASS_ARGS
         uint32_t *t = ki;
         ki = ko;
         ko = t;
@@ -876,13 +884,9 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     // (b) sample sort and segments
     if (ev) cudaEventRecord(ev[STAGE_SAMPLE_SORT], s);
     run_sort(b, 0, b.keysA, b.valsA, b.keysB, b.valsB, nullptr, b.totalSamples, b.totalSamples,
-             b.samplePasses, sm, s);
-    uint32_t *sk = (b.samplePasses & 1) ? b.keysB : b.keysA;
+             b.samplePasses, sm, s, 0, b.binSampleStart, b.binSampleEnd, 0, (uint32_t)b.totalBins + 1u);
     uint32_t *sv = (b.samplePasses & 1) ? b.valsB : b.valsA;
-    k_find_start_end<<<grid_for(b.totalSamples, 256, sm * 8), 256, 0, s>>>(
-        sk, nullptr, b.totalSamples, b.totalSamples, 0, b.binSampleStart, b.binSampleEnd,
-        (uint32_t)b.totalBins + 1u, &b.counters->errorFlags);
-    nl += 2 + b.samplePasses;
+    nl += 1 + b.samplePasses;
     // (a) triangle/bin pairs, in the coverage order when one is asked for
     if (ev) cudaEventRecord(ev[STAGE_TRI_PAIRS], s);
     const uint32_t *order = nullptr;
@@ -928,14 +932,12 @@ cudaError_t run_pipeline(const DeviceBuffers &b, int maxS, int maxT, int maxV, c
     // bits, and the sorted keys are the triangle lists
     const bool packed = b.pairTriBits > 0;
     run_sort(b, 1, b.pkeysA, packed ? nullptr : b.pvalsA, b.pkeysB, packed ? nullptr : b.pvalsB,
-             &b.counters->pairCount, 0, b.pairCapacity, b.pairPasses, sm, s, b.pairTriBits);
+             &b.counters->pairCount, 0, b.pairCapacity, b.pairPasses, sm, s, b.pairTriBits, b.binTriStart,
+             b.binTriEnd, b.pairTriBits, (uint32_t)b.totalBins);
     uint32_t *pk = (b.pairPasses & 1) ? b.pkeysB : b.pkeysA;
     uint32_t *pv = packed ? pk : ((b.pairPasses & 1) ? b.pvalsB : b.pvalsA);
     const uint32_t triMask = packed ? (1u << b.pairTriBits) - 1u : 0xFFFFFFFFu;
-    k_find_start_end<<<grid_for(b.pairCapacity, 256, sm * 8), 256, 0, s>>>(
-        pk, &b.counters->pairCount, 0, b.pairCapacity, b.pairTriBits, b.binTriStart, b.binTriEnd,
-        (uint32_t)b.totalBins, &b.counters->errorFlags);
-    nl += 2 + b.pairPasses;
+    nl += 1 + b.pairPasses;
     // (c) + (d) occlusion and shading
     if (ev) cudaEventRecord(ev[STAGE_OCCLUSION], s);
     k_items<<<grid_for(b.totalBins, 256, sm * 8), 256, 0, s>>>(

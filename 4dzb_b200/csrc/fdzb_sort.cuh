@@ -60,13 +60,22 @@ __global__ void __launch_bounds__(kSortThreads)
 // One digit pass.  status: [tiles * 256] zeroed before the pass; ticket zeroed.
 // KV = false sorts keys alone (vin and vout unused): the pairs' keys can carry
 // their value in the bits below the digits.
-template <bool KV, int ITEMS = kSortItems, int MINB = FDZB_SORT_MINBLOCKS>
+// SEG = true (the last pass of a sort whose keys name segments, key >> segShift):
+// the pass also writes the segment bounds of the sorted output, the restated
+// K/binRaster.inl:5-33 -- segStart[k] = first index of segment k, segEnd[k] =
+// last index + 1.  A tile holds its elements in final order, so an element that
+// begins (ends) a run of its segment inside the tile lowers segStart (raises
+// segEnd) of that segment by an atomic; the smallest first and the largest last
+// over the tiles are the segment's bounds.  The arrays start at (INT_MAX, 0);
+// absent segments keep those and are set to (0, 0) afterwards (k_items).
+template <bool KV, int ITEMS = kSortItems, int MINB = FDZB_SORT_MINBLOCKS, bool SEG = false>
 __global__ void __launch_bounds__(kSortThreads, MINB)
     k_radix_pass(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                  uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, const int *n_dev,
                  int n_static, int cap, int shift, const uint32_t *__restrict__ hist,
                  unsigned long long *status, const uint32_t *epochWord, uint32_t epochLo, int *ticket,
-                 int *err)
+                 int *err, int32_t *segStart = nullptr, int32_t *segEnd = nullptr, int segShift = 0,
+                 uint32_t nslots = 0)
 {
     constexpr int WARPS = kSortThreads / 32;
     constexpr int TILE = kSortThreads * ITEMS;
@@ -205,31 +214,17 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
             if (dst < (uint32_t)cap) {
                 kout[dst] = kk;
                 if (KV) vout[dst] = s_v[j];
+                if (SEG) {
+                    const uint32_t sg = kk >> segShift;
+                    if (sg >= nslots) {
+                        atomicOr(err, (int)ERR_INTERNAL);
+                    } else {
+                        if (j == 0 || (s_k[j - 1] >> segShift) != sg) atomicMin(&segStart[sg], (int)dst);
+                        if (j == tileN - 1 || (s_k[j + 1] >> segShift) != sg) atomicMax(&segEnd[sg], (int)dst + 1);
+                    }
+                }
             }
         }
-    }
-}
-
-// Segment bounds of a sorted key array (K/binRaster.inl:5-33): start[key] = first
-// index, end[key] = last index + 1, for keys present (arrays pre-zeroed).
-// The segment key is key >> shift (low bits may carry a secondary sort key).
-__global__ void k_find_start_end(const uint32_t *__restrict__ keys, const int *n_dev, int n_static,
-                                 int cap, int shift, int32_t *__restrict__ start,
-                                 int32_t *__restrict__ end, uint32_t nslots, int *err)
-{
-    const int n = sort_count(n_dev, n_static, cap);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i] >> shift;
-        const uint32_t kp = i > 0 ? (keys[i - 1] >> shift) : 0u;
-        if (k >= nslots || kp >= nslots) {
-            atomicOr(err, (int)ERR_INTERNAL);
-            continue;
-        }
-        if (i == 0 || kp != k) {
-            start[k] = i;
-            if (i > 0) end[kp] = i;
-        }
-        if (i == n - 1) end[k] = n;
     }
 }
 
